@@ -1,0 +1,239 @@
+/*
+ * maxflow_b200.h — C ABI of the B200 exact max-flow engine.
+ *
+ * Drop-in boundary for the per-query solve of the Region-Aware push-relabel
+ * program (reference project file Region_Aware_PR_with_Pruning_BoundaryCore.cu,
+ * "RA" below).  The reference has no library API: its in-process seam is
+ *   init_global_graph_on_device(CSRGraph&, R, region_start, region_end, region_id)  RA:1293
+ *   init_state_for_st(DynamicState&, V, E, R)                                      RA:1336
+ *   flow_t run_gpu_static_with_state(int s, int t, DynamicState&)                  RA:2119
+ *   free_state_for_st(DynamicState&)                                               RA:86
+ * and its outer boundary is the CLI  prog <input_dir> <output_dir> [static|dynamic]
+ * (RA:2561-2570) reading graph.txt / test.txt and writing res_mt.txt.
+ * The entry points below replace that seam; the CLI maxflow_b200 is built on
+ * them.
+ *
+ * Conventions: every function returns an int status (MF_OK = 0, else an
+ * MF_ERR_* code; mf_last_error_string() describes the last failure on the
+ * calling thread).  No exceptions cross the ABI.  The caller owns every host
+ * buffer; the engine owns device memory.  Vertex ids at this ABI are 0-based
+ * ids of the caller's graph (the engine's internal region order is hidden).
+ * Flows and capacities are int64 and exact.  A graph handle may be used by
+ * one thread at a time.
+ */
+#ifndef MAXFLOW_B200_H
+#define MAXFLOW_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MF_OK 0
+#define MF_ERR_ARG 1          /* invalid argument */
+#define MF_ERR_CUDA 2         /* CUDA runtime error (no device, launch failure, ...) */
+#define MF_ERR_NOMEM 3        /* device or host allocation failed / admission refused */
+#define MF_ERR_IO 4           /* file missing or malformed header */
+#define MF_ERR_ITER_LIMIT 5   /* a solve exceeded opts.iter_max rounds */
+#define MF_ERR_TIMEOUT 6      /* a device wait exceeded its time limit */
+#define MF_ERR_INEXACT 7      /* internal consistency check failed */
+#define MF_ERR_CERTIFY 8      /* certificate check failed */
+
+typedef struct mf_graph mf_graph;
+
+/* Solver options.  mf_opts_default() fills the defaults; fields mirror the
+ * reference's knobs (RA:1459-1484, RA:1936, RA:2644-2648). */
+typedef struct mf_opts {
+    int kernel_cycles;     /* K: discharge cycles per active vertex per round (RA:1467); 0 = max(4, avg degree) */
+    int gr_freq;           /* rounds between global relabels at most (GR_FREQ0, RA:1466) */
+    double gr_work_alpha;  /* also relabel once scanned arcs exceed alpha x mask arcs (0 = off) */
+    int prune_mode;        /* 0: RA:1391-1445 mask (fwd(s) & undirected comp(t)); 1: fwd(s) & bwd(t) (default) */
+    int path_push_switch;  /* active count at or below which path-push starts (RA:1480) */
+    int max_path_len;      /* path-push hop limit (RA:1481) */
+    int use_path_push;     /* 1 = enable sparse-phase path push (RA:1765-1831) */
+    int use_hot_sweep;     /* 1 = enable hot-region extra sweep (RA:1899-1984) */
+    int hot_regions;       /* top-K regions for the hot sweep (RA:1936) */
+    int use_rm;            /* 1 = enable region-aware invalid-arc repair (RA:1991-2097) */
+    int rm_freq;           /* initial RM frequency (RM_FREQ0, RA:1468) */
+    int h_cut;             /* height threshold for "high" active vertices (RA:1470) */
+    int stagnate_rounds;   /* stagnation window (RA:1472) */
+    int force_rm;          /* tests: run RM every rm_freq rounds regardless of frac_high */
+    int force_path_push;   /* tests: use path push whenever active <= path_push_switch */
+    long long iter_max;    /* round cap per solve (RA:1476) */
+    int group_ctas;        /* CTAs per query group in batched solves (0 = autotuned default) */
+    int threads;           /* threads per CTA (0 = 512) */
+    int certify;           /* 1 = return excess to the source and check the certificate */
+    int verbose;           /* 1 = per-query log lines on stderr */
+} mf_opts;
+
+/* Per-query statistics (all counts exact device counters). */
+typedef struct mf_stats {
+    long long flow;
+    int status;               /* MF_OK or MF_ERR_* for this query */
+    int mask_vertices;        /* vertices kept by the prune */
+    long long mask_arcs;      /* arcs out of kept vertices */
+    long long rounds;         /* discharge rounds */
+    long long global_relabels;
+    long long arcs_examined;  /* residual-arc examinations (16 B each, algorithmic) */
+    long long vertices_examined; /* vertex examinations (16 B each, algorithmic) */
+    long long pushes;
+    long long rm_fixed;       /* arcs repaired by RM */
+    long long path_push_rounds;
+    long long hot_sweeps;
+    long long deficit_phases; /* times the solver drained deficits back to the sink */
+    long long cut_capacity;   /* certify only: capacity of the residual s-t cut */
+    double time_ms;           /* device time of the solve (single-query calls) */
+} mf_stats;
+
+void mf_opts_default(mf_opts *o);
+const char *mf_last_error_string(void);
+const char *mf_version(void);
+
+/* ---- graphs ---------------------------------------------------------- */
+
+/* Build a graph from 0-based edge arrays with the reference's reader rules
+ * (RA:1068-1089): edges with an endpoint outside [0,n), u == v or cap <= 0
+ * are dropped; each kept edge gives a forward arc and a zero-capacity
+ * reverse arc.  The CSR is partitioned into R regions by capacity-degree
+ * score and renumbered region-contiguously on the device (RA:1130-1276);
+ * R = 0 means 128 (RA:2583), and R is clamped to [1, n]. */
+int mf_graph_create_from_edges(int n, long long m, const int32_t *u, const int32_t *v,
+                               const int64_t *cap, int R, mf_graph **out);
+/* Same, reading <path> in graph.txt format (1-based ids, RA:1051-1075). */
+int mf_graph_load_file(const char *path, int R, mf_graph **out);
+int mf_graph_destroy(mf_graph *g);
+/* n, kept arcs (2 x kept edges), R. */
+int mf_graph_info(const mf_graph *g, int *n, long long *arcs, int *R);
+/* Copy the region-ordered CSR and the maps back to the host (any pointer may
+ * be NULL).  new_id[old] = region-ordered id; region_start has R+1 entries. */
+int mf_graph_export(const mf_graph *g, int32_t *row, int32_t *col, int64_t *cap, int32_t *rev,
+                    int32_t *new_id, int32_t *region_start, double *score, int32_t *part);
+/* Repartition the graph into R regions (rebuilds the region-ordered CSR). */
+int mf_graph_repartition(mf_graph *g, int R);
+
+/* ---- solves ----------------------------------------------------------- */
+
+/* One (s,t) solve on the whole GPU (replaces run_gpu_static_with_state,
+ * RA:2119, plus the per-query prune of RA:2666-2698).  Invalid ids or s == t
+ * give flow 0 and MF_OK (RA:2659-2663).  opts/stats may be NULL. */
+int mf_solve(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, int64_t *flow,
+             mf_stats *stats);
+/* nq independent solves in one persistent launch: query groups of CTAs pull
+ * queries from a device queue, each with its own residual slot.  flows[i]
+ * (and stats[i], if stats != NULL) for query i. */
+int mf_solve_batch(mf_graph *g, int nq, const int32_t *s, const int32_t *t, const mf_opts *opts,
+                   int64_t *flows, mf_stats *stats);
+/* Device time (ms) of the last mf_solve_batch / mf_solve call on g. */
+double mf_last_device_ms(const mf_graph *g);
+
+/* Debug/parity views of single phases (0-based caller ids):
+ * prune mask for (s,t) under opts->prune_mode (mask: n bytes, caller order);
+ * exact residual heights after the initial preflow (heights: n ints, caller
+ * order; unreachable = n). */
+int mf_debug_prune_mask(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, uint8_t *mask,
+                        int *kept);
+int mf_debug_initial_heights(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts,
+                             int32_t *heights);
+/* Solve and copy the final residual capacities back (arcs in region order,
+ * matching mf_graph_export's CSR). */
+int mf_solve_residual(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, int64_t *flow,
+                      int64_t *res, mf_stats *stats);
+
+/* Solve (s,t), return the excess to the source (phase 2), and check on the
+ * device: residuals non-negative and pairwise conserved, zero excess at every
+ * vertex other than s and t, and a residual s-t cut whose capacity equals
+ * the flow.  MF_OK only when every check passes; stats->cut_capacity. */
+int mf_certify(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, int64_t *flow,
+               mf_stats *stats);
+
+/* ---- dynamic capacities ----------------------------------------------- */
+
+/* Apply nb capacity changes: arc u->v (first matching forward arc, caller
+ * ids) gets cap += delta[i], clamped at 0 (extends OnAdd_kernel, RA:959-1000,
+ * which handled increases only).  Pairs with no such arc are skipped and
+ * counted in *skipped (may be NULL). */
+int mf_update_caps(mf_graph *g, int nb, const int32_t *u, const int32_t *v, const int64_t *delta,
+                   int *skipped);
+
+/* Resident queries: a session keeps the residual state of nq queries on the
+ * device across capacity updates (what the reference's dynamic mode,
+ * RA:2844-2916, sets up but never updates).  mf_session_solve solves all of
+ * them from scratch; mf_session_update applies a capacity batch to the graph
+ * and repairs every resident query incrementally from its kept residual
+ * state (flow cancelled on arcs whose capacity fell below their flow, new
+ * capacity saturated from the source, then push-relabel resumes). */
+typedef struct mf_session mf_session;
+int mf_session_create(mf_graph *g, int nq, const int32_t *s, const int32_t *t, const mf_opts *opts,
+                      mf_session **out);
+int mf_session_solve(mf_session *ss, int64_t *flows, mf_stats *stats);
+int mf_session_update(mf_session *ss, int nb, const int32_t *u, const int32_t *v,
+                      const int64_t *delta, int64_t *flows, mf_stats *stats);
+int mf_session_destroy(mf_session *ss);
+
+/* ---- serving ------------------------------------------------------------ */
+
+/* Continuous-batching server over several device-resident graphs.  A
+ * persistent kernel pulls requests from a host-written ring; requests that
+ * arrive while others run are admitted as soon as a residual slot frees up.
+ * Slots are sized for the largest graph and their number is chosen from free
+ * HBM at creation (max_slots caps it; 0 = as many as fit, up to the GPU's
+ * query groups). */
+typedef struct mf_server mf_server;
+int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int max_slots,
+                     mf_server **out);
+int mf_server_slots(const mf_server *sv, int *slots);
+/* Enqueue one request; returns its ticket (0,1,2,...) in *ticket. */
+int mf_server_submit(mf_server *sv, int graph, int32_t s, int32_t t, long long *ticket);
+/* Non-blocking: 1 in *done when the ticket finished (flow, device latency in
+ * ms from admission to completion, status). */
+int mf_server_poll(mf_server *sv, long long ticket, int *done, int64_t *flow, double *latency_ms,
+                   int *status);
+/* Block until every submitted request has finished. */
+int mf_server_drain(mf_server *sv);
+int mf_server_destroy(mf_server *sv);
+
+/* ---- autotuning ---------------------------------------------------------- */
+
+/* Time mf_solve_batch on the given sample of queries over a grid of
+ * (R, kernel_cycles, gr_freq, group_ctas) and write the fastest into *best
+ * (R into *best_R).  Repartitions g to the best R before returning. */
+int mf_autotune(mf_graph *g, int nq, const int32_t *s, const int32_t *t, const mf_opts *base,
+                mf_opts *best, int *best_R);
+
+/* ---- synthetic workloads (seeded; used by the bench and the tests) -------- */
+
+/* Uniform directed graph: u != v uniform in [0,n), cap uniform in [lo,hi]. */
+int mf_gen_uniform(int n, long long m, long long lo, long long hi, unsigned long long seed,
+                   int32_t *u, int32_t *v, int64_t *cap);
+/* R-MAT with n = 2^scale and m draws of probabilities (a,b,c,1-a-b-c); self
+ * loops dropped; returns the kept count in *kept (arrays hold m entries). */
+int mf_gen_rmat(int scale, long long m, double a, double b, double c, long long lo, long long hi,
+                unsigned long long seed, int32_t *u, int32_t *v, int64_t *cap, long long *kept);
+/* W x H 4-connected grid plus source (id W*H) and sink (id W*H+1):
+ * neighbour arcs cap 1+floor(255*exp(-d^2/50)), d ~ N(0,40); each pixel gets
+ * one terminal arc (source->p or p->sink by a seeded coin) with cap uniform
+ * in [0,255].  Arrays hold 4*W*H + W*H entries; *m receives the count. */
+int mf_gen_grid(int W, int H, unsigned long long seed, int32_t *u, int32_t *v, int64_t *cap,
+                long long *m);
+/* Queries for a power-law graph: nhub pairs with s in the top 1% by
+ * out-degree and t in the top 1% by in-degree, then nuni uniform pairs;
+ * s != t. */
+int mf_gen_queries_hub(int n, long long m, const int32_t *u, const int32_t *v, int nhub, int nuni,
+                       unsigned long long seed, int32_t *s, int32_t *t);
+/* Write graph.txt / test.txt (1-based ids). */
+int mf_write_graph_txt(const char *path, int n, long long m, const int32_t *u, const int32_t *v,
+                       const int64_t *cap);
+int mf_write_test_txt(const char *path, int nq, const int32_t *s, const int32_t *t);
+/* Parse graph.txt with the reference's rules (RA:1051-1075) into 0-based
+ * arrays holding cap_len entries; *n, *m_read. */
+int mf_read_graph_txt(const char *path, int *n, long long *m_read, int32_t *u, int32_t *v,
+                      int64_t *cap, long long cap_len);
+/* Count of edge lines in a graph.txt header (to size the arrays). */
+int mf_graph_txt_header(const char *path, int *n, long long *m);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MAXFLOW_B200_H */

@@ -1,0 +1,1235 @@
+// Host side of the C ABI (include/maxflow_b200.h): graph residency, residual
+// slots, launch configuration, batched / session / serving drivers.
+//
+// Reference seam replaced (Region_Aware_PR_with_Pruning_BoundaryCore.cu):
+//   build_graph RA:1044-1126 ............ host CSR build below (same reader rules)
+//   init_global_graph_on_device RA:1293 .. mf_graph_create_from_edges (device-resident,
+//                                          region-ordered CSR built on the device)
+//   init_state_for_st / free_state RA:1336, RA:86 .. residual slots (allocated once,
+//                                          stamp-reset, reused across queries)
+//   run_gpu_static_with_state RA:2119 .... mf_solve / mf_solve_batch
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/maxflow_b200.h"
+#include "mf_build.cuh"
+#include "mf_solver.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(e_ == cudaErrorMemoryAllocation ? MF_ERR_NOMEM : MF_ERR_CUDA,     \
+                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                        __LINE__);                                                        \
+    } while (0)
+
+struct DevInfo {
+    int sms = 0;
+    int bps = 0;  // co-resident mf_kernel CTAs per SM at the default block size
+    int threads = 512;
+    bool ok = false;
+};
+
+int dev_info(DevInfo &d, int threads) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
+    d.threads = threads;
+    d.bps = mf_kernel_max_blocks_per_sm(threads);
+    if (d.bps <= 0) return fail(MF_ERR_CUDA, "mf_kernel cannot be resident with %d threads", threads);
+    d.ok = true;
+    return MF_OK;
+}
+
+size_t slot_bytes(int n, i64 arcs) {
+    size_t b = 0;
+    auto add = [&](size_t x) { b += (x + 255) & ~(size_t)255; };
+    add(sizeof(i64) * (size_t)std::max<i64>(arcs, 1));  // res
+    add(sizeof(i64) * (size_t)n);                        // ex
+    for (int i = 0; i < 7; ++i) add(sizeof(int) * (size_t)n);  // h mark qmark claim vlist qa qb
+    add(sizeof(int) * 1024);                             // hot
+    add(sizeof(int) * 1024);                             // ract
+    add(sizeof(int) * 16);                               // cnt
+    add(sizeof(i64) * 128);                              // acc
+    add(sizeof(GroupBar));
+    add(sizeof(unsigned));                               // clock
+    add(sizeof(int) * 8);                                // meta
+    return b;
+}
+
+struct SlotPool {
+    int n = 0;
+    i64 arcs = 0;
+    std::vector<void *> bases;
+    std::vector<DSlot> host;
+    DSlot *dev = nullptr;
+    int dev_cap = 0;
+
+    int grow(int want) {
+        while ((int)host.size() < want) {
+            size_t bytes = slot_bytes(n, arcs);
+            void *base = nullptr;
+            cudaError_t e = cudaMalloc(&base, bytes);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                return fail(MF_ERR_NOMEM, "residual slot allocation (%zu bytes) failed: %s", bytes,
+                            cudaGetErrorString(e));
+            }
+            CK(cudaMemset(base, 0, bytes));
+            char *p = (char *)base;
+            auto take = [&](size_t x) {
+                char *r = p;
+                p += (x + 255) & ~(size_t)255;
+                return (void *)r;
+            };
+            DSlot s;
+            s.res = (i64 *)take(sizeof(i64) * (size_t)std::max<i64>(arcs, 1));
+            s.ex = (i64 *)take(sizeof(i64) * (size_t)n);
+            s.h = (int *)take(sizeof(int) * (size_t)n);
+            s.mark = (unsigned *)take(sizeof(int) * (size_t)n);
+            s.qmark = (unsigned *)take(sizeof(int) * (size_t)n);
+            s.claim = (unsigned *)take(sizeof(int) * (size_t)n);
+            s.vlist = (int *)take(sizeof(int) * (size_t)n);
+            s.qa = (int *)take(sizeof(int) * (size_t)n);
+            s.qb = (int *)take(sizeof(int) * (size_t)n);
+            s.hot = (int *)take(sizeof(int) * 1024);
+            s.ract = (int *)take(sizeof(int) * 1024);
+            s.cnt = (int *)take(sizeof(int) * 16);
+            s.acc = (i64 *)take(sizeof(i64) * 128);
+            s.bar = (GroupBar *)take(sizeof(GroupBar));
+            s.clock = (unsigned *)take(sizeof(unsigned));
+            s.meta = (int *)take(sizeof(int) * 8);
+            bases.push_back(base);
+            host.push_back(s);
+        }
+        if (dev_cap < (int)host.size()) {
+            if (dev) cudaFree(dev);
+            dev = nullptr;
+            dev_cap = 0;
+            CK(cudaMalloc(&dev, sizeof(DSlot) * host.size()));
+            dev_cap = (int)host.size();
+        }
+        CK(cudaMemcpy(dev, host.data(), sizeof(DSlot) * host.size(), cudaMemcpyHostToDevice));
+        return MF_OK;
+    }
+    void release() {
+        for (void *b : bases) cudaFree(b);
+        bases.clear();
+        host.clear();
+        if (dev) cudaFree(dev);
+        dev = nullptr;
+        dev_cap = 0;
+    }
+};
+
+// Zero the group barriers of the first nslots slots and read their clocks.
+__global__ void k_prepare_slots(DSlot *slots, int nslots, unsigned *clocks) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nslots) {
+        slots[i].bar->arrive = 0;
+        slots[i].bar->gen = 0;
+        clocks[i] = *slots[i].clock;
+    }
+}
+
+// Stamp arrays are only compared against the slot's own monotonic clock;
+// before the 32-bit clock can wrap, the slot is reset to zero.
+__global__ void k_reset_slot(DSlot s, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        s.mark[i] = 0;
+        s.qmark[i] = 0;
+        s.claim[i] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *s.clock = 0;
+}
+
+// Capacity updates: resolve (u,v) to the first forward arc u->v.
+__global__ void k_find_arcs(int nb, const int *u, const int *v, const int *row, const int *col,
+                            const unsigned char *fwd, const i64 *cap, int *arc, i64 *capv) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nb) return;
+    int a = -1;
+    int x = u[i], y = v[i];
+    if (x >= 0 && y >= 0) {
+        for (int e = row[x]; e < row[x + 1]; ++e)
+            if (col[e] == y && fwd[e]) {
+                a = e;
+                break;
+            }
+    }
+    arc[i] = a;
+    capv[i] = (a >= 0) ? cap[a] : 0;
+}
+
+__global__ void k_apply_caps(int nu, const ArcUpdate *upd, i64 *cap) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nu) cap[upd[i].arc] = upd[i].new_cap;
+}
+
+}  // namespace
+
+struct mf_graph {
+    int n = 0;
+    i64 arcs = 0;
+    int R = 0;
+    int avg_deg = 0;
+    std::vector<int> new_id;  // caller id -> internal id
+    std::vector<int> old_id;  // internal id -> caller id
+    std::vector<double> score_caller;
+    std::vector<int> part_caller;
+    // region-ordered device CSR
+    int *row = nullptr, *col = nullptr, *rev = nullptr, *region_of = nullptr,
+        *region_start = nullptr;
+    i64 *cap = nullptr;
+    unsigned char *fwd = nullptr;
+    DGraph *d_graph = nullptr;
+    SlotPool pool;
+    DevInfo dev;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int *d_err = nullptr, *d_qnext = nullptr;
+    unsigned *d_clocks = nullptr;
+    int clocks_cap = 0;
+    QOut *d_out = nullptr;
+    int out_cap = 0;
+    int *d_q = nullptr;  // s | t | slot, 3*q_cap
+    int q_cap = 0;
+    int *h_pin = nullptr;  // pinned staging for queries
+    QOut *h_out = nullptr;
+    int pin_cap = 0;
+    double last_ms = 0.0;
+    long launches = 0;
+};
+
+struct mf_session {
+    mf_graph *g = nullptr;
+    int nq = 0;
+    std::vector<int> s, t;  // internal
+    SlotPool pool;
+    mf_opts opts;
+    bool solved = false;
+};
+
+namespace {
+
+void free_graph_arrays(mf_graph *g) {
+    cudaFree(g->row);
+    cudaFree(g->col);
+    cudaFree(g->rev);
+    cudaFree(g->cap);
+    cudaFree(g->fwd);
+    cudaFree(g->region_of);
+    cudaFree(g->region_start);
+    cudaFree(g->d_graph);
+    g->row = g->col = g->rev = g->region_of = g->region_start = nullptr;
+    g->cap = nullptr;
+    g->fwd = nullptr;
+    g->d_graph = nullptr;
+}
+
+// Partition + reorder the device CSR given in (row,col,cap,rev,fwd), whose
+// vertex i is caller vertex in_ids[i].  Replaces the graph arrays.
+int partition_into(mf_graph *g, int R, int *row, int *col, i64 *cap, int *rev, unsigned char *fwd,
+                   const std::vector<int> &in_to_caller) {
+    const int n = g->n;
+    const i64 arcs = g->arcs;
+    BuildIn in{n, R, arcs, row, col, cap, rev, fwd};
+    BuildOut out{};
+    CK(cudaMalloc(&out.row, sizeof(int) * ((size_t)n + 1)));
+    CK(cudaMalloc(&out.col, sizeof(int) * (size_t)std::max<i64>(arcs, 1)));
+    CK(cudaMalloc(&out.cap, sizeof(i64) * (size_t)std::max<i64>(arcs, 1)));
+    CK(cudaMalloc(&out.rev, sizeof(int) * (size_t)std::max<i64>(arcs, 1)));
+    CK(cudaMalloc(&out.fwd, (size_t)std::max<i64>(arcs, 1)));
+    CK(cudaMalloc(&out.new_id, sizeof(int) * (size_t)n));
+    CK(cudaMalloc(&out.old_id, sizeof(int) * (size_t)n));
+    CK(cudaMalloc(&out.region_start, sizeof(int) * ((size_t)R + 1)));
+    CK(cudaMalloc(&out.region_of, sizeof(int) * (size_t)n));
+    CK(cudaMalloc(&out.score, sizeof(double) * (size_t)n));
+    CK(cudaMalloc(&out.part, sizeof(int) * (size_t)n));
+    void *scratch = nullptr;
+    CK(cudaMalloc(&scratch, mf_partition_scratch_bytes(n, arcs, R)));
+    CK(mf_partition_reorder(in, out, scratch, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    cudaFree(scratch);
+    std::vector<int> nid(n), sc_part(n);
+    std::vector<double> sc(n);
+    CK(cudaMemcpy(nid.data(), out.new_id, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(sc.data(), out.score, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(sc_part.data(), out.part, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    cudaFree(out.new_id);
+    cudaFree(out.old_id);
+    cudaFree(out.score);
+    cudaFree(out.part);
+    // compose: caller -> input index -> internal
+    std::vector<int> new_id(n), old_id(n);
+    g->score_caller.assign(n, 0.0);
+    g->part_caller.assign(n, 0);
+    for (int i = 0; i < n; ++i) {
+        int x = in_to_caller[i];
+        new_id[x] = nid[i];
+        old_id[nid[i]] = x;
+        g->score_caller[x] = sc[i];
+        g->part_caller[x] = sc_part[i];
+    }
+    free_graph_arrays(g);
+    g->row = out.row;
+    g->col = out.col;
+    g->cap = out.cap;
+    g->rev = out.rev;
+    g->fwd = out.fwd;
+    g->region_start = out.region_start;
+    g->region_of = out.region_of;
+    g->new_id.swap(new_id);
+    g->old_id.swap(old_id);
+    g->R = R;
+    DGraph dg{n, R, arcs, g->row, g->col, g->rev, g->cap, g->region_of};
+    CK(cudaMalloc(&g->d_graph, sizeof(DGraph)));
+    CK(cudaMemcpy(g->d_graph, &dg, sizeof(DGraph), cudaMemcpyHostToDevice));
+    return MF_OK;
+}
+
+int ensure_launch_buffers(mf_graph *g, int nq, int nslots) {
+    if (!g->d_err) {
+        CK(cudaMalloc(&g->d_err, sizeof(int) * 2));
+        g->d_qnext = g->d_err + 1;
+    }
+    if (g->out_cap < nq) {
+        cudaFree(g->d_out);
+        cudaFreeHost(g->h_out);
+        g->d_out = nullptr;
+        g->h_out = nullptr;
+        CK(cudaMalloc(&g->d_out, sizeof(QOut) * nq));
+        CK(cudaMallocHost(&g->h_out, sizeof(QOut) * nq));
+        g->out_cap = nq;
+    }
+    if (g->q_cap < nq) {
+        cudaFree(g->d_q);
+        cudaFreeHost(g->h_pin);
+        g->d_q = nullptr;
+        g->h_pin = nullptr;
+        CK(cudaMalloc(&g->d_q, sizeof(int) * 3 * (size_t)nq));
+        CK(cudaMallocHost(&g->h_pin, sizeof(int) * 3 * (size_t)nq));
+        g->q_cap = nq;
+    }
+    if (g->clocks_cap < nslots) {
+        cudaFree(g->d_clocks);
+        g->d_clocks = nullptr;
+        CK(cudaMalloc(&g->d_clocks, sizeof(unsigned) * nslots));
+        g->clocks_cap = nslots;
+    }
+    return MF_OK;
+}
+
+KOpts resolve_opts(const mf_opts &o, int avg_deg) {
+    KOpts k;
+    k.K = o.kernel_cycles > 0 ? o.kernel_cycles : std::max(4, avg_deg);
+    k.gr_freq = std::max(1, o.gr_freq);
+    k.gr_alpha = o.gr_work_alpha;
+    k.prune_mode = o.prune_mode;
+    k.pp_switch = o.path_push_switch;
+    k.max_path = std::max(1, o.max_path_len);
+    k.use_pp = o.use_path_push;
+    k.use_hot = o.use_hot_sweep;
+    k.hot_k = std::max(1, o.hot_regions);
+    k.use_rm = o.use_rm;
+    k.rm_freq = std::max(1, o.rm_freq);
+    k.h_cut = o.h_cut;
+    k.stagnate = std::max(1, o.stagnate_rounds);
+    k.force_rm = o.force_rm;
+    k.force_pp = o.force_path_push;
+    k.iter_max = o.iter_max > 0 ? o.iter_max : 20000000;
+    return k;
+}
+
+// Device time limit per solve launch: MF_TIME_LIMIT_S seconds (default 600).
+u64 launch_time_limit_ns() {
+    const char *e = getenv("MF_TIME_LIMIT_S");
+    double s = e ? atof(e) : 600.0;
+    if (s <= 0) return 0;
+    return (u64)(s * 1e9);
+}
+
+int status_from_err(int e) {
+    switch (e) {
+    case MFD_OK: return MF_OK;
+    case MFD_ITER_LIMIT: return MF_ERR_ITER_LIMIT;
+    case MFD_TIMEOUT: return MF_ERR_TIMEOUT;
+    case MFD_INEXACT: return MF_ERR_INEXACT;
+    case MFD_CERTIFY: return MF_ERR_CERTIFY;
+    default: return MF_ERR_CUDA;
+    }
+}
+
+// Core launcher: nq queries (internal ids; s < 0 = skip) in `pool`'s slots.
+// per_query_slot: query i uses slot i (sessions); else a slot per group.
+int launch(mf_graph *g, SlotPool &pool, int nq, const int *s_int, const int *t_int,
+           bool per_query_slot, const mf_opts &o, int mode, void *dbg, const ArcUpdate *d_upd,
+           int nupd, int G_req, QOut *outs) {
+    if (!g->dev.ok) {
+        int rc = dev_info(g->dev, o.threads > 0 ? o.threads : 512);
+        if (rc) return rc;
+    }
+    const int threads = g->dev.threads;
+    const int max_grid = g->dev.sms * g->dev.bps;
+    int G, ngroups;
+    if (G_req <= 0 || G_req >= max_grid) {
+        G = max_grid;
+        ngroups = 1;
+    } else {
+        G = G_req;
+        ngroups = std::max(1, max_grid / G);
+    }
+    ngroups = std::min(ngroups, std::max(1, nq));
+    int nslots = per_query_slot ? nq : ngroups;
+    if (!per_query_slot) {
+        if ((int)pool.host.size() < nslots) {
+            size_t fr = 0, tot = 0;
+            CK(cudaMemGetInfo(&fr, &tot));
+            size_t per = slot_bytes(pool.n, pool.arcs);
+            int fit = (int)pool.host.size() + (int)((fr * 0.85) / (double)per);
+            if (fit < 1) return fail(MF_ERR_NOMEM, "admission: no HBM for a residual slot (%zu bytes)", per);
+            nslots = std::min(nslots, fit);
+            ngroups = nslots;
+        }
+        int rc = pool.grow(nslots);
+        if (rc) return rc;
+    } else {
+        ngroups = std::min(ngroups, (int)pool.host.size());
+    }
+    int rc = ensure_launch_buffers(g, nq, (int)pool.host.size());
+    if (rc) return rc;
+    int *hp = g->h_pin;
+    for (int i = 0; i < nq; ++i) {
+        hp[i] = s_int[i];
+        hp[nq + i] = t_int[i];
+        hp[2 * nq + i] = per_query_slot ? i : 0;
+    }
+    CK(cudaMemcpyAsync(g->d_q, hp, sizeof(int) * 3 * (size_t)nq, cudaMemcpyHostToDevice, g->stream));
+    CK(cudaMemsetAsync(g->d_err, 0, sizeof(int) * 2, g->stream));
+    int ns = (int)pool.host.size();
+    k_prepare_slots<<<(ns + 127) / 128, 128, 0, g->stream>>>(pool.dev, ns, g->d_clocks);
+    KParams p{};
+    p.graphs = g->d_graph;
+    p.slots = pool.dev;
+    p.G = G;
+    p.nq = nq;
+    p.q_s = g->d_q;
+    p.q_t = g->d_q + nq;
+    p.q_g = nullptr;
+    p.q_slot = per_query_slot ? g->d_q + 2 * nq : nullptr;
+    p.q_next = g->d_qnext;
+    p.out = g->d_out;
+    p.err = g->d_err;
+    p.bar_limit_ns = 20ull * 1000 * 1000 * 1000;
+    p.time_limit_ns = launch_time_limit_ns();
+    p.o = resolve_opts(o, g->avg_deg);
+    p.mode = mode;
+    p.dbg = dbg;
+    p.upd = d_upd;
+    p.nupd = nupd;
+    int grid = ngroups * G;
+    cudaError_t le = cudaSuccess;
+    CK(cudaEventRecord(g->ev0, g->stream));
+    mf_launch_kernel(p, grid, threads, g->stream, G > 1, &le);
+    if (le != cudaSuccess) return fail(MF_ERR_CUDA, "mf_kernel launch (grid %d x %d): %s", grid, threads, cudaGetErrorString(le));
+    CK(cudaEventRecord(g->ev1, g->stream));
+    CK(cudaMemcpyAsync(g->h_out, g->d_out, sizeof(QOut) * nq, cudaMemcpyDeviceToHost, g->stream));
+    int herr[2] = {0, 0};
+    CK(cudaMemcpyAsync(herr, g->d_err, sizeof(int) * 2, cudaMemcpyDeviceToHost, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+    g->last_ms = ms;
+    g->launches++;
+    if (herr[0] != 0) {
+        // bounded wait expired somewhere: reset barriers, report
+        return fail(status_from_err(herr[0]), "device solve aborted (status %d)", herr[0]);
+    }
+    if (outs) memcpy(outs, g->h_out, sizeof(QOut) * nq);
+    // clock housekeeping: reset slots whose stamp clock passed 2^30
+    if ((g->launches & 15) == 0) {
+        std::vector<unsigned> clk(ns);
+        CK(cudaMemcpy(clk.data(), g->d_clocks, sizeof(unsigned) * ns, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < ns; ++i)
+            if (clk[i] > (1u << 30)) k_reset_slot<<<256, 256, 0, g->stream>>>(pool.host[i], pool.n);
+        CK(cudaStreamSynchronize(g->stream));
+    }
+    return MF_OK;
+}
+
+void fill_stats(mf_stats *st, const QOut &q, double ms) {
+    memset(st, 0, sizeof(*st));
+    st->flow = q.flow;
+    st->status = status_from_err(q.status);
+    st->mask_vertices = q.mask_n;
+    st->mask_arcs = q.mask_arcs;
+    st->rounds = q.rounds;
+    st->global_relabels = q.relabels;
+    st->arcs_examined = q.arcs_ex;
+    st->vertices_examined = q.verts_ex;
+    st->pushes = q.pushes;
+    st->rm_fixed = q.rm_fixed;
+    st->path_push_rounds = q.pp_rounds;
+    st->hot_sweeps = q.hot_sweeps;
+    st->deficit_phases = q.deficit_phases;
+    st->cut_capacity = q.cut;
+    st->time_ms = ms;
+}
+
+int to_internal(const mf_graph *g, int s, int t, int &si, int &ti) {
+    if (s < 0 || s >= g->n || t < 0 || t >= g->n || s == t) {
+        si = ti = -1;
+        return 0;
+    }
+    si = g->new_id[s];
+    ti = g->new_id[t];
+    return 1;
+}
+
+// Host CSR build with the reference reader's rules (RA:1068-1122).
+void host_csr(int n, i64 m, const int32_t *u, const int32_t *v, const int64_t *c,
+              std::vector<int> &row, std::vector<int> &col, std::vector<i64> &cap,
+              std::vector<int> &rev, std::vector<unsigned char> &fwd) {
+    std::vector<int> deg(n + 1, 0);
+    i64 kept = 0;
+    for (i64 i = 0; i < m; ++i) {
+        int a = u[i], b = v[i];
+        if (a < 0 || a >= n || b < 0 || b >= n || a == b || c[i] <= 0) continue;
+        deg[a]++;
+        deg[b]++;
+        ++kept;
+    }
+    row.assign(n + 1, 0);
+    for (int x = 0; x < n; ++x) row[x + 1] = row[x] + deg[x];
+    i64 arcs = row[n];
+    col.resize(arcs);
+    cap.resize(arcs);
+    rev.resize(arcs);
+    fwd.resize(arcs);
+    for (int x = 0; x < n; ++x) deg[x] = row[x];
+    for (i64 i = 0; i < m; ++i) {
+        int a = u[i], b = v[i];
+        if (a < 0 || a >= n || b < 0 || b >= n || a == b || c[i] <= 0) continue;
+        int ea = deg[a]++, eb = deg[b]++;
+        col[ea] = b;
+        cap[ea] = c[i];
+        rev[ea] = eb;
+        fwd[ea] = 1;
+        col[eb] = a;
+        cap[eb] = 0;
+        rev[eb] = ea;
+        fwd[eb] = 0;
+    }
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+void mf_opts_default(mf_opts *o) {
+    memset(o, 0, sizeof(*o));
+    o->kernel_cycles = 0;
+    o->gr_freq = 128;        // GR_FREQ0 (RA:1466)
+    o->gr_work_alpha = 2.0;  // also relabel after ~2 passes over the kept arcs
+    o->prune_mode = 1;
+    o->path_push_switch = 8;  // PATH_PUSH_SWITCH (RA:1480)
+    o->max_path_len = 256;    // MAX_PATH_LENGTH (RA:1481)
+    o->use_path_push = 1;
+    o->use_hot_sweep = 1;
+    o->hot_regions = 32;  // RA:1936
+    o->use_rm = 1;
+    o->rm_freq = 64;   // RM_FREQ0 (RA:1468)
+    o->h_cut = 100;    // H_cut (RA:1470)
+    o->stagnate_rounds = 128;  // STAGNATE_ROUNDS (RA:1472)
+    o->iter_max = 20000000;    // ITER_MAX (RA:1476)
+    o->group_ctas = 0;
+    o->threads = 512;
+    o->certify = 0;
+    o->verbose = 0;
+}
+
+const char *mf_last_error_string(void) { return g_err.c_str(); }
+const char *mf_version(void) { return "mscresearch_b200 maxflow 0.1 (sm_100a)"; }
+
+int mf_graph_create_from_edges(int n, long long m, const int32_t *u, const int32_t *v,
+                               const int64_t *cap, int R, mf_graph **out) {
+    if (!out) return fail(MF_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (n <= 0) return fail(MF_ERR_ARG, "n must be positive (got %d)", n);
+    if (m < 0 || (m > 0 && (!u || !v || !cap))) return fail(MF_ERR_ARG, "bad edge arrays");
+    if (2 * m > 0x7fffffffLL) return fail(MF_ERR_ARG, "too many edges for int32 arc ids");
+    if (R <= 0) R = 128;
+    R = std::min(std::min(R, n), 1024);
+    std::vector<int> row, col, rev;
+    std::vector<i64> cp;
+    std::vector<unsigned char> fwd;
+    host_csr(n, m, u, v, cap, row, col, cp, rev, fwd);
+    mf_graph *g = new mf_graph();
+    g->n = n;
+    g->arcs = row[n];
+    g->avg_deg = (int)(g->arcs / n);
+    cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete g;
+        return fail(MF_ERR_CUDA, "no CUDA device usable: %s", cudaGetErrorString(e));
+    }
+    cudaEventCreate(&g->ev0);
+    cudaEventCreate(&g->ev1);
+    int *drow = nullptr, *dcol = nullptr, *drev = nullptr;
+    i64 *dcap = nullptr;
+    unsigned char *dfwd = nullptr;
+    size_t A = (size_t)std::max<i64>(g->arcs, 1);
+    int rc = MF_OK;
+    do {
+        if (cudaMalloc(&drow, sizeof(int) * ((size_t)n + 1)) || cudaMalloc(&dcol, sizeof(int) * A) ||
+            cudaMalloc(&drev, sizeof(int) * A) || cudaMalloc(&dcap, sizeof(i64) * A) ||
+            cudaMalloc(&dfwd, A)) {
+            rc = fail(MF_ERR_NOMEM, "graph upload allocation failed");
+            break;
+        }
+        cudaMemcpy(drow, row.data(), sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice);
+        if (g->arcs) {
+            cudaMemcpy(dcol, col.data(), sizeof(int) * g->arcs, cudaMemcpyHostToDevice);
+            cudaMemcpy(drev, rev.data(), sizeof(int) * g->arcs, cudaMemcpyHostToDevice);
+            cudaMemcpy(dcap, cp.data(), sizeof(i64) * g->arcs, cudaMemcpyHostToDevice);
+            cudaMemcpy(dfwd, fwd.data(), g->arcs, cudaMemcpyHostToDevice);
+        }
+        std::vector<int> ident(n);
+        for (int i = 0; i < n; ++i) ident[i] = i;
+        rc = partition_into(g, R, drow, dcol, dcap, drev, dfwd, ident);
+    } while (0);
+    cudaFree(drow);
+    cudaFree(dcol);
+    cudaFree(drev);
+    cudaFree(dcap);
+    cudaFree(dfwd);
+    if (rc != MF_OK) {
+        mf_graph_destroy(g);
+        return rc;
+    }
+    g->pool.n = n;
+    g->pool.arcs = g->arcs;
+    *out = g;
+    return MF_OK;
+}
+
+int mf_graph_repartition(mf_graph *g, int R) {
+    if (!g) return fail(MF_ERR_ARG, "graph is NULL");
+    if (R <= 0) R = 128;
+    R = std::min(std::min(R, g->n), 1024);
+    if (R == g->R) return MF_OK;
+    // current region-ordered arrays become the input; their vertex i is
+    // caller vertex old_id[i]
+    int *row = g->row, *col = g->col, *rev = g->rev;
+    i64 *cap = g->cap;
+    unsigned char *fwd = g->fwd;
+    int *ro = g->region_of, *rs = g->region_start;
+    DGraph *dg = g->d_graph;
+    g->row = g->col = g->rev = g->region_of = g->region_start = nullptr;
+    g->cap = nullptr;
+    g->fwd = nullptr;
+    g->d_graph = nullptr;
+    std::vector<int> in_to_caller = g->old_id;
+    int rc = partition_into(g, R, row, col, cap, rev, fwd, in_to_caller);
+    cudaFree(row);
+    cudaFree(col);
+    cudaFree(rev);
+    cudaFree(cap);
+    cudaFree(fwd);
+    cudaFree(ro);
+    cudaFree(rs);
+    cudaFree(dg);
+    return rc;
+}
+
+int mf_graph_destroy(mf_graph *g) {
+    if (!g) return MF_OK;
+    free_graph_arrays(g);
+    g->pool.release();
+    cudaFree(g->d_err);
+    cudaFree(g->d_clocks);
+    cudaFree(g->d_out);
+    cudaFree(g->d_q);
+    cudaFreeHost(g->h_pin);
+    cudaFreeHost(g->h_out);
+    if (g->ev0) cudaEventDestroy(g->ev0);
+    if (g->ev1) cudaEventDestroy(g->ev1);
+    if (g->stream) cudaStreamDestroy(g->stream);
+    delete g;
+    return MF_OK;
+}
+
+int mf_graph_info(const mf_graph *g, int *n, long long *arcs, int *R) {
+    if (!g) return fail(MF_ERR_ARG, "graph is NULL");
+    if (n) *n = g->n;
+    if (arcs) *arcs = g->arcs;
+    if (R) *R = g->R;
+    return MF_OK;
+}
+
+int mf_graph_export(const mf_graph *g, int32_t *row, int32_t *col, int64_t *cap, int32_t *rev,
+                    int32_t *new_id, int32_t *region_start, double *score, int32_t *part) {
+    if (!g) return fail(MF_ERR_ARG, "graph is NULL");
+    if (row) CK(cudaMemcpy(row, g->row, sizeof(int) * ((size_t)g->n + 1), cudaMemcpyDeviceToHost));
+    if (col && g->arcs) CK(cudaMemcpy(col, g->col, sizeof(int) * g->arcs, cudaMemcpyDeviceToHost));
+    if (cap && g->arcs) CK(cudaMemcpy(cap, g->cap, sizeof(i64) * g->arcs, cudaMemcpyDeviceToHost));
+    if (rev && g->arcs) CK(cudaMemcpy(rev, g->rev, sizeof(int) * g->arcs, cudaMemcpyDeviceToHost));
+    if (region_start)
+        CK(cudaMemcpy(region_start, g->region_start, sizeof(int) * ((size_t)g->R + 1), cudaMemcpyDeviceToHost));
+    if (new_id) memcpy(new_id, g->new_id.data(), sizeof(int) * g->n);
+    if (score) memcpy(score, g->score_caller.data(), sizeof(double) * g->n);
+    if (part) memcpy(part, g->part_caller.data(), sizeof(int) * g->n);
+    return MF_OK;
+}
+
+static int solve_common(mf_graph *g, int nq, const int32_t *s, const int32_t *t, const mf_opts *opts,
+                        int64_t *flows, mf_stats *stats, int mode, void *dbg, bool single) {
+    if (!g) return fail(MF_ERR_ARG, "graph is NULL");
+    if (nq < 0 || (nq > 0 && (!s || !t || !flows))) return fail(MF_ERR_ARG, "bad query arrays");
+    if (nq == 0) return MF_OK;
+    mf_opts o;
+    if (opts) o = *opts;
+    else mf_opts_default(&o);
+    std::vector<int> si(nq), ti(nq);
+    for (int i = 0; i < nq; ++i) to_internal(g, s[i], t[i], si[i], ti[i]);
+    std::vector<QOut> outs(nq);
+    int G = single ? 0 : (o.group_ctas > 0 ? o.group_ctas : 2);
+    int rc = launch(g, g->pool, nq, si.data(), ti.data(), false, o, mode, dbg, nullptr, 0, G, outs.data());
+    if (rc) return rc;
+    int worst = MF_OK;
+    for (int i = 0; i < nq; ++i) {
+        flows[i] = outs[i].flow;
+        if (stats) fill_stats(&stats[i], outs[i], single ? g->last_ms : 0.0);
+        int st = status_from_err(outs[i].status);
+        if (st != MF_OK && worst == MF_OK) worst = st;
+        if (o.verbose)
+            fprintf(stderr, "[mf] q=%d s=%d t=%d flow=%lld kept=%d rounds=%lld relabels=%lld status=%d\n",
+                    i, s[i], t[i], (long long)outs[i].flow, outs[i].mask_n, (long long)outs[i].rounds,
+                    (long long)outs[i].relabels, outs[i].status);
+    }
+    if (worst != MF_OK) return fail(worst, "a query ended with status %d", worst);
+    return MF_OK;
+}
+
+int mf_solve(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, int64_t *flow, mf_stats *stats) {
+    int64_t f = 0;
+    int rc = solve_common(g, 1, &s, &t, opts, &f, stats, KM_SOLVE, nullptr, true);
+    if (flow) *flow = f;
+    return rc;
+}
+
+int mf_solve_batch(mf_graph *g, int nq, const int32_t *s, const int32_t *t, const mf_opts *opts,
+                   int64_t *flows, mf_stats *stats) {
+    return solve_common(g, nq, s, t, opts, flows, stats, KM_SOLVE, nullptr, false);
+}
+
+double mf_last_device_ms(const mf_graph *g) { return g ? g->last_ms : 0.0; }
+
+int mf_debug_prune_mask(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, uint8_t *mask, int *kept) {
+    if (!g || !mask) return fail(MF_ERR_ARG, "bad arguments");
+    unsigned char *d = nullptr;
+    CK(cudaMalloc(&d, g->n));
+    CK(cudaMemset(d, 0, g->n));
+    int64_t f = 0;
+    mf_stats st;
+    int rc = solve_common(g, 1, &s, &t, opts, &f, &st, KM_PRUNE, d, true);
+    if (rc == MF_OK) {
+        std::vector<unsigned char> h(g->n);
+        cudaMemcpy(h.data(), d, g->n, cudaMemcpyDeviceToHost);
+        int k = 0;
+        for (int x = 0; x < g->n; ++x) {
+            mask[x] = (s < 0 || t < 0 || s >= g->n || t >= g->n) ? 0 : h[g->new_id[x]];
+            k += mask[x];
+        }
+        if (kept) *kept = k;
+    }
+    cudaFree(d);
+    return rc;
+}
+
+int mf_debug_initial_heights(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, int32_t *heights) {
+    if (!g || !heights) return fail(MF_ERR_ARG, "bad arguments");
+    int *d = nullptr;
+    CK(cudaMalloc(&d, sizeof(int) * g->n));
+    int64_t f = 0;
+    mf_stats st;
+    int rc = solve_common(g, 1, &s, &t, opts, &f, &st, KM_HEIGHTS, d, true);
+    if (rc == MF_OK) {
+        std::vector<int> h(g->n);
+        cudaMemcpy(h.data(), d, sizeof(int) * g->n, cudaMemcpyDeviceToHost);
+        for (int x = 0; x < g->n; ++x) heights[x] = h[g->new_id[x]];
+    }
+    cudaFree(d);
+    return rc;
+}
+
+int mf_solve_residual(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, int64_t *flow,
+                      int64_t *res, mf_stats *stats) {
+    if (!g || !res) return fail(MF_ERR_ARG, "bad arguments");
+    i64 *d = nullptr;
+    CK(cudaMalloc(&d, sizeof(i64) * (size_t)std::max<i64>(g->arcs, 1)));
+    int64_t f = 0;
+    mf_stats st;
+    int rc = solve_common(g, 1, &s, &t, opts, &f, stats ? stats : &st, KM_RESIDUAL, d, true);
+    if (rc == MF_OK && g->arcs) cudaMemcpy(res, d, sizeof(i64) * g->arcs, cudaMemcpyDeviceToHost);
+    if (flow) *flow = f;
+    cudaFree(d);
+    return rc;
+}
+
+int mf_certify(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, int64_t *flow, mf_stats *stats) {
+    int64_t f = 0;
+    mf_stats st;
+    int rc = solve_common(g, 1, &s, &t, opts, &f, stats ? stats : &st, KM_CERTIFY, nullptr, true);
+    if (flow) *flow = f;
+    return rc;
+}
+
+// ---- capacity updates ------------------------------------------------------
+
+static int resolve_updates(mf_graph *g, int nb, const int32_t *u, const int32_t *v,
+                           const int64_t *delta, std::vector<ArcUpdate> &ups, int *skipped) {
+    std::vector<int> ui(nb), vi(nb);
+    for (int i = 0; i < nb; ++i) {
+        bool ok = u[i] >= 0 && u[i] < g->n && v[i] >= 0 && v[i] < g->n && u[i] != v[i];
+        ui[i] = ok ? g->new_id[u[i]] : -1;
+        vi[i] = ok ? g->new_id[v[i]] : -1;
+    }
+    int *du = nullptr, *dv = nullptr, *darc = nullptr;
+    i64 *dcap = nullptr;
+    CK(cudaMalloc(&du, sizeof(int) * nb));
+    CK(cudaMalloc(&dv, sizeof(int) * nb));
+    CK(cudaMalloc(&darc, sizeof(int) * nb));
+    CK(cudaMalloc(&dcap, sizeof(i64) * nb));
+    CK(cudaMemcpy(du, ui.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dv, vi.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
+    k_find_arcs<<<(nb + 255) / 256, 256, 0, g->stream>>>(nb, du, dv, g->row, g->col, g->fwd, g->cap, darc, dcap);
+    std::vector<int> arc(nb);
+    std::vector<i64> capv(nb);
+    CK(cudaMemcpyAsync(arc.data(), darc, sizeof(int) * nb, cudaMemcpyDeviceToHost, g->stream));
+    CK(cudaMemcpyAsync(capv.data(), dcap, sizeof(i64) * nb, cudaMemcpyDeviceToHost, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    cudaFree(du);
+    cudaFree(dv);
+    cudaFree(darc);
+    cudaFree(dcap);
+    // apply sequentially (clamp at 0 after each change), one entry per arc
+    std::unordered_map<int, int> at;
+    int skip = 0;
+    for (int i = 0; i < nb; ++i) {
+        if (arc[i] < 0) {
+            ++skip;
+            continue;
+        }
+        auto it = at.find(arc[i]);
+        if (it == at.end()) {
+            ArcUpdate a;
+            a.arc = arc[i];
+            a.pad = 0;
+            a.old_cap = capv[i];
+            a.new_cap = capv[i];
+            at[arc[i]] = (int)ups.size();
+            ups.push_back(a);
+            it = at.find(arc[i]);
+        }
+        ArcUpdate &a = ups[it->second];
+        a.new_cap = std::max<i64>(0, a.new_cap + delta[i]);
+    }
+    if (skipped) *skipped = skip;
+    return MF_OK;
+}
+
+static int apply_updates(mf_graph *g, const std::vector<ArcUpdate> &ups, ArcUpdate **d_out) {
+    *d_out = nullptr;
+    if (ups.empty()) return MF_OK;
+    ArcUpdate *d = nullptr;
+    CK(cudaMalloc(&d, sizeof(ArcUpdate) * ups.size()));
+    CK(cudaMemcpy(d, ups.data(), sizeof(ArcUpdate) * ups.size(), cudaMemcpyHostToDevice));
+    k_apply_caps<<<((int)ups.size() + 255) / 256, 256, 0, g->stream>>>((int)ups.size(), d, g->cap);
+    CK(cudaStreamSynchronize(g->stream));
+    *d_out = d;
+    return MF_OK;
+}
+
+int mf_update_caps(mf_graph *g, int nb, const int32_t *u, const int32_t *v, const int64_t *delta,
+                   int *skipped) {
+    if (!g) return fail(MF_ERR_ARG, "graph is NULL");
+    if (nb <= 0) return MF_OK;
+    if (!u || !v || !delta) return fail(MF_ERR_ARG, "bad update arrays");
+    std::vector<ArcUpdate> ups;
+    int rc = resolve_updates(g, nb, u, v, delta, ups, skipped);
+    if (rc) return rc;
+    ArcUpdate *d = nullptr;
+    rc = apply_updates(g, ups, &d);
+    cudaFree(d);
+    return rc;
+}
+
+// ---- sessions ----------------------------------------------------------------
+
+int mf_session_create(mf_graph *g, int nq, const int32_t *s, const int32_t *t, const mf_opts *opts,
+                      mf_session **out) {
+    if (!g || !out || nq <= 0 || !s || !t) return fail(MF_ERR_ARG, "bad arguments");
+    mf_session *ss = new mf_session();
+    ss->g = g;
+    ss->nq = nq;
+    ss->s.resize(nq);
+    ss->t.resize(nq);
+    for (int i = 0; i < nq; ++i) to_internal(g, s[i], t[i], ss->s[i], ss->t[i]);
+    if (opts) ss->opts = *opts;
+    else mf_opts_default(&ss->opts);
+    ss->pool.n = g->n;
+    ss->pool.arcs = g->arcs;
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    if ((double)slot_bytes(g->n, g->arcs) * nq > 0.9 * (double)fr) {
+        delete ss;
+        return fail(MF_ERR_NOMEM, "admission: %d resident queries need %.1f GB, %.1f GB free", nq,
+                    slot_bytes(g->n, g->arcs) * (double)nq / 1e9, fr / 1e9);
+    }
+    int rc = ss->pool.grow(nq);
+    if (rc) {
+        ss->pool.release();
+        delete ss;
+        return rc;
+    }
+    *out = ss;
+    return MF_OK;
+}
+
+static int session_run(mf_session *ss, int mode, const ArcUpdate *d_upd, int nupd, int64_t *flows,
+                       mf_stats *stats) {
+    mf_graph *g = ss->g;
+    std::vector<QOut> outs(ss->nq);
+    int G = ss->opts.group_ctas > 0 ? ss->opts.group_ctas : 2;
+    int rc = launch(g, ss->pool, ss->nq, ss->s.data(), ss->t.data(), true, ss->opts, mode, nullptr,
+                    d_upd, nupd, G, outs.data());
+    if (rc) return rc;
+    int worst = MF_OK;
+    for (int i = 0; i < ss->nq; ++i) {
+        if (flows) flows[i] = outs[i].flow;
+        if (stats) fill_stats(&stats[i], outs[i], 0.0);
+        int st = status_from_err(outs[i].status);
+        if (st != MF_OK && worst == MF_OK) worst = st;
+    }
+    if (worst != MF_OK) return fail(worst, "a resident query ended with status %d", worst);
+    return MF_OK;
+}
+
+int mf_session_solve(mf_session *ss, int64_t *flows, mf_stats *stats) {
+    if (!ss) return fail(MF_ERR_ARG, "session is NULL");
+    int rc = session_run(ss, KM_SOLVE, nullptr, 0, flows, stats);
+    if (rc == MF_OK) ss->solved = true;
+    return rc;
+}
+
+int mf_session_update(mf_session *ss, int nb, const int32_t *u, const int32_t *v, const int64_t *delta,
+                      int64_t *flows, mf_stats *stats) {
+    if (!ss) return fail(MF_ERR_ARG, "session is NULL");
+    if (!ss->solved) {
+        int rc = mf_update_caps(ss->g, nb, u, v, delta, nullptr);
+        if (rc) return rc;
+        return mf_session_solve(ss, flows, stats);
+    }
+    std::vector<ArcUpdate> ups;
+    int rc = MF_OK;
+    if (nb > 0) {
+        if (!u || !v || !delta) return fail(MF_ERR_ARG, "bad update arrays");
+        rc = resolve_updates(ss->g, nb, u, v, delta, ups, nullptr);
+        if (rc) return rc;
+    }
+    ArcUpdate *d = nullptr;
+    rc = apply_updates(ss->g, ups, &d);
+    if (rc) return rc;
+    rc = session_run(ss, KM_REPAIR, d, (int)ups.size(), flows, stats);
+    cudaFree(d);
+    return rc;
+}
+
+int mf_session_destroy(mf_session *ss) {
+    if (!ss) return MF_OK;
+    ss->pool.release();
+    delete ss;
+    return MF_OK;
+}
+
+}  // extern "C"
+
+// ---- continuous-batching server ---------------------------------------------
+
+struct mf_server {
+    std::vector<mf_graph *> graphs;
+    DGraph *d_graphs = nullptr;
+    SlotPool pool;
+    mf_opts opts;
+    KOpts ko;
+    int G = 2;
+    int nslots = 0;
+    int threads = 512;
+    int cap = 0;  // ring capacity (requests)
+    // mapped pinned host memory
+    int *h_tail = nullptr, *h_stop = nullptr, *h_done = nullptr;
+    int4 *h_req = nullptr;
+    u64 *h_t0 = nullptr;
+    QOut *h_out = nullptr;
+    int *d_qnext = nullptr, *d_err = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done_ev = nullptr;
+    bool running = false;
+    long long submitted = 0;
+};
+
+static int server_launch(mf_server *sv) {
+    // resume after the last claimed request
+    long long first = 0;
+    while (first < sv->submitted && sv->h_done[first] != 0) ++first;
+    int q0 = (int)first;
+    CK(cudaMemcpyAsync(sv->d_qnext, &q0, sizeof(int), cudaMemcpyHostToDevice, sv->stream));
+    CK(cudaMemsetAsync(sv->d_err, 0, sizeof(int), sv->stream));
+    int ns = (int)sv->pool.host.size();
+    unsigned *clk = nullptr;
+    CK(cudaMalloc(&clk, sizeof(unsigned) * ns));
+    k_prepare_slots<<<(ns + 127) / 128, 128, 0, sv->stream>>>(sv->pool.dev, ns, clk);
+    CK(cudaStreamSynchronize(sv->stream));
+    cudaFree(clk);
+    *(volatile int *)sv->h_stop = 0;
+    KParams p{};
+    p.graphs = sv->d_graphs;
+    p.slots = sv->pool.dev;
+    p.G = sv->G;
+    p.nq = sv->cap;
+    p.q_next = sv->d_qnext;
+    int *dtail = nullptr, *dstop = nullptr, *ddone = nullptr;
+    int4 *dreq = nullptr;
+    u64 *dt0 = nullptr;
+    QOut *dout = nullptr;
+    CK(cudaHostGetDevicePointer((void **)&dtail, sv->h_tail, 0));
+    CK(cudaHostGetDevicePointer((void **)&dstop, sv->h_stop, 0));
+    CK(cudaHostGetDevicePointer((void **)&ddone, sv->h_done, 0));
+    CK(cudaHostGetDevicePointer((void **)&dreq, sv->h_req, 0));
+    CK(cudaHostGetDevicePointer((void **)&dt0, sv->h_t0, 0));
+    CK(cudaHostGetDevicePointer((void **)&dout, sv->h_out, 0));
+    p.out = dout;
+    p.err = sv->d_err;
+    p.bar_limit_ns = 20ull * 1000 * 1000 * 1000;
+    p.o = sv->ko;
+    p.mode = KM_SOLVE;
+    p.ring_tail = dtail;
+    p.ring_req = dreq;
+    p.ring_done = ddone;
+    p.ring_t0 = dt0;
+    p.ring_stop = dstop;
+    p.idle_limit_ns = 300ull * 1000 * 1000;  // groups idle this long end the launch
+    cudaError_t le = cudaSuccess;
+    mf_launch_kernel(p, sv->nslots * sv->G, sv->threads, sv->stream, sv->G > 1, &le);
+    if (le != cudaSuccess) return fail(MF_ERR_CUDA, "server launch: %s", cudaGetErrorString(le));
+    CK(cudaEventRecord(sv->done_ev, sv->stream));
+    sv->running = true;
+    return MF_OK;
+}
+
+static bool server_alive(mf_server *sv) {
+    if (!sv->running) return false;
+    cudaError_t q = cudaEventQuery(sv->done_ev);
+    if (q == cudaErrorNotReady) return true;
+    sv->running = false;
+    return false;
+}
+
+extern "C" {
+
+int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int max_slots,
+                     mf_server **out) {
+    if (!graphs || ngraphs <= 0 || !out) return fail(MF_ERR_ARG, "bad arguments");
+    *out = nullptr;
+    mf_server *sv = new mf_server();
+    if (opts) sv->opts = *opts;
+    else mf_opts_default(&sv->opts);
+    int nmax = 0;
+    i64 amax = 0, arcs_sum = 0, n_sum = 0;
+    std::vector<DGraph> dg(ngraphs);
+    for (int i = 0; i < ngraphs; ++i) {
+        mf_graph *g = graphs[i];
+        if (!g) {
+            delete sv;
+            return fail(MF_ERR_ARG, "graph %d is NULL", i);
+        }
+        sv->graphs.push_back(g);
+        nmax = std::max(nmax, g->n);
+        amax = std::max(amax, g->arcs);
+        arcs_sum += g->arcs;
+        n_sum += g->n;
+        dg[i] = DGraph{g->n, g->R, g->arcs, g->row, g->col, g->rev, g->cap, g->region_of};
+    }
+    sv->ko = resolve_opts(sv->opts, (int)(arcs_sum / std::max<i64>(1, n_sum)));
+    DevInfo di;
+    sv->threads = sv->opts.threads > 0 ? sv->opts.threads : 512;
+    int rc = dev_info(di, sv->threads);
+    if (rc) {
+        delete sv;
+        return rc;
+    }
+    sv->G = sv->opts.group_ctas > 0 ? sv->opts.group_ctas : 2;
+    int groups = std::max(1, di.sms * di.bps / sv->G);
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    size_t per = slot_bytes(nmax, amax);
+    int fit = (int)((fr * 0.85) / (double)per);
+    int ns = std::min(groups, fit);
+    if (max_slots > 0) ns = std::min(ns, max_slots);
+    if (ns < 1) {
+        delete sv;
+        return fail(MF_ERR_NOMEM, "admission: no HBM for one residual slot (%zu bytes)", per);
+    }
+    sv->nslots = ns;
+    sv->pool.n = nmax;
+    sv->pool.arcs = amax;
+    rc = sv->pool.grow(ns);
+    if (rc) {
+        sv->pool.release();
+        delete sv;
+        return rc;
+    }
+    if (cudaMalloc(&sv->d_graphs, sizeof(DGraph) * ngraphs) != cudaSuccess ||
+        cudaMemcpy(sv->d_graphs, dg.data(), sizeof(DGraph) * ngraphs, cudaMemcpyHostToDevice) != cudaSuccess) {
+        sv->pool.release();
+        delete sv;
+        return fail(MF_ERR_NOMEM, "server graph table");
+    }
+    sv->cap = 1 << 20;
+    bool ok = cudaHostAlloc(&sv->h_tail, sizeof(int) * 2, cudaHostAllocMapped) == cudaSuccess &&
+              cudaHostAlloc(&sv->h_done, sizeof(int) * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
+              cudaHostAlloc(&sv->h_req, sizeof(int4) * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
+              cudaHostAlloc(&sv->h_t0, sizeof(u64) * 2 * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
+              cudaHostAlloc(&sv->h_out, sizeof(QOut) * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
+              cudaMalloc(&sv->d_qnext, sizeof(int) * 2) == cudaSuccess;
+    if (!ok) {
+        mf_server_destroy(sv);
+        return fail(MF_ERR_NOMEM, "server ring allocation failed");
+    }
+    sv->h_stop = sv->h_tail + 1;
+    sv->d_err = sv->d_qnext + 1;
+    memset(sv->h_tail, 0, sizeof(int) * 2);
+    memset(sv->h_done, 0, sizeof(int) * sv->cap);
+    cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&sv->done_ev, cudaEventDisableTiming);
+    *out = sv;
+    return MF_OK;
+}
+
+int mf_server_slots(const mf_server *sv, int *slots) {
+    if (!sv || !slots) return fail(MF_ERR_ARG, "bad arguments");
+    *slots = sv->nslots;
+    return MF_OK;
+}
+
+int mf_server_submit(mf_server *sv, int graph, int32_t s, int32_t t, long long *ticket) {
+    if (!sv) return fail(MF_ERR_ARG, "server is NULL");
+    if (graph < 0 || graph >= (int)sv->graphs.size()) return fail(MF_ERR_ARG, "graph index %d", graph);
+    if (sv->submitted >= sv->cap) return fail(MF_ERR_NOMEM, "server ring full (%d requests)", sv->cap);
+    mf_graph *g = sv->graphs[graph];
+    int si = -1, ti = -1;
+    to_internal(g, s, t, si, ti);
+    long long k = sv->submitted;
+    sv->h_req[k] = make_int4(si, ti, graph, 0);
+    sv->h_done[k] = 0;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    sv->submitted = k + 1;
+    *(volatile int *)sv->h_tail = (int)sv->submitted;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    if (ticket) *ticket = k;
+    if (!server_alive(sv)) {
+        int rc = server_launch(sv);
+        if (rc) return rc;
+    }
+    return MF_OK;
+}
+
+int mf_server_poll(mf_server *sv, long long ticket, int *done, int64_t *flow, double *latency_ms,
+                   int *status) {
+    if (!sv || ticket < 0 || ticket >= sv->submitted) return fail(MF_ERR_ARG, "bad ticket");
+    int d = *(volatile int *)&sv->h_done[ticket];
+    if (d != 1) {
+        if (!server_alive(sv)) {
+            int herr = 0;
+            cudaMemcpy(&herr, sv->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+            if (herr) return fail(status_from_err(herr), "server kernel aborted (status %d)", herr);
+            int rc = server_launch(sv);
+            if (rc) return rc;
+        }
+        if (done) *done = 0;
+        return MF_OK;
+    }
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    const QOut &q = sv->h_out[ticket];
+    if (done) *done = 1;
+    if (flow) *flow = q.flow;
+    if (status) *status = status_from_err(q.status);
+    if (latency_ms) {
+        volatile u64 *t0 = sv->h_t0;
+        *latency_ms = (double)(t0[2 * ticket + 1] - t0[2 * ticket]) * 1e-6;
+    }
+    return MF_OK;
+}
+
+int mf_server_drain(mf_server *sv) {
+    if (!sv) return fail(MF_ERR_ARG, "server is NULL");
+    for (long long k = 0; k < sv->submitted; ++k) {
+        for (;;) {
+            int done = 0;
+            int rc = mf_server_poll(sv, k, &done, nullptr, nullptr, nullptr);
+            if (rc) return rc;
+            if (done) break;
+            std::this_thread::sleep_for(std::chrono::microseconds(20));
+        }
+    }
+    return MF_OK;
+}
+
+int mf_server_destroy(mf_server *sv) {
+    if (!sv) return MF_OK;
+    if (sv->h_stop) *(volatile int *)sv->h_stop = 1;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    if (sv->stream) cudaStreamSynchronize(sv->stream);
+    sv->pool.release();
+    cudaFree(sv->d_graphs);
+    cudaFree(sv->d_qnext);
+    cudaFreeHost(sv->h_tail);
+    cudaFreeHost(sv->h_done);
+    cudaFreeHost(sv->h_req);
+    cudaFreeHost(sv->h_t0);
+    cudaFreeHost(sv->h_out);
+    if (sv->done_ev) cudaEventDestroy(sv->done_ev);
+    if (sv->stream) cudaStreamDestroy(sv->stream);
+    delete sv;
+    return MF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,189 @@
+// maxflow_b200 — drop-in CLI for the reference program
+// (Region_Aware_PR_with_Pruning_BoundaryCore.cu main, RA:2561-2933):
+//
+//   maxflow_b200 <input_dir> <output_dir> [static|dynamic] [--batch] [--R N]
+//
+// Reads <input_dir>/graph.txt and test.txt (1-based ids), writes
+// <output_dir>/res_mt.txt (static) or res_dynamic.txt (dynamic), one
+// "flow time_ms" line per query in input order; invalid queries or s == t
+// give "0 0" (RA:2659-2663).  Diagnostics go to stderr.
+//   static   one plain whole-GPU solve per query (time_ms = that solve's
+//            wall time, prune included, as in RA:2808).
+//   --batch  all queries in one batched launch; time_ms = launch wall time
+//            divided evenly over the queries.
+//   dynamic  queries in windows of 10 (RA:2852), each window a resident
+//            session whose residual state stays on the GPU.
+#include <sys/stat.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/maxflow_b200.h"
+
+static double now_ms() {
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+int main(int argc, char **argv) {
+    if (argc < 3) {
+        fprintf(stderr, "Usage: %s <input_dir> <output_dir> [mode] [--batch] [--R N]\n", argv[0]);
+        fprintf(stderr, "  mode = static (default) | dynamic\n");
+        return 1;
+    }
+    std::string in = argv[1], outd = argv[2], mode = "static";
+    bool batch = false;
+    int R = 128;  // RA:2583
+    for (int i = 3; i < argc; ++i) {
+        if (!strcmp(argv[i], "--batch")) batch = true;
+        else if (!strcmp(argv[i], "--R") && i + 1 < argc) R = atoi(argv[++i]);
+        else mode = argv[i];
+    }
+    if (mode != "static" && mode != "dynamic") {
+        fprintf(stderr, "Unknown mode: %s (use static or dynamic)\n", mode.c_str());
+        return 1;
+    }
+    mkdir(outd.c_str(), 0755);
+    mf_graph *g = nullptr;
+    double t0 = now_ms();
+    int rc = mf_graph_load_file((in + "/graph.txt").c_str(), R, &g);
+    if (rc != MF_OK) {
+        fprintf(stderr, "Cannot load %s/graph.txt: %s\n", in.c_str(), mf_last_error_string());
+        return 1;
+    }
+    int n = 0, Rg = 0;
+    long long arcs = 0;
+    mf_graph_info(g, &n, &arcs, &Rg);
+    FILE *tf = fopen((in + "/test.txt").c_str(), "r");
+    if (!tf) {
+        fprintf(stderr, "Cannot open %s/test.txt\n", in.c_str());
+        mf_graph_destroy(g);
+        return 1;
+    }
+    std::vector<int32_t> qs, qt;
+    int a, b;
+    while (fscanf(tf, "%d %d", &a, &b) == 2) {
+        int s = a - 1, t = b - 1;
+        if (s >= 0 && s < n && t >= 0 && t < n) {
+            qs.push_back(s);
+            qt.push_back(t);
+        } else {
+            qs.push_back(-1);
+            qt.push_back(-1);
+        }
+    }
+    fclose(tf);
+    fprintf(stderr, "Graph (reordered by Region): n=%d, m=%lld, Regions=%d, Queries=%zu (load %.0f ms)\n",
+            n, arcs, Rg, qs.size(), now_ms() - t0);
+    const size_t Q = qs.size();
+    std::vector<long long> flows(Q, 0), times(Q, 0);
+    mf_opts o;
+    mf_opts_default(&o);
+    int status = 0;
+    if (mode == "static") {
+        if (batch && Q > 0) {
+            double b0 = now_ms();
+            std::vector<int64_t> f(Q);
+            rc = mf_solve_batch(g, (int)Q, qs.data(), qt.data(), &o, f.data(), nullptr);
+            double el = now_ms() - b0;
+            if (rc != MF_OK) {
+                fprintf(stderr, "batch solve failed: %s\n", mf_last_error_string());
+                status = 1;
+            }
+            for (size_t i = 0; i < Q; ++i) {
+                bool valid = qs[i] >= 0 && qs[i] != qt[i];
+                flows[i] = valid ? f[i] : 0;
+                times[i] = valid ? (long long)(el / Q) : 0;
+            }
+            fprintf(stderr, "[Batch] %zu queries in %.3f ms\n", Q, el);
+        } else {
+            for (size_t i = 0; i < Q; ++i) {
+                if (qs[i] < 0 || qs[i] == qt[i]) {
+                    fprintf(stderr, "[Static] Query %zu: Invalid.\n", i + 1);
+                    continue;
+                }
+                mf_stats st;
+                int64_t f = 0;
+                double q0 = now_ms();
+                rc = mf_solve(g, qs[i], qt[i], &o, &f, &st);
+                double el = now_ms() - q0;
+                if (rc != MF_OK) {
+                    fprintf(stderr, "query %zu failed: %s\n", i + 1, mf_last_error_string());
+                    status = 1;
+                }
+                flows[i] = f;
+                times[i] = (long long)el;
+                fprintf(stderr,
+                        "[Static] Query %zu: s=%d, t=%d kept_n=%d, kept_m=%lld, rounds=%lld, "
+                        "relabels=%lld, Flow=%lld, Time=%lld ms (device %.3f ms)\n",
+                        i + 1, qs[i] + 1, qt[i] + 1, st.mask_vertices, st.mask_arcs, st.rounds,
+                        st.global_relabels, (long long)f, times[i], st.time_ms);
+            }
+        }
+        std::string res = outd + "/res_mt.txt";
+        FILE *out = fopen(res.c_str(), "w");
+        if (!out) {
+            fprintf(stderr, "Cannot open output file %s\n", res.c_str());
+            mf_graph_destroy(g);
+            return 1;
+        }
+        long long total = 0;
+        for (size_t i = 0; i < Q; ++i) {
+            fprintf(out, "%lld %lld\n", flows[i], times[i]);
+            total += times[i];
+        }
+        fclose(out);
+        fprintf(stderr, "Total time: %lld ms\n", total);
+    } else {
+        std::string res = outd + "/res_dynamic.txt";
+        FILE *out = fopen(res.c_str(), "w");
+        if (!out) {
+            fprintf(stderr, "Cannot open dynamic output file %s\n", res.c_str());
+            mf_graph_destroy(g);
+            return 1;
+        }
+        const size_t WINDOW = 10;  // RA:2852
+        long long total = 0;
+        for (size_t q0 = 0; q0 < Q; q0 += WINDOW) {
+            size_t q1 = std::min(Q, q0 + WINDOW);
+            std::vector<int32_t> ws, wt;
+            std::vector<size_t> idx;
+            for (size_t i = q0; i < q1; ++i)
+                if (qs[i] >= 0 && qs[i] != qt[i]) {
+                    ws.push_back(qs[i]);
+                    wt.push_back(qt[i]);
+                    idx.push_back(i);
+                }
+            if (!ws.empty()) {
+                mf_session *ss = nullptr;
+                double w0 = now_ms();
+                rc = mf_session_create(g, (int)ws.size(), ws.data(), wt.data(), &o, &ss);
+                std::vector<int64_t> f(ws.size(), 0);
+                if (rc == MF_OK) rc = mf_session_solve(ss, f.data(), nullptr);
+                double el = now_ms() - w0;
+                if (rc != MF_OK) {
+                    fprintf(stderr, "window [%zu,%zu) failed: %s\n", q0, q1, mf_last_error_string());
+                    status = 1;
+                }
+                for (size_t k = 0; k < idx.size(); ++k) {
+                    flows[idx[k]] = f[k];
+                    times[idx[k]] = (long long)(el / idx.size());
+                }
+                mf_session_destroy(ss);
+            }
+            for (size_t i = q0; i < q1; ++i) {
+                fprintf(out, "%lld %lld\n", flows[i], times[i]);
+                total += times[i];
+            }
+        }
+        fclose(out);
+        fprintf(stderr, "Total time: %lld ms\n", total);
+    }
+    mf_graph_destroy(g);
+    return status;
+}

@@ -1,0 +1,1278 @@
+// Device solver: one persistent cooperative launch in which groups of CTAs
+// each take (s,t) queries from a work queue and solve them to an exact
+// maximum preflow (optionally a certified flow) in their own residual slot.
+//
+// Mapping to the reference (Region_Aware_PR_with_Pruning_BoundaryCore.cu,
+// "RA"):
+//   prune (fwd/bwd or fwd/undirected BFS) ... build_reachable_refined_from_st RA:1391-1445
+//   init + source preflow ................... staticMaxFlow_kernel_1 / _7   RA:151-200
+//   global relabel (frontier BFS from sink
+//     and deficit vertices, warp-ballot
+//     frontier compaction) .................. init_height_level_frontier + bfs_expand_frontier
+//                                             RA:203-233, 322-348, driver RA:1499-1581
+//   discharge (warp per active vertex,
+//     ballot/shuffle arc scan, multi-push
+//     with native 64-bit atomics) ........... staticMaxFlow_kernel_14_region RA:432-515
+//   active worklist + counts ................ build_active_list_and_count RA:664-695
+//   hot-region extra sweep .................. count_region_active_kernel + hot pass RA:283-318, 1899-1984
+//   sparse-phase path push .................. try_push_along_path / _with_path_push RA:773-955
+//   region-aware invalid-arc repair (RM) .... staticMaxFlow_kernel_17_region RA:605-657
+//   stagnation / adaptive K, GR frequency ... RA:1845-1891
+//   termination + read excess(t) ............ RA:1988, 2114, 2202-2204
+//
+// Exactness.  Every kernel keeps residuals non-negative and pairwise
+// conserved with atomic updates; only the owner of a vertex (one warp per
+// vertex per pass, ownership stamps for path push) lowers its excess.  RM is
+// the only step that creates negative excess (deficits), as in the
+// reference; deficits are relabel seeds, and if any remain when no active
+// vertex is left the solver drains them back from the sink (phase B) before
+// resuming.  A solve ends only when an exact global relabel finds no vertex
+// with positive excess that can reach the sink and no deficit: the preflow
+// is then maximum and excess(t) is the max-flow value.
+#include "mf_solver.cuh"
+
+#include <climits>
+
+// cnt[0..7]: list tails, handed out in rotation; taking bank k zeroes bank
+// k+4 (mod 8), which was last read at least one group barrier earlier (no
+// code path takes more than three banks between two barriers).
+#define NBANKS 8
+#define CNT_Q 8      // query handed to the group
+#define CNT_FLAG 9   // misc uniform flag
+#define CNT_RS 10    // serving: request source / sink / graph
+#define CNT_RT 11
+#define CNT_RG 12
+#define ACC_BANK 16  // i64 fields per accumulator bank
+#define ACC_TOT 64   // start of per-query totals (within acc, 64 i64 reserved for banks)
+
+// accumulator fields (per bank)
+#define A_SUMEX 0
+#define A_HIGH 1
+#define A_WORK 2
+#define A_PUSH 3
+#define A_HMIN 4
+#define A_HMAX 5
+#define A_FIXED 6
+#define A_NDEF 7
+#define A_VERTS 8
+#define A_CUT 9
+#define A_BAD 10
+
+// per-query totals
+#define T_ARCS 0
+#define T_VERTS 1
+#define T_PUSH 2
+#define T_MASKARCS 3
+
+enum Phase { PH_A = 0, PH_B = 1, PH_C = 2 };
+
+struct QCtx {
+    // group geometry
+    int G, crank, gw, gW, lane, wpc;
+    GroupBar *bar;
+    int *err;
+    u64 lim;
+    // graph
+    int n, R;
+    const int *row, *col, *rev, *rof;
+    const i64 *cap;
+    // slot
+    DSlot st;
+    // uniform control
+    unsigned clock;
+    int seq;   // list-bank sequence
+    int aseq;  // accumulator-bank sequence
+    bool leader;
+    u64 t_start;
+    u64 time_limit;
+    // per-warp counters (flushed at the end of the query)
+    i64 w_arcs, w_verts, w_push;
+
+    __device__ bool sync() { return gsync(G, bar, err, lim); }
+    // barrier that also returns the list tail cnt[bank] as of the barrier
+    __device__ bool sync_tail(int bank, int &tail) {
+        return gsync_snap(G, bar, err, lim, &st.cnt[bank], &tail);
+    }
+    __device__ int take_bank() {
+        int b = seq & (NBANKS - 1);
+        if (leader) st.cnt[(seq + 4) & (NBANKS - 1)] = 0;
+        ++seq;
+        return b;
+    }
+    __device__ i64 *take_abank() {
+        int b = aseq & 3;
+        if (leader) {
+            i64 *z = st.acc + ((aseq + 2) & 3) * ACC_BANK;
+            for (int i = 0; i < ACC_BANK; ++i) z[i] = 0;
+            z[A_HMIN] = INT_MAX;
+            z[A_HMAX] = -1;
+        }
+        ++aseq;
+        return st.acc + b * ACC_BANK;
+    }
+    __device__ void flush_warp_counts() {
+        if (lane == 0) {
+            i64 *tot = st.acc + ACC_TOT;
+            if (w_arcs) atomic_add_i64(&tot[T_ARCS], w_arcs);
+            if (w_verts) atomic_add_i64(&tot[T_VERTS], w_verts);
+            if (w_push) atomic_add_i64(&tot[T_PUSH], w_push);
+        }
+        w_arcs = w_verts = w_push = 0;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Level-synchronous frontier BFS over a growing queue Q[0..tail).  The
+// frontier at level L is Q[lo,hi); claimed vertices are appended with warp
+// ballot + prefix ranks (one atomicAdd per warp).  Functor cl(v, e, w) returns
+// true when arc e = v->w claims w (it performs the claim itself).
+template <class Claim>
+__device__ bool bfs_levels(QCtx &c, int *Q, int bank, int hi, Claim cl, int *levels_out) {
+    int lo = 0, level = 0;
+    while (lo < hi) {
+        for (int i = lo + c.gw; i < hi; i += c.gW) {
+            int v = ldcg(&Q[i]);
+            int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+            for (int base = b; base < e1; base += 32) {
+                int e = base + c.lane;
+                bool ok = false;
+                int w = 0;
+                if (e < e1) {
+                    w = ldro(&c.col[e]);
+                    ok = cl(v, e, w, level);
+                }
+                warp_append(ok, w, Q, &c.st.cnt[bank]);
+            }
+            if (c.lane == 0) {
+                c.w_arcs += e1 - b;
+                c.w_verts += 1;
+            }
+        }
+        int tail = 0;
+        if (!c.sync_tail(bank, tail)) return false;
+        lo = hi;
+        hi = tail;
+        ++level;
+    }
+    if (levels_out) *levels_out = level;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Prune.  Stamps: S (forward reach), M = S+1 (kept), U (undirected, mode 0).
+// Leaves the kept vertices in vlist[0..nv) and returns nv (0 if t is not
+// reachable from s, in which case the flow is 0).
+__device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, int &nv,
+                      bool &t_reach) {
+    // forward BFS from s over cap > 0
+    int bank = c.take_bank();
+    if (c.leader) {
+        c.st.mark[s] = S;
+        c.st.qa[0] = s;
+        c.st.cnt[bank] = 1;
+    }
+    if (!c.sync()) return false;
+    unsigned *mark = c.st.mark;
+    const i64 *cap = c.cap;
+    auto fwd = [&](int v, int e, int w, int) -> bool {
+        if (ldro(&cap[e]) <= 0) return false;
+        if (ldcg(&mark[w]) >= S) return false;
+        return atomicMax(&mark[w], S) < S;
+    };
+    if (!bfs_levels(c, c.st.qa, bank, 1, fwd, nullptr)) return false;
+    int nf = ldcg(&c.st.cnt[bank]);
+    t_reach = ldcg(&mark[t]) >= S;
+
+    int vb = c.take_bank();
+    if (mode == 1) {
+        if (!t_reach) {
+            nv = 0;
+            return true;
+        }
+        // backward BFS from t over arcs whose reverse (y->x) has capacity,
+        // restricted to forward-reached vertices
+        if (c.leader) {
+            mark[t] = M;
+            c.st.vlist[0] = t;
+            c.st.cnt[vb] = 1;
+        }
+        if (!c.sync()) return false;
+        const int *rev = c.rev;
+        auto bwd = [&](int v, int e, int w, int) -> bool {
+            if (ldcg(&mark[w]) != S) return false;
+            if (ldro(&cap[ldro(&rev[e])]) <= 0) return false;
+            return atomicCAS(&mark[w], S, M) == S;
+        };
+        if (!bfs_levels(c, c.st.vlist, vb, 1, bwd, nullptr)) return false;
+        nv = ldcg(&c.st.cnt[vb]);
+        return true;
+    }
+    // mode 0: undirected component of t (all arcs) with qmark stamp U = M
+    // (qmark stamps come from the same clock, so M is unused there), then
+    // kept = forward-reached & undirected-reached, plus s and t.
+    int ub = c.take_bank();
+    unsigned *qm = c.st.qmark;
+    if (c.leader) {
+        qm[t] = M;
+        c.st.qb[0] = t;
+        c.st.cnt[ub] = 1;
+    }
+    if (!c.sync()) return false;
+    auto und = [&](int v, int e, int w, int) -> bool {
+        if (ldcg(&qm[w]) >= M) return false;
+        return atomicMax(&qm[w], M) < M;
+    };
+    if (!bfs_levels(c, c.st.qb, ub, 1, und, nullptr)) return false;
+    // intersect: sweep the forward list (s is its first entry)
+    for (int base = c.gw * 32; base < nf; base += c.gW * 32) {
+        int i = base + c.lane;
+        bool keep = false;
+        int v = 0;
+        if (i < nf) {
+            v = ldcg(&c.st.qa[i]);
+            keep = (ldcg(&qm[v]) == M) || v == s;
+            if (keep) mark[v] = M;
+        }
+        warp_append(keep, v, c.st.vlist, &c.st.cnt[vb]);
+    }
+    if (!c.sync()) return false;
+    if (c.leader && !t_reach) {
+        // t is always kept (RA:1443-1444) even when s cannot reach it
+        int k = atomicAdd(&c.st.cnt[vb], 1);
+        c.st.vlist[k] = t;
+        mark[t] = M;
+    }
+    if (!c.sync()) return false;
+    nv = ldcg(&c.st.cnt[vb]);
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Fresh residual state over the kept vertices: excess 0; res[e] = cap[e]
+// when the head is kept, else 0 (the arc is outside the induced subgraph).
+__device__ bool init_state(QCtx &c, int nv, unsigned M) {
+    i64 mask_arcs = 0;
+    for (int i = c.gw; i < nv; i += c.gW) {
+        int v = ldcg(&c.st.vlist[i]);
+        int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+        if (c.lane == 0) {
+            c.st.ex[v] = 0;
+            c.st.h[v] = 0;
+        }
+        for (int e = b + c.lane; e < e1; e += 32) {
+            int w = ldro(&c.col[e]);
+            c.st.res[e] = (ldcg(&c.st.mark[w]) >= M) ? ldro(&c.cap[e]) : 0;
+        }
+        mask_arcs += e1 - b;
+        if (c.lane == 0) {
+            c.w_arcs += e1 - b;
+            c.w_verts += 1;
+        }
+    }
+    if (c.lane == 0 && mask_arcs) atomic_add_i64(&c.st.acc[ACC_TOT + T_MASKARCS], mask_arcs);
+    return c.sync();
+}
+
+// Saturate every residual arc out of s (RA:173-200; parallel over arcs).
+__device__ bool preflow(QCtx &c, int s) {
+    int b = ldro(&c.row[s]), e1 = ldro(&c.row[s + 1]);
+    int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+    for (int e = b + gt; e < e1; e += gT) {
+        i64 d = ldcg(&c.st.res[e]);
+        if (d > 0) {
+            c.st.res[e] = 0;
+            atomic_add_i64(&c.st.res[ldro(&c.rev[e])], d);
+            atomic_add_i64(&c.st.ex[ldro(&c.col[e])], d);
+        }
+    }
+    return c.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Exact global relabel.  Seeds at height 0: the phase sink (if any) and, in
+// phases A and B, every deficit vertex (RA:224-231 seeds the sink and
+// negative-excess vertices).  Backward BFS over residual arcs through kept
+// vertices; the blocked vertex is never labeled.  Afterwards unreached kept
+// vertices get height n, and the active list (excess > 0, height < n, not
+// the phase sink or blocked vertex) is compacted into L.
+// Returns counts in na / nd (active / deficits).
+__device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int blockv, int srcv,
+                               bool deficit_seeds, int *L, int &na, int &nd, i64 *&ab) {
+    unsigned cur = ++c.clock;
+    int qbk = c.take_bank();
+    const int n = c.n;
+    unsigned *mark = c.st.mark;
+    // seeds
+    for (int base = c.gw * 32; base < nv; base += c.gW * 32) {
+        int i = base + c.lane;
+        bool seed = false;
+        int v = 0;
+        if (i < nv) {
+            v = ldcg(&c.st.vlist[i]);
+            if (v == sinkv) seed = true;
+            else if (deficit_seeds && v != blockv && v != srcv && ldcg(&c.st.ex[v]) < 0) seed = true;
+            if (seed) {
+                mark[v] = cur;
+                c.st.h[v] = 0;
+            }
+        }
+        warp_append(seed, v, c.st.qa, &c.st.cnt[qbk]);
+    }
+    int hi = 0;
+    if (!c.sync_tail(qbk, hi)) return false;
+    const int *rev = c.rev;
+    i64 *res = c.st.res;
+    int *h = c.st.h;
+    auto relab = [&](int v, int e, int w, int level) -> bool {
+        if (w == blockv) return false;
+        unsigned mw = ldcg(&mark[w]);
+        if (mw < M || mw >= cur) return false;
+        if (ldcg(&res[ldro(&rev[e])]) <= 0) return false;
+        if (atomicCAS(&mark[w], mw, cur) != mw) return false;
+        h[w] = level + 1;
+        return true;
+    };
+    if (!bfs_levels(c, c.st.qa, qbk, hi, relab, nullptr)) return false;
+
+    // sweep: heights of unreached vertices, active list, counts
+    int lbk = c.take_bank();
+    ab = c.take_abank();
+    i64 l_sum = 0, l_high = 0, l_def = 0;
+    int l_hmin = INT_MAX, l_hmax = -1;
+    for (int base = c.gw * 32; base < nv; base += c.gW * 32) {
+        int i = base + c.lane;
+        bool act = false;
+        int v = 0;
+        if (i < nv) {
+            v = ldcg(&c.st.vlist[i]);
+            int hv;
+            if (ldcg(&mark[v]) != cur) {
+                h[v] = n;
+                hv = n;
+            } else {
+                hv = ldcg(&h[v]);
+            }
+            i64 ev = ldcg(&c.st.ex[v]);
+            if (ev > 0 && hv < n && v != sinkv && v != blockv) {
+                act = true;
+                l_sum += ev;
+                if (hv > 0) l_hmin = min(l_hmin, hv);
+                l_hmax = max(l_hmax, hv);
+                l_high += (hv > 0);
+            }
+            if (ev < 0 && v != srcv && v != blockv) ++l_def;
+        }
+        warp_append(act, v, L, &c.st.cnt[lbk]);
+    }
+    l_sum = warp_sum_i64(l_sum);
+    l_def = warp_sum_i64(l_def);
+    if (c.lane == 0) {
+        if (l_sum) atomic_add_i64(&ab[A_SUMEX], l_sum);
+        if (l_def) atomic_add_i64(&ab[A_NDEF], l_def);
+    }
+    if (!c.sync()) return false;
+    na = ldcg(&c.st.cnt[lbk]);
+    nd = (int)ldcg(&ab[A_NDEF]);
+    (void)l_high;
+    (void)l_hmin;
+    (void)l_hmax;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Push d along arc e = v->w; returns true when w turns active (its excess
+// crosses from <= 0 to > 0) and should join the next worklist.
+__device__ __forceinline__ bool push_arc(QCtx &c, int e, int w, i64 d, int sinkv, int blockv) {
+    atomic_add_i64(&c.st.res[e], -d);
+    atomic_add_i64(&c.st.res[ldro(&c.rev[e])], d);
+    i64 old = atomic_add_i64(&c.st.ex[w], d);
+    return old <= 0 && old + d > 0 && w != sinkv && w != blockv;
+}
+
+// Claim w for the next worklist (stamp de-dup) — true if this caller adds it.
+__device__ __forceinline__ bool enlist(QCtx &c, int w, unsigned rstamp) {
+    return atomicMax(&c.st.qmark[w], rstamp) < rstamp;
+}
+
+// Discharge one vertex with a whole warp for up to K cycles.  Each cycle
+// scans v's arcs 32 at a time: lanes read residual + head height, a ballot
+// finds downhill residual arcs, a 64-bit inclusive shuffle scan splits the
+// remaining excess over them in arc order, and every lane pushes its share
+// with native 64-bit atomics.  If excess remains after all arcs, v is
+// relabeled to 1 + the lowest height over arcs that still have residual
+// (n when none).  Newly active heads and v itself (if still active) are
+// appended to N.
+__device__ void discharge_vertex(QCtx &c, int v, int K, int sinkv, int blockv, int *N, int nbk,
+                                 unsigned rstamp, i64 *ab) {
+    const int n = c.n;
+    int hv = ldcg(&c.st.h[v]);
+    i64 ev = ldcg(&c.st.ex[v]);
+    int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+    i64 pushes = 0, arcs = 0;
+    for (int cyc = 0; cyc < K; ++cyc) {
+        if (ev <= 0 || hv >= n) break;
+        i64 rem = ev;
+        int minh = MF_INF_H;
+        for (int base = b; base < e1; base += 32) {
+            int e = base + c.lane;
+            i64 r = 0;
+            int w = 0, hw = MF_INF_H;
+            if (e < e1) {
+                r = ldcg(&c.st.res[e]);
+                if (r > 0) {
+                    w = ldro(&c.col[e]);
+                    hw = ldcg(&c.st.h[w]);
+                }
+            }
+            bool adm = r > 0 && hw < hv;
+            unsigned am = __ballot_sync(MF_FULL, adm);
+            i64 d = 0;
+            bool act = false;
+            if (am) {
+                i64 x = adm ? r : 0;
+                i64 incl = warp_incl_scan_i64(x);
+                i64 excl = incl - x;
+                if (adm && rem > excl) d = min(r, rem - excl);
+                if (d > 0) act = push_arc(c, e, w, d, sinkv, blockv);
+                i64 tot = __shfl_sync(MF_FULL, incl, 31);
+                rem -= min(tot, rem);
+                pushes += __popc(__ballot_sync(MF_FULL, d > 0));
+            }
+            if (r - d > 0) minh = min(minh, hw);
+            bool add = act && enlist(c, w, rstamp);
+            warp_append(add, w, N, &c.st.cnt[nbk]);
+            arcs += min(32, e1 - base);
+            if (rem == 0) break;
+        }
+        i64 pushed = ev - rem;
+        if (c.lane == 0 && pushed) atomic_add_i64(&c.st.ex[v], -pushed);
+        if (rem > 0) {
+            int mh = __reduce_min_sync(MF_FULL, minh);
+            hv = (mh >= n - 1) ? n : mh + 1;
+            if (c.lane == 0) c.st.h[v] = hv;
+        }
+        __syncwarp();
+        ev = ldcg(&c.st.ex[v]);
+        ev = __shfl_sync(MF_FULL, ev, 0);
+    }
+    bool again = (c.lane == 0) && ev > 0 && hv < n && enlist(c, v, rstamp);
+    warp_append(again, v, N, &c.st.cnt[nbk]);
+    if (c.lane == 0) {
+        c.w_arcs += arcs;
+        c.w_verts += 1;
+        c.w_push += pushes;
+        if (arcs) atomic_add_i64(&ab[A_WORK], arcs);
+    }
+}
+
+// Path push (RA:773-955): follow exactly-one-lower residual arcs from v for
+// up to max_path hops, pushing the whole excess along; vertices on the path
+// are claimed with a per-round ownership stamp so that only one warp ever
+// lowers a vertex's excess.  Relabels in place when stuck (bounded retries).
+__device__ void path_push_vertex(QCtx &c, int v, int max_path, int sinkv, int blockv, int *N,
+                                 int nbk, unsigned rstamp, unsigned pstamp, i64 *ab) {
+    const int n = c.n;
+    bool own = false;
+    if (c.lane == 0) own = atomicMax(&c.st.claim[v], pstamp) < pstamp;
+    own = __shfl_sync(MF_FULL, own, 0);
+    if (!own) return;
+    int cur = v;
+    int hops = 0, steps = 0;
+    i64 arcs = 0, pushes = 0;
+    while (hops < max_path && steps < 2 * max_path + 8) {
+        ++steps;
+        i64 ec = ldcg(&c.st.ex[cur]);
+        ec = __shfl_sync(MF_FULL, ec, 0);
+        if (ec <= 0 || cur == sinkv) break;
+        int hc = ldcg(&c.st.h[cur]);
+        hc = __shfl_sync(MF_FULL, hc, 0);
+        if (hc >= n) break;
+        int b = ldro(&c.row[cur]), e1 = ldro(&c.row[cur + 1]);
+        int best_e = INT_MAX, minh = MF_INF_H;
+        for (int base = b; base < e1; base += 32) {
+            int e = base + c.lane;
+            if (e < e1) {
+                i64 r = ldcg(&c.st.res[e]);
+                if (r > 0) {
+                    int hw = ldcg(&c.st.h[ldro(&c.col[e])]);
+                    minh = min(minh, hw);
+                    if (hw == hc - 1) best_e = min(best_e, e);
+                }
+            }
+            arcs += min(32, e1 - base);
+        }
+        best_e = __reduce_min_sync(MF_FULL, best_e);
+        minh = __reduce_min_sync(MF_FULL, minh);
+        if (best_e != INT_MAX) {
+            int nxt = 0;
+            bool cont = false;
+            if (c.lane == 0) {
+                int w = ldro(&c.col[best_e]);
+                i64 r = ldcg(&c.st.res[best_e]);
+                i64 d = min(ec, r);
+                bool act = false;
+                if (d > 0) {
+                    act = push_arc(c, best_e, w, d, sinkv, blockv);
+                    atomic_add_i64(&c.st.ex[cur], -d);
+                    ++pushes;
+                }
+                if (ec - d > 0 && enlist(c, cur, rstamp)) {
+                    int k = atomicAdd(&c.st.cnt[nbk], 1);
+                    N[k] = cur;
+                }
+                if (w != sinkv && w != blockv && atomicMax(&c.st.claim[w], pstamp) < pstamp) {
+                    cont = true;
+                    nxt = w;
+                } else if (act && enlist(c, w, rstamp)) {
+                    int k = atomicAdd(&c.st.cnt[nbk], 1);
+                    N[k] = w;
+                }
+            }
+            cont = __shfl_sync(MF_FULL, cont, 0);
+            nxt = __shfl_sync(MF_FULL, nxt, 0);
+            ++hops;
+            if (!cont) {
+                cur = -1;
+                break;
+            }
+            cur = nxt;
+        } else {
+            int nh = (minh >= n - 1) ? n : minh + 1;
+            if (c.lane == 0) c.st.h[cur] = nh;
+            if (nh >= n) break;
+        }
+    }
+    if (c.lane == 0 && cur >= 0) {
+        i64 ec = ldcg(&c.st.ex[cur]);
+        if (ec > 0 && ldcg(&c.st.h[cur]) < n && cur != sinkv && enlist(c, cur, rstamp)) {
+            int k = atomicAdd(&c.st.cnt[nbk], 1);
+            N[k] = cur;
+        }
+    }
+    if (c.lane == 0) {
+        c.w_arcs += arcs;
+        c.w_verts += hops + 1;
+        c.w_push += pushes;
+        if (arcs) atomic_add_i64(&ab[A_WORK], arcs);
+    }
+}
+
+// Hot-region selection (RA:1902-1946): per-region counts of the worklist,
+// top-K regions with a non-zero count become hot.  CTA 0 of the group
+// bitonic-sorts (count desc, region asc) in shared memory.
+__device__ bool select_hot(QCtx &c, const int *N, int nN, int hot_k) {
+    const int R = c.R;
+    int *hot = c.st.hot;
+    int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+    for (int i = gt; i < nN; i += gT) atomicAdd(&hot[ldro(&c.rof[ldcg(&N[i])])], 1);
+    if (!c.sync()) return false;
+    if (c.crank == 0) {
+        __shared__ long long keys[1024];
+        int P = 1;
+        while (P < R) P <<= 1;
+        for (int i = threadIdx.x; i < P; i += blockDim.x) {
+            long long k = LLONG_MAX;
+            if (i < R) k = ((long long)(INT_MAX - ldcg(&hot[i])) << 16) | i;
+            keys[i] = k;
+        }
+        __syncthreads();
+        for (int k = 2; k <= P; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = threadIdx.x; i < P; i += blockDim.x) {
+                    int ixj = i ^ j;
+                    if (ixj > i) {
+                        long long a = keys[i], b2 = keys[ixj];
+                        bool up = ((i & k) == 0);
+                        if ((a > b2) == up) {
+                            keys[i] = b2;
+                            keys[ixj] = a;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        for (int i = threadIdx.x; i < R; i += blockDim.x) {
+            long long k = keys[i];
+            int r = (int)(k & 0xffff);
+            int cntv = INT_MAX - (int)(k >> 16);
+            // reuse hot[] as the flag array: hot iff rank < hot_k and count > 0
+            // (written after all reads above, separated by __syncthreads)
+            keys[i] = ((long long)r << 1) | ((i < hot_k && cntv > 0) ? 1 : 0);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < R; i += blockDim.x) {
+            long long k = keys[i];
+            hot[(int)(k >> 1)] = (int)(k & 1);
+        }
+    }
+    return c.sync();
+}
+
+// RM (RA:605-657): for kept vertices in active regions with height in the
+// band, every arc v->w with h(w) > h(v)+1, excess(w) <= 0 and residual on
+// w->v has that residual moved from w to v (saturating the steep arc w->v).
+// Residuals updated atomically; w may go negative (a deficit).
+__device__ bool rm_pass(QCtx &c, int nv, unsigned M, int hlo, int hhi, int s, int t, int *N,
+                        int nbk, unsigned rstamp, i64 *ab) {
+    const int n = c.n;
+    i64 fixed = 0;
+    for (int i = c.gw; i < nv; i += c.gW) {
+        int v = ldcg(&c.st.vlist[i]);
+        if (v == s || v == t) continue;
+        if (!ldcg(&c.st.ract[ldro(&c.rof[v])])) continue;
+        int hv = ldcg(&c.st.h[v]);
+        if (hv < hlo || hv > hhi || hv >= n) continue;
+        int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+        i64 gained = 0;
+        for (int base = b; base < e1; base += 32) {
+            int e = base + c.lane;
+            i64 d = 0;
+            if (e < e1) {
+                int w = ldro(&c.col[e]);
+                if (ldcg(&c.st.mark[w]) >= M && ldcg(&c.st.h[w]) > hv + 1 &&
+                    ldcg(&c.st.ex[w]) <= 0) {
+                    int re = ldro(&c.rev[e]);
+                    if (ldcg(&c.st.res[re]) > 0) {
+                        d = (i64)atomicExch(reinterpret_cast<u64 *>(&c.st.res[re]), 0ull);
+                        if (d > 0) {
+                            atomic_add_i64(&c.st.res[e], d);
+                            atomic_add_i64(&c.st.ex[w], -d);
+                        }
+                    }
+                }
+            }
+            gained += d;
+            fixed += (d > 0);
+        }
+        gained = warp_sum_i64(gained);
+        bool add = false;
+        if (c.lane == 0 && gained > 0) {
+            i64 old = atomic_add_i64(&c.st.ex[v], gained);
+            add = old <= 0 && old + gained > 0 && enlist(c, v, rstamp);
+            if (!add && old > 0) add = enlist(c, v, rstamp);
+        }
+        warp_append(add, v, N, &c.st.cnt[nbk]);
+        if (c.lane == 0) {
+            c.w_arcs += e1 - b;
+            c.w_verts += 1;
+        }
+    }
+    fixed = warp_sum_i64(fixed);
+    if (c.lane == 0 && fixed) atomic_add_i64(&ab[A_FIXED], fixed);
+    return c.sync();
+}
+
+// ---------------------------------------------------------------------------
+// The push-relabel driver for one phase set (RA:1450-2115, device-resident):
+// relabel -> rounds of discharge (+ hot sweep, path push, RM, stagnation
+// control) -> relabel ... until a relabel finds nothing to do.
+// final_phase == PH_A: max preflow for (s,t); PH_C: return excess to s.
+__device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsigned M,
+                           int start_phase, QOut &qo, int &status) {
+    const int n = c.n;
+    int phase = start_phase;
+    int K = o.K;
+    int gr_freq = o.gr_freq;
+    const int gr_base = o.gr_freq;
+    int rm_freq = o.rm_freq;
+    int stag = 0, calm = 0;
+    i64 last_sum = LLONG_MAX;
+    int pp_stable = 0, p_count = 64, pp_iter = 0;
+    i64 round = 0;
+    i64 mask_arcs = ldcg(&c.st.acc[ACC_TOT + T_MASKARCS]);
+    int *L = c.st.qb, *N = c.st.qa;
+    for (;;) {
+        int sinkv = (phase == PH_A) ? t : (phase == PH_B ? -1 : s);
+        int blockv = (phase == PH_C) ? t : s;
+        bool defseeds = (phase != PH_C);
+        int na = 0, nd = 0;
+        i64 *ab = nullptr;
+        L = c.st.qb;
+        N = c.st.qa;
+        if (!global_relabel(c, nv, M, sinkv, blockv, s, defseeds, L, na, nd, ab)) return false;
+        qo.relabels++;
+        if (na == 0) {
+            if (phase == PH_A) {
+                if (nd == 0) return true;
+                phase = PH_B;
+                qo.deficit_phases++;
+                continue;
+            }
+            if (phase == PH_B) {
+                if (nd == 0) {
+                    phase = PH_A;
+                    continue;
+                }
+                status = MFD_INEXACT;
+                return true;
+            }
+            if (nd != 0) status = MFD_INEXACT;
+            return true;  // PH_C done
+        }
+        i64 work_since = 0;
+        int rounds_since = 0;
+        bool force_gr = false;
+        while (na > 0) {
+            if (round >= o.iter_max) {
+                status = MFD_ITER_LIMIT;
+                return true;
+            }
+            // launch time limit: the leader raises the error word; every CTA
+            // then leaves at its next group barrier
+            if (c.leader && c.time_limit && globaltimer_ns() - c.t_start > c.time_limit)
+                atomicCAS(c.err, 0, MFD_TIMEOUT);
+            // ---- one discharge round over L -> N
+            unsigned rstamp = ++c.clock;
+            int nbk = c.take_bank();
+            i64 *rb = c.take_abank();
+            if (na > 0 && na <= o.pp_switch) ++pp_stable;
+            else {
+                pp_stable = 0;
+                p_count = 64;
+            }
+            bool use_pp = o.use_pp && na > 0 && na <= o.pp_switch &&
+                          (o.force_pp || pp_stable >= p_count);
+            // round-start counts over L (RA:1738-1763): active-high, sum of excess, band
+            i64 l_sum = 0, l_high = 0;
+            int l_hmin = INT_MAX, l_hmax = -1;
+            for (int i = c.gw * 32 + c.lane; i < na; i += c.gW * 32) {
+                int v = ldcg(&L[i]);
+                i64 ev = ldcg(&c.st.ex[v]);
+                int hv = ldcg(&c.st.h[v]);
+                if (ev > 0 && hv < n) {
+                    l_sum += ev;
+                    l_high += (hv > o.h_cut);
+                    l_hmin = min(l_hmin, hv);
+                    l_hmax = max(l_hmax, hv);
+                }
+            }
+            l_sum = warp_sum_i64(l_sum);
+            l_high = warp_sum_i64(l_high);
+            l_hmin = __reduce_min_sync(MF_FULL, l_hmin);
+            l_hmax = __reduce_max_sync(MF_FULL, l_hmax);
+            if (c.lane == 0) {
+                if (l_sum) atomic_add_i64(&rb[A_SUMEX], l_sum);
+                if (l_high) atomic_add_i64(&rb[A_HIGH], l_high);
+                if (l_hmin != INT_MAX) atomicMin(reinterpret_cast<long long *>(&rb[A_HMIN]), (long long)l_hmin);
+                if (l_hmax >= 0) atomicMax(reinterpret_cast<long long *>(&rb[A_HMAX]), (long long)l_hmax);
+            }
+            if (use_pp) {
+                unsigned pstamp = ++c.clock;
+                for (int i = c.gw; i < na; i += c.gW)
+                    path_push_vertex(c, ldcg(&L[i]), o.max_path, sinkv, blockv, N, nbk, rstamp,
+                                     pstamp, rb);
+                pp_stable = 0;
+                if (++pp_iter >= 4) {
+                    pp_iter = 0;
+                    p_count = 2;
+                }
+                qo.pp_rounds++;
+            } else {
+                for (int i = c.gw; i < na; i += c.gW)
+                    discharge_vertex(c, ldcg(&L[i]), K, sinkv, blockv, N, nbk, rstamp, rb);
+            }
+            // clear region scratch for this round's optional passes
+            {
+                int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+                for (int r = gt; r < c.R; r += gT) {
+                    c.st.hot[r] = 0;
+                    c.st.ract[r] = 0;
+                }
+            }
+            if (!c.sync()) return false;
+            int nN = ldcg(&c.st.cnt[nbk]);
+            i64 sum = ldcg(&rb[A_SUMEX]);
+            i64 high = ldcg(&rb[A_HIGH]);
+            int hmin = (int)ldcg(&rb[A_HMIN]), hmax = (int)ldcg(&rb[A_HMAX]);
+            i64 work_round = ldcg(&rb[A_WORK]);
+            work_since += work_round;
+            ++round;
+            ++rounds_since;
+            qo.rounds = round;
+            float frac_high = (na > 0) ? (float)high / (float)na : 0.0f;
+            if (frac_high > 0.8f && (round % 2048) == 0) force_gr = true;
+            // stagnation control (RA:1860-1891)
+            bool hotspot = false;
+            if (last_sum != LLONG_MAX) {
+                if (sum >= last_sum) ++stag;
+                else stag = 0;
+            }
+            last_sum = sum;
+            if (stag >= o.stagnate && !use_pp) {
+                hotspot = true;
+                force_gr = true;
+                stag = 0;
+                gr_freq = min(2 * gr_base, gr_freq * 2);
+                K = min(16, K * 2);
+                calm = 0;
+            } else if (++calm >= o.stagnate) {
+                gr_freq = max(gr_base, gr_freq / 2);
+                K = max(4, K / 2);
+                calm = 0;
+            }
+            // hot-region extra sweep over the next worklist (RA:1899-1984)
+            if (o.use_hot && !use_pp && !hotspot && nN >= 64 && (round % 2) == 1 && c.R > 1) {
+                if (!select_hot(c, N, nN, o.hot_k)) return false;
+                for (int i = c.gw; i < nN; i += c.gW) {
+                    int v = ldcg(&N[i]);
+                    if (ldcg(&c.st.hot[ldro(&c.rof[v])]))
+                        discharge_vertex(c, v, K, sinkv, blockv, N, nbk, rstamp, rb);
+                }
+                if (!c.sync()) return false;
+                nN = ldcg(&c.st.cnt[nbk]);
+                work_since += ldcg(&rb[A_WORK]) - work_round;
+                qo.hot_sweeps++;
+            }
+            // RM (RA:1991-2097)
+            bool do_rm = o.use_rm && start_phase != PH_C && nN > 0 && (round % rm_freq) == 0 &&
+                         (o.force_rm || frac_high >= 0.5f);
+            if (do_rm) {
+                int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+                for (int i = gt; i < nN; i += gT) c.st.ract[ldro(&c.rof[ldcg(&N[i])])] = 1;
+                if (!c.sync()) return false;
+                int hlo = max(0, (hmin == INT_MAX ? 0 : hmin) - 4);
+                int hhi = min(n - 1, (hmax < 0 ? n - 1 : hmax) + 4);
+                if (!rm_pass(c, nv, M, hlo, hhi, s, t, N, nbk, rstamp, rb)) return false;
+                nN = ldcg(&c.st.cnt[nbk]);
+                i64 fixed = ldcg(&rb[A_FIXED]);
+                qo.rm_fixed += fixed;
+                double frac_fix = (double)fixed / (double)max((i64)1, mask_arcs);
+                if (frac_fix < 1e-5) rm_freq = min(rm_freq * 2, 256);
+                else rm_freq = max(o.rm_freq, rm_freq / 2);
+                if (fixed) force_gr = true;  // deficits are relabel seeds
+            }
+            // next round
+            int *tmp = L;
+            L = N;
+            N = tmp;
+            na = nN;
+            bool gr_due = force_gr || rounds_since >= gr_freq ||
+                          (o.gr_alpha > 0.0 && (double)work_since >= o.gr_alpha * (double)mask_arcs);
+            if (gr_due) break;
+        }
+        // relabel (either na == 0 -> exact termination check, or due)
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Certificate (after phase C): zero excess off {s,t}; residuals >= 0 and
+// pairwise conserved on kept arcs; T = vertices reaching t in the full-graph
+// residual (kept arcs: res; other arcs: cap); s not in T; capacity of
+// (V\T -> T) == flow.  Uses qmark as the full-graph BFS stamp.
+__device__ bool certify(QCtx &c, int s, int t, int nv, unsigned M, i64 flow, QOut &qo, int &status) {
+    i64 *ab = c.take_abank();
+    i64 bad = 0;
+    for (int i = c.gw; i < nv; i += c.gW) {
+        int v = ldcg(&c.st.vlist[i]);
+        if (c.lane == 0 && v != s && v != t && ldcg(&c.st.ex[v]) != 0) ++bad;
+        int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+        for (int e = b + c.lane; e < e1; e += 32) {
+            int w = ldro(&c.col[e]);
+            i64 r = ldcg(&c.st.res[e]);
+            if (r < 0) ++bad;
+            if (ldcg(&c.st.mark[w]) >= M) {
+                int re = ldro(&c.rev[e]);
+                if (r + ldcg(&c.st.res[re]) != ldro(&c.cap[e]) + ldro(&c.cap[re])) ++bad;
+            }
+        }
+    }
+    bad = warp_sum_i64(bad);
+    if (c.lane == 0 && bad) atomic_add_i64(&ab[A_BAD], bad);
+    // full-graph backward BFS from t
+    unsigned Z = ++c.clock;
+    int bk = c.take_bank();
+    if (c.leader) {
+        c.st.qmark[t] = Z;
+        c.st.qa[0] = t;
+        c.st.cnt[bk] = 1;
+    }
+    if (!c.sync()) return false;
+    unsigned *qm = c.st.qmark, *mark = c.st.mark;
+    const int *rev = c.rev;
+    const i64 *cap = c.cap;
+    i64 *res = c.st.res;
+    auto cut_bfs = [&](int v, int e, int w, int) -> bool {
+        if (ldcg(&qm[w]) == Z) return false;
+        int re = ldro(&rev[e]);  // arc w->v
+        bool kept = ldcg(&mark[w]) >= M && ldcg(&mark[v]) >= M;
+        i64 r = kept ? ldcg(&res[re]) : ldro(&cap[re]);
+        if (r <= 0) return false;
+        return atomicMax(&qm[w], Z) < Z;
+    };
+    if (!bfs_levels(c, c.st.qa, bk, 1, cut_bfs, nullptr)) return false;
+    // cut capacity over all vertices
+    i64 cut = 0;
+    for (int v = c.gw; v < c.n; v += c.gW) {
+        if (ldcg(&qm[v]) == Z) continue;
+        int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+        for (int e = b + c.lane; e < e1; e += 32) {
+            i64 cp = ldro(&cap[e]);
+            if (cp > 0 && ldcg(&qm[ldro(&c.col[e])]) == Z) cut += cp;
+        }
+    }
+    cut = warp_sum_i64(cut);
+    if (c.lane == 0 && cut) atomic_add_i64(&ab[A_CUT], cut);
+    if (!c.sync()) return false;
+    i64 total_bad = ldcg(&ab[A_BAD]);
+    i64 cutv = ldcg(&ab[A_CUT]);
+    bool s_in_t = ldcg(&qm[s]) == Z;
+    qo.cut = cutv;
+    if (total_bad != 0 || s_in_t || cutv != flow) status = MFD_CERTIFY;
+    return true;
+}
+
+// Full-graph residuals for host-side certification: kept arcs res, others cap.
+__device__ bool write_full_residual(QCtx &c, unsigned M, i64 *out) {
+    for (int v = c.gw; v < c.n; v += c.gW) {
+        bool kv = ldcg(&c.st.mark[v]) >= M;
+        int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+        for (int e = b + c.lane; e < e1; e += 32) {
+            int w = ldro(&c.col[e]);
+            bool kept = kv && ldcg(&c.st.mark[w]) >= M;
+            out[e] = kept ? ldcg(&c.st.res[e]) : ldro(&c.cap[e]);
+        }
+    }
+    return c.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Warm start after capacity updates (mode KM_REPAIR).  The slot keeps the
+// previous solve's residual, excess and kept set (meta: M_old, nv_old).
+// 1. old kept vertices get claim stamp O; 2. re-prune on the new capacities;
+// new kept = old kept U new prune; 3. vertices new to the kept set get fresh
+// state and their arc pairs with kept vertices are reopened; 4. each updated
+// arc inside the kept set adjusts its residual, cancelling flow above the
+// new capacity (tail gains excess, head loses it); 5. s re-saturates.
+__device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int &nv, bool &t_reach) {
+    int *meta = c.st.meta;
+    unsigned M_old = (unsigned)ldcg(&meta[0]);
+    int nv_old = ldcg(&meta[1]);
+    unsigned O = ++c.clock;
+    for (int i = c.crank * blockDim.x + threadIdx.x; i < nv_old; i += c.G * blockDim.x)
+        c.st.claim[ldcg(&c.st.vlist[i])] = O;
+    if (!c.sync()) return false;
+    unsigned S = ++c.clock;
+    unsigned Mn = ++c.clock;
+    // prune into qb-list of vertices new to the kept set (vlist kept as-is)
+    int bank = c.take_bank();
+    if (c.leader) {
+        c.st.mark[s] = S;
+        c.st.qa[0] = s;
+        c.st.cnt[bank] = 1;
+    }
+    if (!c.sync()) return false;
+    unsigned *mark = c.st.mark, *claim = c.st.claim;
+    const i64 *cap = c.cap;
+    const int *rev = c.rev;
+    auto fwd = [&](int v, int e, int w, int) -> bool {
+        if (ldro(&cap[e]) <= 0) return false;
+        if (ldcg(&mark[w]) >= S) return false;
+        return atomicMax(&mark[w], S) < S;
+    };
+    if (!bfs_levels(c, c.st.qa, bank, 1, fwd, nullptr)) return false;
+    t_reach = ldcg(&mark[t]) >= S;
+    int nb = c.take_bank();
+    int addb = c.take_bank();
+    if (t_reach) {
+        if (c.leader) {
+            mark[t] = Mn;
+            c.st.qb[0] = t;
+            c.st.cnt[nb] = 1;
+        }
+        if (!c.sync()) return false;
+        auto bwd = [&](int v, int e, int w, int) -> bool {
+            if (ldcg(&mark[w]) != S) return false;
+            if (ldro(&cap[ldro(&rev[e])]) <= 0) return false;
+            return atomicCAS(&mark[w], S, Mn) == S;
+        };
+        if (!bfs_levels(c, c.st.qb, nb, 1, bwd, nullptr)) return false;
+    }
+    int nnew_bfs = t_reach ? ldcg(&c.st.cnt[nb]) : 0;
+    // new kept vertices = bwd-reached not in the old set -> appended to vlist
+    if (c.leader) c.st.cnt[addb] = nv_old;
+    if (!c.sync()) return false;
+    for (int base = c.gw * 32; base < nnew_bfs; base += c.gW * 32) {
+        int i = base + c.lane;
+        bool add = false;
+        int v = 0;
+        if (i < nnew_bfs) {
+            v = ldcg(&c.st.qb[i]);
+            add = ldcg(&claim[v]) != O;
+        }
+        warp_append(add, v, c.st.vlist, &c.st.cnt[addb]);
+    }
+    if (!c.sync()) return false;
+    nv = ldcg(&c.st.cnt[addb]);
+    // every kept vertex (old and new) gets the current mask stamp
+    for (int i = c.crank * blockDim.x + threadIdx.x; i < nv; i += c.G * blockDim.x)
+        mark[ldcg(&c.st.vlist[i])] = Mn;
+    if (!c.sync()) return false;
+    // fresh state for new vertices; reopen their arc pairs
+    i64 add_arcs = 0;
+    for (int i = nv_old + c.gw; i < nv; i += c.gW) {
+        int v = ldcg(&c.st.vlist[i]);
+        int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+        if (c.lane == 0) {
+            c.st.ex[v] = 0;
+            c.st.h[v] = 0;
+        }
+        for (int e = b + c.lane; e < e1; e += 32) {
+            int w = ldro(&c.col[e]);
+            if (ldcg(&mark[w]) == Mn) {
+                c.st.res[e] = ldro(&cap[e]);
+                if (ldcg(&claim[w]) == O) {
+                    int re = ldro(&rev[e]);
+                    c.st.res[re] = ldro(&cap[re]);
+                }
+            } else {
+                c.st.res[e] = 0;
+            }
+        }
+        add_arcs += e1 - b;
+    }
+    if (c.lane == 0 && add_arcs) atomic_add_i64(&c.st.acc[ACC_TOT + T_MASKARCS], add_arcs);
+    if (!c.sync()) return false;
+    // capacity deltas on kept arcs (forward arcs of changed edges)
+    int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+    for (int i = gt; i < p.nupd; i += gT) {
+        ArcUpdate u = p.upd[i];
+        int e = u.arc;
+        int re = ldro(&rev[e]);
+        int w = ldro(&c.col[e]);
+        int x = ldro(&c.col[re]);  // tail of e
+        if (ldcg(&mark[w]) != Mn || ldcg(&mark[x]) != Mn) continue;
+        // arc e (x->w) carries flow f = old_cap - res[e] on its pair
+        // (its partner is a zero-capacity reverse arc).  Arcs that were
+        // opened in step 3 already hold the new capacity.
+        if (ldcg(&claim[x]) != O || ldcg(&claim[w]) != O) continue;
+        i64 r = ldcg(&c.st.res[e]);
+        i64 f = u.old_cap - r;
+        if (f <= u.new_cap) {
+            atomic_add_i64(&c.st.res[e], u.new_cap - u.old_cap);
+        } else {
+            i64 over = f - u.new_cap;
+            atomic_add_i64(&c.st.res[e], -r);
+            atomic_add_i64(&c.st.res[re], -over);
+            atomic_add_i64(&c.st.ex[x], over);
+            atomic_add_i64(&c.st.ex[w], -over);
+        }
+    }
+    if (!c.sync()) return false;
+    M = Mn;
+    if (!t_reach) return true;
+    return preflow(c, s);
+}
+
+// ---------------------------------------------------------------------------
+__device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
+    QOut qo = {};
+    int status = MFD_OK;
+    const KOpts &o = p.o;
+    if (c.leader) {
+        for (int i = 0; i < NBANKS; ++i) c.st.cnt[i] = 0;
+        for (int i = 0; i < 4 * ACC_BANK; ++i) c.st.acc[i] = 0;
+        for (int b = 0; b < 4; ++b) {
+            c.st.acc[b * ACC_BANK + A_HMIN] = INT_MAX;
+            c.st.acc[b * ACC_BANK + A_HMAX] = -1;
+        }
+        for (int i = 0; i < 8; ++i) c.st.acc[ACC_TOT + i] = 0;
+    }
+    c.seq = 0;
+    c.aseq = 0;
+    if (!c.sync()) return;
+    unsigned M = 0;
+    int nv = 0;
+    bool t_reach = false;
+    if (p.mode == KM_REPAIR) {
+        if (!repair(c, p, s, t, M, nv, t_reach)) return;
+    } else {
+        unsigned S = ++c.clock;
+        M = ++c.clock;
+        if (!prune(c, s, t, o.prune_mode, S, M, nv, t_reach)) return;
+        if (p.mode == KM_PRUNE) {
+            unsigned char *mk = (unsigned char *)p.dbg;
+            int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+            for (int v = gt; v < c.n; v += gT)
+                mk[v] = (ldcg(&c.st.mark[v]) == M || v == s || v == t) ? 1 : 0;
+            if (c.leader) {
+                qo.mask_n = (o.prune_mode == 1 && !t_reach) ? 2 : nv;
+                p.out[q] = qo;
+            }
+            c.sync();
+            return;
+        }
+        if (t_reach && nv > 0) {
+            if (!init_state(c, nv, M)) return;
+            if (!preflow(c, s)) return;
+        }
+    }
+    i64 flow = 0;
+    if (t_reach && nv > 0) {
+        if (p.mode == KM_HEIGHTS) {
+            int na = 0, nd = 0;
+            i64 *ab = nullptr;
+            if (!global_relabel(c, nv, M, t, s, s, true, c.st.qb, na, nd, ab)) return;
+            int *hd = (int *)p.dbg;
+            int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+            for (int v = gt; v < c.n; v += gT)
+                hd[v] = (ldcg(&c.st.mark[v]) >= M) ? ldcg(&c.st.h[v]) : c.n;
+            if (!c.sync()) return;
+        } else {
+            if (!run_phases(c, o, s, t, nv, M, PH_A, qo, status)) return;
+            flow = ldcg(&c.st.ex[t]);
+            if (p.mode == KM_CERTIFY && status == MFD_OK) {
+                if (!run_phases(c, o, s, t, nv, M, PH_C, qo, status)) return;
+                if (status == MFD_OK && !certify(c, s, t, nv, M, flow, qo, status)) return;
+            }
+        }
+    } else if (p.mode == KM_HEIGHTS) {
+        int *hd = (int *)p.dbg;
+        int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+        for (int v = gt; v < c.n; v += gT) hd[v] = c.n;
+        if (!c.sync()) return;
+    }
+    if (p.mode == KM_RESIDUAL) {
+        if (t_reach && nv > 0) {
+            if (!write_full_residual(c, M, (i64 *)p.dbg)) return;
+        } else {
+            i64 *out = (i64 *)p.dbg;
+            int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+            for (i64 e = gt; e < (i64)ldro(&c.row[c.n]); e += gT) out[e] = ldro(&c.cap[e]);
+            if (!c.sync()) return;
+        }
+    }
+    c.flush_warp_counts();
+    if (!c.sync()) return;
+    if (c.leader) {
+        i64 *tot = c.st.acc + ACC_TOT;
+        qo.flow = flow;
+        qo.status = status;
+        qo.mask_n = nv;
+        qo.mask_arcs = tot[T_MASKARCS];
+        qo.arcs_ex = tot[T_ARCS];
+        qo.verts_ex = tot[T_VERTS];
+        qo.pushes = tot[T_PUSH];
+        p.out[q] = qo;
+        c.st.meta[0] = (int)M;
+        c.st.meta[1] = nv;
+        c.st.meta[2] = s;
+        c.st.meta[3] = t;
+        *c.st.clock = c.clock;
+    }
+    c.sync();
+}
+
+__global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
+    QCtx c;
+    c.G = p.G;
+    c.crank = blockIdx.x % p.G;
+    int gid = blockIdx.x / p.G;
+    c.wpc = blockDim.x >> 5;
+    c.gw = c.crank * c.wpc + (threadIdx.x >> 5);
+    c.gW = p.G * c.wpc;
+    c.lane = threadIdx.x & 31;
+    c.err = p.err;
+    c.lim = p.bar_limit_ns;
+    c.leader = (c.crank == 0 && threadIdx.x == 0);
+    c.w_arcs = c.w_verts = c.w_push = 0;
+    c.t_start = globaltimer_ns();
+    c.time_limit = p.time_limit_ns;
+    DSlot gslot = p.slots[gid];
+    c.bar = gslot.bar;
+    for (;;) {
+        // take a query (group leader), broadcast through the group slot
+        int *qcell = gslot.cnt + CNT_Q;
+        if (c.leader) {
+            int q;
+            if (p.ring_tail) {
+                q = atomicAdd(p.q_next, 1);
+                u64 t0 = globaltimer_ns();
+                unsigned spins = 0;
+                for (;;) {
+                    if (q < *p.ring_tail) break;
+                    if (*p.ring_stop) {
+                        q = INT_MAX;
+                        break;
+                    }
+                    __nanosleep(2000);
+                    if ((++spins & 63u) == 0 && globaltimer_ns() - t0 > p.idle_limit_ns) {
+                        q = INT_MAX;
+                        break;
+                    }
+                }
+                if (q != INT_MAX) {
+                    __threadfence_system();
+                    volatile const int *rq = reinterpret_cast<volatile const int *>(p.ring_req + q);
+                    gslot.cnt[CNT_RS] = rq[0];
+                    gslot.cnt[CNT_RT] = rq[1];
+                    gslot.cnt[CNT_RG] = rq[2];
+                    p.ring_done[q] = 2;
+                    p.ring_t0[2 * q] = globaltimer_ns();
+                }
+            } else {
+                q = atomicAdd(p.q_next, 1);
+            }
+            *qcell = q;
+        }
+        if (!gsync(c.G, c.bar, c.err, c.lim)) return;
+        int q = ldcg(qcell);
+        int nlimit = p.ring_tail ? INT_MAX - 1 : p.nq;
+        if (q >= nlimit) break;
+        int s, t, gi, si;
+        if (p.ring_tail) {
+            s = ldcg(&gslot.cnt[CNT_RS]);
+            t = ldcg(&gslot.cnt[CNT_RT]);
+            gi = ldcg(&gslot.cnt[CNT_RG]);
+            si = gid;
+        } else {
+            s = p.q_s[q];
+            t = p.q_t[q];
+            gi = p.q_g ? p.q_g[q] : 0;
+            si = p.q_slot ? p.q_slot[q] : gid;
+        }
+        DGraph g = p.graphs[gi];
+        c.n = g.n;
+        c.R = g.R;
+        c.row = g.row;
+        c.col = g.col;
+        c.rev = g.rev;
+        c.rof = g.region_of;
+        c.cap = g.cap;
+        c.st = p.slots[si];
+        c.clock = ldcg(c.st.clock);
+        if (s < 0 || t < 0 || s >= g.n || t >= g.n || s == t) {
+            if (c.leader) {
+                QOut z = {};
+                p.out[q] = z;
+            }
+        } else {
+            solve_query(c, p, q, s, t);
+        }
+        if (*(volatile int *)p.err) return;
+        if (p.ring_tail && c.leader) {
+            __threadfence_system();
+            p.ring_t0[2 * q + 1] = globaltimer_ns();
+            __threadfence_system();
+            p.ring_done[q] = 1;
+        }
+        if (!gsync(c.G, c.bar, c.err, c.lim)) return;
+    }
+}
+
+void mf_launch_kernel(const KParams &p, int grid, int threads, cudaStream_t st, bool cooperative,
+                      cudaError_t *err) {
+    void *args[] = {(void *)&p};
+    if (cooperative)
+        *err = cudaLaunchCooperativeKernel((void *)mf_kernel, dim3(grid), dim3(threads), args, 0, st);
+    else {
+        mf_kernel<<<grid, threads, 0, st>>>(p);
+        *err = cudaGetLastError();
+    }
+}
+
+int mf_kernel_max_blocks_per_sm(int threads) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mf_kernel, threads, 0) != cudaSuccess)
+        return 0;
+    return nb;
+}

@@ -1,0 +1,124 @@
+// Solver-side device structures shared by mf_solver.cu and the host API.
+#pragma once
+#include "mf_common.cuh"
+
+// Region-ordered CSR of one graph (device pointers).
+struct DGraph {
+    int n;
+    int R;
+    i64 arcs;
+    const int *row;        // n+1
+    const int *col;        // arcs
+    const int *rev;        // arcs
+    const i64 *cap;        // arcs (current capacities)
+    const int *region_of;  // n
+};
+
+// Working state of one residual slot.  All arrays are full-size for the
+// graph the slot serves; stamps make resets unnecessary between queries.
+struct DSlot {
+    i64 *res;          // arcs: residual capacity
+    i64 *ex;           // n: excess
+    int *h;            // n: height
+    unsigned *mark;    // n: prune / mask / relabel stamps
+    unsigned *qmark;   // n: worklist de-dup stamps (also undirected-prune stamps)
+    unsigned *claim;   // n: path-push ownership stamps / old-mask stamps
+    int *vlist;        // n: the query's kept (mask) vertices
+    int *qa;           // n: BFS queue / worklist
+    int *qb;           // n: worklist
+    int *hot;          // 1024: region counts / hot flags
+    int *ract;         // 1024: active-region flags
+    int *cnt;          // 16 ints: rotating list tails + control words
+    i64 *acc;          // 64 i64: rotating round accumulators + query totals
+    GroupBar *bar;     // group barrier
+    unsigned *clock;   // persistent stamp clock
+    int *meta;         // per-slot query meta (mask stamp, nv, s, t) for warm starts
+};
+
+// Options as seen by the kernel (resolved on the host).
+struct KOpts {
+    int K;
+    int gr_freq;
+    double gr_alpha;
+    int prune_mode;
+    int pp_switch;
+    int max_path;
+    int use_pp;
+    int use_hot;
+    int hot_k;
+    int use_rm;
+    int rm_freq;
+    int h_cut;
+    int stagnate;
+    int force_rm;
+    int force_pp;
+    i64 iter_max;
+};
+
+// Per-query outputs.
+struct QOut {
+    i64 flow;
+    i64 rounds;
+    i64 relabels;
+    i64 arcs_ex;
+    i64 verts_ex;
+    i64 pushes;
+    i64 rm_fixed;
+    i64 pp_rounds;
+    i64 hot_sweeps;
+    i64 deficit_phases;
+    i64 cut;
+    i64 mask_arcs;
+    int mask_n;
+    int status;
+};
+
+// One capacity change, resolved to an arc (region-ordered index).
+struct ArcUpdate {
+    int arc;
+    int pad;
+    i64 old_cap;
+    i64 new_cap;
+};
+
+enum KMode {
+    KM_SOLVE = 0,       // prune + solve
+    KM_PRUNE = 1,       // prune only; writes the 0/1 mask into dbg (n bytes, internal order)
+    KM_HEIGHTS = 2,     // prune + init + preflow + one global relabel; heights into dbg (ints)
+    KM_CERTIFY = 3,     // solve + return excess to source + certificate checks
+    KM_RESIDUAL = 4,    // solve, then write full-graph residuals into dbg (i64 per arc)
+    KM_REPAIR = 5,      // warm start from the slot's kept state after capacity updates
+};
+
+struct KParams {
+    const DGraph *graphs;
+    DSlot *slots;
+    int G;            // CTAs per query group
+    int nq;
+    const int *q_s;   // internal ids
+    const int *q_t;
+    const int *q_g;   // graph index per query (NULL = 0)
+    const int *q_slot;// slot per query (NULL = group id)
+    int *q_next;      // work queue head
+    QOut *out;
+    int *err;
+    u64 bar_limit_ns;
+    u64 time_limit_ns;  // per launch; 0 = none.  Past it the solve stops with MFD_TIMEOUT.
+    KOpts o;
+    int mode;
+    void *dbg;
+    const ArcUpdate *upd;
+    int nupd;
+    // serving ring (mode KM_SOLVE with ring != NULL): requests are read from
+    // ring_req[i] once ring_tail (host-written) exceeds i; completion flags.
+    volatile int *ring_tail;
+    const int4 *ring_req;        // (s, t, graph, unused)
+    volatile int *ring_done;     // 1 when the request finished
+    u64 *ring_t0;                // admission / completion timestamps (ns)
+    volatile int *ring_stop;     // host sets 1 to end the persistent kernel
+    u64 idle_limit_ns;
+};
+
+void mf_launch_kernel(const KParams &p, int grid, int threads, cudaStream_t st, bool cooperative,
+                      cudaError_t *err);
+int mf_kernel_max_blocks_per_sm(int threads);

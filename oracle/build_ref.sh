@@ -1,0 +1,19 @@
+#!/usr/bin/env bash
+# Compiles the reference's own CUDA solver from its sources where they lie
+# (read-only) into oracle/_ref/ra_ref, for sm_100a, with the device shim
+# above.  Nothing is copied out of the reference tree; the only output is the
+# executable.  Test infrastructure only: the engine never runs it.
+#   usage: oracle/build_ref.sh [reference_root]
+set -euo pipefail
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF="${1:-/root/reference}"
+SRC="$REF/Region_Aware_PR_with_Pruning_BoundaryCore.cu"
+if [ ! -f "$SRC" ]; then
+  echo "build_ref: $SRC not found; keeping any prebuilt oracle/_ref/ra_ref" >&2
+  exit 0
+fi
+mkdir -p "$HERE/_ref"
+NVCC="${NVCC:-nvcc}"
+"$NVCC" -O3 -gencode arch=compute_100a,code=sm_100a -cudart shared \
+  -o "$HERE/_ref/ra_ref" "$SRC" "$HERE/ref_device_shim.c" -ldl
+echo "build_ref: built $HERE/_ref/ra_ref"

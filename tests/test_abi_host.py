@@ -1,0 +1,86 @@
+"""CPU tests of the C ABI library: it loads, exports every entry point the
+header declares, and its host-only parts (generators, graph.txt reader and
+writer) behave as specified.  No GPU compute is called here."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "maxflow_b200.h")
+
+
+def header_functions():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(mf_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    import mscresearch_b200 as mf
+    from mscresearch_b200 import _capi
+    lib = C.CDLL(_capi.LIB_PATH)
+    names = header_functions()
+    assert len(names) >= 30
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(_capi.SIGNATURES), set(names) ^ set(_capi.SIGNATURES)
+    assert b"sm_100a" in mf.lib.mf_version()
+
+
+def test_opts_defaults_match_reference_knobs():
+    import mscresearch_b200 as mf
+    o = mf.opts()
+    assert (o.gr_freq, o.rm_freq, o.h_cut, o.stagnate_rounds) == (128, 64, 100, 128)
+    assert (o.path_push_switch, o.max_path_len, o.hot_regions) == (8, 256, 32)
+    assert o.iter_max == 20000000
+
+
+def test_generators_deterministic_and_in_range():
+    import mscresearch_b200 as mf
+    u, v, c = mf.gen_uniform(100, 5000, 1, 100, seed=3)
+    u2, v2, c2 = mf.gen_uniform(100, 5000, 1, 100, seed=3)
+    assert np.array_equal(u, u2) and np.array_equal(v, v2) and np.array_equal(c, c2)
+    assert (u != v).all() and u.min() >= 0 and u.max() < 100 and c.min() >= 1 and c.max() <= 100
+    a, b, w = mf.gen_rmat(12, 40000, seed=5)
+    assert (a != b).all() and a.max() < 4096 and w.min() >= 1 and w.max() <= 1000
+    assert len(a) < 40000  # self loops dropped
+    # power law: vertex 0 (quadrant a) is the top out-degree vertex
+    assert np.bincount(a).argmax() == 0
+    gu, gv, gc = mf.gen_grid(8, 6, seed=1)
+    S, T = 48, 49
+    nb = ((gu < 48) & (gv < 48)).sum()
+    assert nb == 2 * (7 * 6 + 8 * 5)
+    assert (((gu == S) & (gv < 48)) | ((gu < 48) & (gv == T))).sum() == 48
+    s, t = mf.gen_queries_hub(4096, a, b, 10, 10, seed=2)
+    assert (s != t).all()
+    dout = np.bincount(a, minlength=4096)
+    top = np.argsort(-dout, kind="stable")[:40]
+    assert set(s[:10]).issubset(set(top))
+
+
+def test_graph_txt_round_trip_matches_oracle_reader(tmp_path):
+    import mscresearch_b200 as mf
+    from oracle import oracle as O
+    u, v, c = mf.gen_uniform(50, 300, 1, 9, seed=1)
+    p = str(tmp_path / "graph.txt")
+    mf.write_graph_txt(p, 50, u, v, c)
+    n, a, b, w = mf.read_graph_txt(p)
+    assert n == 50 and np.array_equal(a, u) and np.array_equal(b, v) and np.array_equal(w, c)
+    n2, a2, b2, w2 = O.parse_graph(p)
+    assert np.array_equal(a, a2) and np.array_equal(b, b2) and np.array_equal(w, w2)
+    # malformed: reading stops at the first triple that does not scan (RA:1071)
+    q = tmp_path / "bad.txt"
+    q.write_text("5 6\n1 2 3\n  2   3\n4\n4 5 -7\n3 z 1\n1 5 2\n")
+    n, a, b, w = mf.read_graph_txt(str(q))
+    n2, a2, b2, w2 = O.parse_graph(str(q))
+    assert list(a) == list(a2) and list(w) == list(w2) and len(a) == 3
+
+
+def test_cli_usage_without_gpu():
+    import subprocess
+    import mscresearch_b200 as mf
+    r = subprocess.run([mf.CLI_PATH], capture_output=True, text=True)
+    assert r.returncode == 1 and "Usage" in r.stderr

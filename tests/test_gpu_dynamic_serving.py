@@ -1,0 +1,134 @@
+"""GPU tests of the resident-session (dynamic capacity) path, the
+continuous-batching server and the autotuner: every answer must equal a
+fresh exact solve of the same graph state."""
+import time
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+import mscresearch_b200 as mf  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+
+def apply_updates_oracle(g, fwd, u, v, d):
+    """Reference semantics of mf_update_caps on the oracle CSR (caller ids):
+    first forward arc u->v, cap += delta clamped at 0, applied in order."""
+    for a, b, x in zip(u, v, d):
+        if not (0 <= a < g.n and 0 <= b < g.n) or a == b:
+            continue
+        for e in range(g.row[a], g.row[a + 1]):
+            if g.col[e] == b and fwd[e]:
+                g.cap[e] = max(0, g.cap[e] + x)
+                break
+
+
+def make_updates(rng, u, v, k, n):
+    idx = rng.integers(0, len(u), k)
+    uu, vv = u[idx].copy(), v[idx].copy()
+    # a few pairs with no arc, a few repeated arcs
+    uu[: k // 50] = rng.integers(0, n, k // 50)
+    vv[: k // 50] = rng.integers(0, n, k // 50)
+    if k >= 4:
+        uu[-2:], vv[-2:] = uu[-4:-2], vv[-4:-2]
+    d = rng.integers(1, 101, k) * np.where(rng.random(k) < 0.5, -1, 1)
+    return uu, vv, d
+
+
+@pytest.mark.parametrize("scale", [10, 14])
+def test_session_incremental_equals_fresh(scale):
+    n = 1 << scale
+    u, v, c = mf.gen_rmat(scale, 16 * n, seed=31 + scale)
+    s, t = mf.gen_queries_hub(n, u, v, 6, 6, seed=8)
+    g = O.build_csr(n, u, v, c)
+    fwd = g.cap > 0
+    rng = np.random.default_rng(scale)
+    with mf.Graph.from_edges(n, u, v, c, R=32) as eg:
+        ss = mf.Session(eg, s, t)
+        f0 = ss.solve()
+        assert list(f0) == [O.dinic(g, a, b) for a, b in zip(s, t)]
+        for k in (10, 200, 3000):
+            uu, vv, d = make_updates(rng, u, v, k, n)
+            fr = ss.update(uu, vv, d)
+            apply_updates_oracle(g, fwd, uu, vv, d)
+            exp = [O.dinic(g, a, b) for a, b in zip(s, t)]
+            assert list(fr) == exp, k
+            # and a fresh static solve on the updated device graph agrees
+            assert list(eg.solve_batch(s, t)) == exp
+        ss.close()
+
+
+def test_update_caps_then_fresh_solve():
+    n = 2000
+    u, v, c = mf.gen_uniform(n, 12000, 1, 50, seed=2)
+    g = O.build_csr(n, u, v, c)
+    fwd = g.cap > 0
+    rng = np.random.default_rng(1)
+    with mf.Graph.from_edges(n, u, v, c, R=16) as eg:
+        uu, vv, d = make_updates(rng, u, v, 500, n)
+        skipped = eg.update_caps(uu, vv, d)
+        apply_updates_oracle(g, fwd, uu, vv, d)
+        assert skipped >= 1
+        ex = eg.export()
+        assert np.array_equal(np.sort(ex["cap"]), np.sort(g.cap))
+        for a, b in [(0, 1), (5, 77), (1999, 3)]:
+            assert eg.solve(a, b)[0] == O.dinic(g, a, b)
+
+
+def test_server_results_equal_alone_and_in_the_mix():
+    graphs, ocsr, queries = [], [], []
+    for i, scale in enumerate((10, 12, 13)):
+        n = 1 << scale
+        u, v, c = mf.gen_rmat(scale, 16 * n, seed=40 + i)
+        graphs.append(mf.Graph.from_edges(n, u, v, c, R=32))
+        ocsr.append(O.build_csr(n, u, v, c))
+        s, t = mf.gen_queries_hub(n, u, v, 8, 8, seed=50 + i)
+        queries.append((s, t))
+    # expected: each query alone (plain whole-GPU solve) and the oracle
+    alone = {}
+    for gi, (s, t) in enumerate(queries):
+        for a, b in zip(s, t):
+            alone[(gi, int(a), int(b))] = graphs[gi].solve(a, b)[0]
+            assert alone[(gi, int(a), int(b))] == O.dinic(ocsr[gi], a, b)
+    sv = mf.Server(graphs, mf.opts(group_ctas=2), max_slots=8)
+    assert 1 <= sv.slots <= 8
+    rng = np.random.default_rng(0)
+    reqs = [(gi, int(a), int(b)) for gi, (s, t) in enumerate(queries) for a, b in zip(s, t)]
+    order = rng.permutation(len(reqs))
+    tickets = []
+    for k, i in enumerate(order):
+        gi, a, b = reqs[i]
+        tickets.append((sv.submit(gi, a, b), reqs[i]))
+        if k % 7 == 3:
+            time.sleep(0.002)  # requests keep arriving while others run
+    sv.drain()
+    lat = []
+    for tk, key in tickets:
+        done, f, l, st = sv.poll(tk)
+        assert done and st == 0
+        assert f == alone[key], key
+        lat.append(l)
+    assert min(lat) >= 0
+    # a second wave after the persistent kernel went idle
+    time.sleep(0.5)
+    gi, a, b = reqs[0]
+    tk = sv.submit(gi, a, b)
+    sv.drain()
+    assert sv.poll(tk)[1] == alone[(gi, a, b)]
+    sv.close()
+    for g in graphs:
+        g.close()
+
+
+def test_autotune_consistent():
+    n = 1 << 12
+    u, v, c = mf.gen_rmat(12, 16 * n, seed=3)
+    s, t = mf.gen_queries_hub(n, u, v, 6, 6, seed=1)
+    g = O.build_csr(n, u, v, c)
+    exp = [O.dinic(g, a, b) for a, b in zip(s, t)]
+    with mf.Graph.from_edges(n, u, v, c, R=128) as eg:
+        best, R = eg.autotune(s, t)
+        assert R in (32, 64, 128, 256, 512)
+        assert eg.info[2] == R
+        assert list(eg.solve_batch(s, t, best)) == exp

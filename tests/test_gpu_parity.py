@@ -1,0 +1,214 @@
+"""GPU parity tests: the CUDA engine, called through its C ABI, against the
+CPU oracle on the same seeded inputs.  Integer results are compared exactly
+(max-flow values, masks, heights, CSR arrays, ids)."""
+import glob
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+import mscresearch_b200 as mf  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CASES = sorted(d for d in glob.glob(os.path.join(GOLDEN, "*")) if os.path.isdir(d))
+
+
+def oracle_flows(g, s, t):
+    return [O.dinic(g, a, b) if (0 <= a < g.n and 0 <= b < g.n and a != b) else 0 for a, b in zip(s, t)]
+
+
+@pytest.mark.parametrize("d", CASES, ids=[os.path.basename(x) for x in CASES])
+def test_golden_plain_and_batch(d):
+    exp = np.loadtxt(os.path.join(d, "expected.txt"), dtype=np.int64, ndmin=1)
+    s, t = O.parse_queries(os.path.join(d, "test.txt"))
+    R = 16 if "c1" in d else 128
+    with mf.Graph.load(os.path.join(d, "graph.txt"), R=R) as g:
+        for i, (a, b) in enumerate(zip(s, t)):
+            f, st = g.solve(a, b)
+            assert f == exp[i], (i, a, b)
+            assert st.status == 0
+        fb = g.solve_batch(s, t)
+        assert list(fb) == list(exp)
+
+
+@pytest.mark.parametrize("d", CASES, ids=[os.path.basename(x) for x in CASES])
+def test_golden_cli_res_mt(d):
+    exp = np.loadtxt(os.path.join(d, "expected.txt"), dtype=np.int64, ndmin=1)
+    with tempfile.TemporaryDirectory() as out:
+        for mode, extra, fname in (("static", (), "res_mt.txt"), ("static", ("--batch",), "res_mt.txt"),
+                                   ("dynamic", (), "res_dynamic.txt")):
+            rc, err = mf.run_cli(d, out, mode, extra, timeout=600)
+            assert rc == 0, err[-2000:]
+            res = np.loadtxt(os.path.join(out, fname), dtype=np.int64, ndmin=2)
+            assert res.shape == (len(exp), 2)
+            assert list(res[:, 0]) == list(exp)
+            assert (res[:, 1] >= 0).all()
+
+
+@pytest.mark.parametrize("R", [1, 16, 128, 300])
+def test_partition_reorder_bit_exact(R):
+    u, v, c = mf.gen_rmat(12, 30000, seed=11)
+    n = 4096
+    g = O.build_csr(n, u, v, c)
+    part, score = O.partition(g, min(R, n))
+    g2, new_id, old_id, rs = O.reorder(g, min(R, n), part)
+    with mf.Graph.from_edges(n, u, v, c, R=R) as eg:
+        ex = eg.export()
+    assert np.array_equal(ex["score"].view(np.int64), score.view(np.int64))
+    assert np.array_equal(ex["part"], part)
+    assert np.array_equal(ex["new_id"], new_id)
+    assert np.array_equal(ex["region_start"], rs)
+    assert np.array_equal(ex["row"], g2.row)
+    assert np.array_equal(ex["col"], g2.col)
+    assert np.array_equal(ex["cap"], g2.cap)
+    assert np.array_equal(ex["rev"], g2.rev)
+
+
+def test_partition_uniform_large_bit_exact():
+    # several chunks of the stable region placement and a non-power-of-2 n
+    u, v, c = mf.gen_uniform(50000, 300000, 1, 100, seed=2)
+    g = O.build_csr(50000, u, v, c)
+    part, score = O.partition(g, 128)
+    g2, new_id, _, rs = O.reorder(g, 128, part)
+    with mf.Graph.from_edges(50000, u, v, c, R=128) as eg:
+        ex = eg.export()
+    assert np.array_equal(ex["part"], part)
+    assert np.array_equal(ex["new_id"], new_id)
+    assert np.array_equal(ex["col"], g2.col) and np.array_equal(ex["rev"], g2.rev)
+
+
+@pytest.fixture(scope="module")
+def rmat14():
+    u, v, c = mf.gen_rmat(14, 1 << 18, seed=21)
+    n = 1 << 14
+    g = O.build_csr(n, u, v, c)
+    s, t = mf.gen_queries_hub(n, u, v, 12, 12, seed=4)
+    eg = mf.Graph.from_edges(n, u, v, c, R=64)
+    yield n, u, v, c, g, s, t, eg
+    eg.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_prune_masks_match_oracle(rmat14, mode):
+    n, u, v, c, g, s, t, eg = rmat14
+    for a, b in list(zip(s, t))[:10] + [(0, 1), (5, 5)]:
+        m = eg.prune_mask(a, b, mode)
+        if a == b:
+            assert m.sum() == 0
+            continue
+        assert np.array_equal(m, O.prune_mask(g, a, b, mode)), (a, b)
+
+
+def test_initial_heights_match_oracle_bfs(rmat14):
+    n, u, v, c, g, s, t, eg = rmat14
+    for a, b in list(zip(s, t))[:8]:
+        h = eg.initial_heights(a, b)
+        mk = O.prune_mask(g, a, b, 1)
+        sub, o2s, s2o = O.induced_subgraph(g, mk)
+        if mk[b] == 0 or sub.n == 0 or mk.sum() <= 2 and O.dinic(g, a, b) == 0:
+            continue
+        res = sub.cap.copy()
+        sa = o2s[a]
+        for e in range(sub.row[sa], sub.row[sa + 1]):
+            res[sub.rev[e]] += res[e]
+            res[e] = 0
+        blocked = np.zeros(sub.n, np.uint8)
+        blocked[sa] = 1
+        d = O.bfs_heights(sub, res, o2s[b], blocked=blocked)
+        exp = np.full(n, n, np.int32)
+        for i in range(sub.n):
+            exp[s2o[i]] = n if d[i] >= sub.n else d[i]
+        assert np.array_equal(h, exp), (a, b)
+
+
+def test_rmat_batch_plain_groups_match_dinic(rmat14):
+    n, u, v, c, g, s, t, eg = rmat14
+    exp = oracle_flows(g, s, t)
+    assert [eg.solve(a, b)[0] for a, b in zip(s, t)] == exp
+    for G in (1, 2, 4, 16):
+        assert list(eg.solve_batch(s, t, mf.opts(group_ctas=G))) == exp, G
+
+
+def test_residual_certified_by_oracle(rmat14):
+    n, u, v, c, g, s, t, eg = rmat14
+    ex = eg.export()
+    gi = O.CSR(n, ex["row"], ex["col"], ex["cap"], ex["rev"])
+    nid = ex["new_id"]
+    for a, b in list(zip(s, t))[:8]:
+        f, res, st = eg.solve_residual(a, b)
+        rc, cut = O.certify(gi, nid[a], nid[b], res, f, require_flow=False)
+        assert rc == 0 and cut == f, (a, b, rc, cut, f)
+
+
+def test_device_certificate(rmat14):
+    n, u, v, c, g, s, t, eg = rmat14
+    for a, b in list(zip(s, t))[:8]:
+        f, st = eg.certify(a, b)
+        assert st.status == 0 and st.cut_capacity == f == O.dinic(g, a, b)
+
+
+@pytest.mark.parametrize("kw", [
+    dict(use_rm=1, force_rm=1, rm_freq=1),
+    dict(use_path_push=1, force_path_push=1, path_push_switch=1 << 30),
+    dict(use_hot_sweep=1, hot_regions=2, kernel_cycles=1),
+    dict(use_rm=0, use_path_push=0, use_hot_sweep=0, gr_freq=1, gr_work_alpha=0.0),
+    dict(kernel_cycles=64, gr_freq=100000, gr_work_alpha=0.0),
+    dict(prune_mode=0),
+], ids=["rm", "path_push", "hot", "relabel_every_round", "rare_relabel", "ref_prune"])
+def test_heuristics_stay_exact(rmat14, kw):
+    n, u, v, c, g, s, t, eg = rmat14
+    exp = oracle_flows(g, s, t)
+    o = mf.opts(**kw)
+    assert list(eg.solve_batch(s, t, o)) == exp
+    f, st = eg.certify(s[0], t[0], o)
+    assert f == exp[0] and st.cut_capacity == f
+
+
+def test_random_small_graphs_edge_cases():
+    rng = np.random.default_rng(5)
+    for trial in range(40):
+        n = int(rng.integers(2, 60))
+        m = int(rng.integers(0, 400))
+        u = rng.integers(-2, n + 2, m)
+        v = rng.integers(-2, n + 2, m)
+        c = rng.integers(-5, 1000, m)
+        g = O.build_csr(n, u, v, c)
+        s = list(rng.integers(-1, n + 1, 6)) + [0, n - 1]
+        t = list(rng.integers(-1, n + 1, 6)) + [0, 0]
+        exp = oracle_flows(g, s, t)
+        with mf.Graph.from_edges(n, u, v, c, R=int(rng.integers(1, 20))) as eg:
+            assert list(eg.solve_batch(s, t)) == exp, trial
+            assert [eg.solve(a, b)[0] for a, b in zip(s, t)] == exp, trial
+
+
+def test_grid_segmentation():
+    W, H = 64, 48
+    u, v, c = mf.gen_grid(W, H, seed=9)
+    n = W * H + 2
+    g = O.build_csr(n, u, v, c)
+    s = [W * H, W * H, 3]
+    t = [W * H + 1, 100, W * H + 1]
+    exp = oracle_flows(g, s, t)
+    with mf.Graph.from_edges(n, u, v, c, R=32) as eg:
+        assert list(eg.solve_batch(s, t)) == exp
+        f, st = eg.certify(s[0], t[0])
+        assert f == exp[0] and st.cut_capacity == f
+
+
+def test_full_size_rmat20_properties():
+    """R-MAT n=2^20, 2^24 draws (the headline graph): batched == plain and
+    device-certified (zero-excess flow + equal-capacity cut) on a sample."""
+    u, v, c = mf.gen_rmat(20, 1 << 24, seed=1)
+    n = 1 << 20
+    s, t = mf.gen_queries_hub(n, u, v, 6, 6, seed=2)
+    with mf.Graph.from_edges(n, u, v, c, R=128) as eg:
+        fb = eg.solve_batch(s, t)
+        for i in (0, 1, 6):
+            f, st = eg.solve(s[i], t[i])
+            assert f == fb[i]
+            fc, stc = eg.certify(s[i], t[i])
+            assert fc == f and stc.cut_capacity == f and stc.status == 0
