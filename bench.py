@@ -1,0 +1,377 @@
+"""Benchmark: exact max-flow queries/s (+ p50/p99 latency), batched vs plain,
+on the R-MAT power-law workload (n = 2^20, 2^24 draws with
+(a,b,c,d) = (0.57,0.19,0.19,0.05), self loops dropped, capacities uniform
+in [1,1000], R = 128 regions, 256 queries: 128 between top-1% out-degree
+and top-1% in-degree vertices, 128 uniform; seeded synthetic data).
+
+One step = one batched persistent launch solving all 256 queries exactly
+(mf_solve_batch) on a device-resident graph.  `value` is device-timed
+(CUDA events around the launch, on its stream); `e2e` times the same public
+C-ABI call from host buffers (query upload + answers back) with a host clock.
+The graph (~0.9 GB) and the per-query residual slots (~0.3 GB each) exceed
+the 126 MB L2, so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+--impl reference runs the reference's own CUDA program (built from its
+sources by oracle/build_ref.sh into oracle/_ref/ra_ref) on the same graph
+and a bounded sample of the same queries, and reports its own per-query
+times (res_mt.txt, integer ms, prune included, RA:2808).
+Multi-GPU (torchrun): queries shard across ranks (one graph replica per
+GPU, no data-path collective); timing is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "exact max-flow queries/sec + p50/p99 latency, batched vs plain, same B200"
+WORKLOAD = "rmat20_256q"
+SCALE, DRAWS, NHUB, NUNI, R = 20, 1 << 24, 128, 128, 128
+GRAPH_SEED, QUERY_SEED = 1, 2
+QOUT_BYTES = 120  # device per-query record copied back by mf_solve_batch
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu=0):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu),
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 6:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = max(mx, float(f[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[2:6]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(rank=0):
+    import mscresearch_b200 as mf
+    u, v, c = mf.gen_rmat(SCALE, DRAWS, 0.57, 0.19, 0.19, 1, 1000, GRAPH_SEED)
+    n = 1 << SCALE
+    s, t = mf.gen_queries_hub(n, u, v, NHUB, NUNI, QUERY_SEED + 1000 * rank)
+    return n, u, v, c, s, t
+
+
+def pct(xs, q):
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, world
+
+
+def dist_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(n, u, v, c, s, t, budget_s=20.0):
+    """Oracle Dinic on the box's host cores over a bounded sample of the same
+    queries (hub and uniform alternating), queries spread over threads."""
+    from oracle import oracle as O
+    t0 = time.time()
+    g = O.build_csr(n, u, v, c)
+    build_s = time.time() - t0
+    threads = os.cpu_count() or 1
+    order = [i for pair in zip(range(NHUB), range(NHUB, NHUB + NUNI)) for i in pair]
+    done, flows, t_solve = 0, [], 0.0
+    k = max(threads, 4)
+    while done < len(order) and t_solve < budget_s:
+        idx = order[done:done + k]
+        t1 = time.time()
+        flows += list(O.dinic_batch(g, s[idx], t[idx], threads))
+        t_solve += time.time() - t1
+        done += len(idx)
+    return {"value": done / t_solve, "unit": "queries/s", "cores": threads, "kind": "port",
+            "sample": "%d of the 256 queries (alternating hub/uniform), C Dinic over %d threads, "
+                      "%.1f s solve (+%.1f s CSR build)" % (done, threads, t_solve, build_s)}, \
+        order[:done], flows
+
+
+def run_engine(args):
+    rank, world = dist_init(args)
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    import mscresearch_b200 as mf
+    n, u, v, c, s, t = make_workload(rank)
+    g = mf.Graph.from_edges(n, u, v, c, R=R)
+    _, arcs, _ = g.info
+    o = mf.opts(group_ctas=args.group)
+    nq = len(s)
+    # warm-up (also sizes the residual slot pool)
+    for _ in range(args.warmup):
+        g.solve_batch(s, t, o)
+    # ---- timed region: device-timed batched launches
+    dev_ms, stats_last = [], None
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        for k in range(args.steps):
+            flows, sts = g.solve_batch(s, t, o, with_stats=True)
+            dev_ms.append(g.last_device_ms)
+            stats_last = sts
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    step_ms = dist_max(float(np.mean(dev_ms)), world)
+    total_q = nq * world
+    value = total_q / (step_ms / 1e3)
+    # ---- e2e through the public C-ABI from host buffers (host clock)
+    e2e_ms = []
+    s_host, t_host = np.ascontiguousarray(s), np.ascontiguousarray(t)
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        g.solve_batch(s_host, t_host, o)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_step = dist_max(float(np.mean(e2e_ms)), world)
+    # ---- plain per-query solver on the same queries (drop-in path)
+    plain_ms, plain_flows = [], []
+    for a, b in zip(s, t):
+        f, st = g.solve(a, b)
+        plain_ms.append(st.time_ms)
+        plain_flows.append(f)
+    plain_total = dist_max(float(np.sum(plain_ms)), world)
+    assert list(plain_flows) == list(flows), "plain and batched answers differ"
+    # ---- served: Poisson arrivals at ~60% of batched capacity
+    served = None
+    if args.serve:
+        served = serve_run(mf, g, s, t, flows, o, rate=0.6 * nq / (step_ms / 1e3))
+    # roofline: algorithmic bytes = 16 B x (arc + vertex examinations)
+    ax = sum(x.arcs_examined for x in stats_last)
+    vx = sum(x.vertices_examined for x in stats_last)
+    alg_bytes = 16.0 * (ax + vx)
+    hbm, kind = peaks()
+    achieved = alg_bytes / (np.mean(dev_ms) / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "mf_kernel_rmat20_traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get("bytes_per_launch")
+    edges = sum(x.mask_arcs for x in stats_last)
+    finish = [x.finish_ms for x in stats_last]
+    res = {
+        "metric": METRIC, "value": round(value, 3), "unit": "queries/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded R-MAT 2^20, 2^24 draws, caps U[1,1000]; 128 hub + 128 uniform queries)",
+        "config": {"workload": WORKLOAD, "n": n, "edges": len(u), "arcs": arcs, "queries_per_gpu": nq,
+                   "R": R, "prune": "fwd(s) & bwd(t)", "group_ctas": o.group_ctas,
+                   "l2": "inputs larger than L2 (graph %.2f GB, residual slot %.2f GB)" % (
+                       arcs * 20 / 1e9, arcs * 8 / 1e9),
+                   "parallelism": "query shards, graph replica per GPU"},
+        "e2e": {"value": round(total_q / (e2e_step / 1e3), 3), "unit": "queries/s",
+                "h2d_bytes_per_step": 12 * nq, "d2h_bytes_per_step": QOUT_BYTES * nq + 8},
+        "gpu_launches": 2 * args.steps,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "traffic": traffic,
+                     "peak_kind": kind, "alg_bytes_per_launch": alg_bytes},
+        "batched": {"qps": round(value, 3), "p50_ms": pct(finish, 50), "p99_ms": pct(finish, 99),
+                    "edges_per_s": edges / (np.mean(dev_ms) / 1e3)},
+        "plain": {"qps": round(total_q / (plain_total / 1e3), 3), "p50_ms": pct(plain_ms, 50),
+                  "p99_ms": pct(plain_ms, 99)},
+        "clocks": clk.summary(),
+    }
+    if served:
+        res["served"] = served
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cb, idx, cflows = cpu_baseline(n, u, v, c, s, t, budget_s=args.cpu_budget)
+        assert [int(flows[i]) for i in idx] == [int(x) for x in cflows], "engine differs from oracle"
+        res["cpu_baseline"] = cb
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    g.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def serve_run(mf, g, s, t, flows, o, rate, nreq=256, seed=0):
+    """Continuous batching: requests arrive by a Poisson process; latency is
+    host-measured from submission to the answer being visible."""
+    sv = mf.Server([g], o)
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, nreq)
+    idx = rng.integers(0, len(s), nreq)
+    sub_t, tickets = [], []
+    t0 = time.perf_counter()
+    nxt = t0
+    done_t = {}
+    for k in range(nreq):
+        nxt += gaps[k]
+        while time.perf_counter() < nxt:
+            for tk in tickets:
+                if tk not in done_t and sv.poll(tk)[0]:
+                    done_t[tk] = time.perf_counter()
+        sub_t.append(time.perf_counter())
+        tickets.append(sv.submit(0, int(s[idx[k]]), int(t[idx[k]])))
+    while len(done_t) < nreq:
+        for tk in tickets:
+            if tk not in done_t and sv.poll(tk)[0]:
+                done_t[tk] = time.perf_counter()
+    wall = time.perf_counter() - t0
+    lat = [(done_t[tk] - sub_t[i]) * 1e3 for i, tk in enumerate(tickets)]
+    exact = all(sv.poll(tk)[1] == int(flows[idx[i]]) for i, tk in enumerate(tickets))
+    slots = sv.slots
+    sv.close()
+    assert exact, "served answers differ from the batched ones"
+    return {"arrival_rate_qps": round(rate, 2), "requests": nreq, "qps": round(nreq / wall, 3),
+            "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "slots": slots, "exact": exact}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    if not os.path.exists(O.REF_BIN):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ra_ref not built "
+                          "(needs the reference sources; oracle/build_ref.sh)"}))
+        return
+    import mscresearch_b200 as mf
+    n, u, v, c, s, t = make_workload(0)
+    per_step = args.ref_queries_per_step
+    nsteps = args.warmup + args.steps
+    order = [i for pair in zip(range(NHUB), range(NHUB, NHUB + NUNI)) for i in pair]
+    idx = order[: per_step * nsteps]
+    d = tempfile.mkdtemp()
+    out = os.path.join(d, "out")
+    mf.write_graph_txt(os.path.join(d, "graph.txt"), n, u, v, c)
+    mf.write_test_txt(os.path.join(d, "test.txt"), s[idx], t[idx])
+    t0 = time.time()
+    with ClockSampler(0) as clk:
+        r = subprocess.run(["timeout", str(args.ref_timeout), O.REF_BIN, d, out, "static"],
+                           capture_output=True, text=True)
+    wall = time.time() - t0
+    if r.returncode != 0 or not os.path.exists(os.path.join(out, "res_mt.txt")):
+        print(json.dumps({"impl": "reference", "unavailable": "reference run failed (rc %d): %s" % (
+            r.returncode, r.stderr.strip().splitlines()[-1] if r.stderr.strip() else "")}))
+        return
+    res = np.loadtxt(os.path.join(out, "res_mt.txt"), dtype=np.int64, ndmin=2)
+    times = res[:, 1].astype(np.float64)
+    timed = times[args.warmup * per_step:]
+    ms_step = float(np.mean([timed[i * per_step:(i + 1) * per_step].sum() for i in range(args.steps)]))
+    value = per_step / (ms_step / 1e3) if ms_step > 0 else None
+    sample = "%d queries (alternating hub/uniform of the 256), %d per step; reference's own per-query " \
+             "times from res_mt.txt (integer ms, prune included, upload excluded); run wall %.1f s" % (
+                 len(idx), per_step, wall)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic (seeded R-MAT 2^20, 2^24 draws, caps U[1,1000])",
+            "config": {"workload": WORKLOAD, "n": n, "edges": len(u), "queries_sampled": len(idx), "R": 128},
+            "p50_ms": pct(timed, 50), "p99_ms": pct(timed, 99),
+            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": 1, "kind": "reference",
+                             "sample": sample + "; the reference is a CUDA program: host prune on 1 core "
+                                                "+ kernels on the B200"},
+            "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "clocks": clk.summary()}
+    if args.check:
+        from oracle import oracle as O2
+        g = O2.build_csr(n, u, v, c)
+        exp = O2.dinic_batch(g, s[idx], t[idx], os.cpu_count() or 1)
+        line["flows_match_oracle"] = int((res[:, 0] == exp).sum())
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--group", type=int, default=2)
+    ap.add_argument("--serve", type=int, default=1)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--ref-queries-per-step", type=int, default=2)
+    ap.add_argument("--ref-timeout", type=int, default=900)
+    ap.add_argument("--check", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

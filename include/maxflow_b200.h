@@ -83,7 +83,10 @@ typedef struct mf_stats {
     long long hot_sweeps;
     long long deficit_phases; /* times the solver drained deficits back to the sink */
     long long cut_capacity;   /* certify only: capacity of the residual s-t cut */
-    double time_ms;           /* device time of the solve (single-query calls) */
+    double time_ms;           /* device time of the launch (single-query calls) */
+    double service_ms;        /* device time from the query's start to its answer */
+    double finish_ms;         /* batched calls: device time from the launch's first
+                                 query start to this query's answer */
 } mf_stats;
 
 void mf_opts_default(mf_opts *o);

@@ -8,7 +8,9 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libmfb200.so")
+# MF_LIB_VARIANT=chk selects the self-check build (traces + index checks)
+LIB_PATH = os.path.join(_HERE, "libmfb200_chk.so" if os.environ.get("MF_LIB_VARIANT") == "chk"
+                        else "libmfb200.so")
 
 i32p = C.POINTER(C.c_int32)
 i64p = C.POINTER(C.c_int64)
@@ -58,6 +60,8 @@ class MfStats(C.Structure):
         ("deficit_phases", C.c_longlong),
         ("cut_capacity", C.c_longlong),
         ("time_ms", C.c_double),
+        ("service_ms", C.c_double),
+        ("finish_ms", C.c_double),
     ]
 
 

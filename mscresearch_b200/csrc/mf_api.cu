@@ -483,8 +483,10 @@ int launch(mf_graph *g, SlotPool &pool, int nq, const int *s_int, const int *t_i
     return MF_OK;
 }
 
-void fill_stats(mf_stats *st, const QOut &q, double ms) {
+void fill_stats(mf_stats *st, const QOut &q, double ms, u64 launch_t0) {
     memset(st, 0, sizeof(*st));
+    st->service_ms = (double)(q.t_done - q.t_begin) * 1e-6;
+    st->finish_ms = launch_t0 ? (double)(q.t_done - launch_t0) * 1e-6 : 0.0;
     st->flow = q.flow;
     st->status = status_from_err(q.status);
     st->mask_vertices = q.mask_n;
@@ -724,9 +726,11 @@ static int solve_common(mf_graph *g, int nq, const int32_t *s, const int32_t *t,
     int rc = launch(g, g->pool, nq, si.data(), ti.data(), false, o, mode, dbg, nullptr, 0, G, outs.data());
     if (rc) return rc;
     int worst = MF_OK;
+    u64 t0min = ~0ull;
+    for (int i = 0; i < nq; ++i) t0min = std::min(t0min, outs[i].t_begin);
     for (int i = 0; i < nq; ++i) {
         flows[i] = outs[i].flow;
-        if (stats) fill_stats(&stats[i], outs[i], single ? g->last_ms : 0.0);
+        if (stats) fill_stats(&stats[i], outs[i], single ? g->last_ms : 0.0, t0min);
         int st = status_from_err(outs[i].status);
         if (st != MF_OK && worst == MF_OK) worst = st;
         if (o.verbose)
@@ -935,7 +939,7 @@ static int session_run(mf_session *ss, int mode, const ArcUpdate *d_upd, int nup
     int worst = MF_OK;
     for (int i = 0; i < ss->nq; ++i) {
         if (flows) flows[i] = outs[i].flow;
-        if (stats) fill_stats(&stats[i], outs[i], 0.0);
+        if (stats) fill_stats(&stats[i], outs[i], 0.0, 0);
         int st = status_from_err(outs[i].status);
         if (st != MF_OK && worst == MF_OK) worst = st;
     }

@@ -28,6 +28,45 @@ __device__ __forceinline__ int ldcg(const int *p) { return __ldcg(p); }
 __device__ __forceinline__ unsigned ldcg(const unsigned *p) { return __ldcg(p); }
 __device__ __forceinline__ i64 ldcg(const i64 *p) { return __ldcg(p); }
 
+// ---------------------------------------------------------------------------
+// Self-check builds (-DMF_CHECKS, libmfb200_chk.so): every warp records the
+// last site it reached into host-mapped memory (readable after a failed
+// launch), and list/vertex indices are range-checked; a bad index is recorded
+// and the access skipped.  Production builds compile these to nothing.
+#ifdef MF_CHECKS
+struct MfChk {
+    volatile unsigned *trace;  // [warp][4]: site, aux, count, -
+    volatile int *bad;         // [0]: count, [1]: site, [2]: index, [3]: limit
+};
+static __device__ MfChk g_chk;  // per translation unit (no -rdc); the solver TU installs it
+__device__ __forceinline__ void mf_trace(int site, int aux) {
+    if (g_chk.trace && (threadIdx.x & 31) == 0) {
+        unsigned w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        g_chk.trace[4 * w + 0] = site;
+        g_chk.trace[4 * w + 1] = (unsigned)aux;
+        g_chk.trace[4 * w + 2] += 1;
+        __threadfence_system();
+    }
+}
+__device__ __forceinline__ bool mf_ok_idx(long long i, long long lim, int site) {
+    if (i >= 0 && i < lim) return true;
+    if (g_chk.bad) {
+        if (atomicAdd((int *)&g_chk.bad[0], 1) == 0) {
+            g_chk.bad[1] = site;
+            g_chk.bad[2] = (int)i;
+            g_chk.bad[3] = (int)lim;
+        }
+        __threadfence_system();
+    }
+    return false;
+}
+#define MF_TRACE(site, aux) mf_trace((site), (int)(aux))
+#define MF_OK_IDX(i, lim, site) mf_ok_idx((i), (lim), (site))
+#else
+#define MF_TRACE(site, aux) ((void)0)
+#define MF_OK_IDX(i, lim, site) true
+#endif
+
 __device__ __forceinline__ i64 atomic_add_i64(i64 *p, i64 v) {
     return (i64)atomicAdd(reinterpret_cast<u64 *>(p), (u64)v);
 }
@@ -64,14 +103,17 @@ __device__ __forceinline__ i64 warp_sum_i64(i64 x) {
 // Warp-aggregated append: every lane with flag != 0 writes val to
 // list[base + rank]; one atomicAdd per warp on *tail.  Must be called by all
 // 32 lanes.
-__device__ __forceinline__ void warp_append(bool flag, int val, int *list, int *tail) {
+__device__ __forceinline__ void warp_append(bool flag, int val, int *list, int *tail, int cap = 0x7fffffff) {
     unsigned b = __ballot_sync(MF_FULL, flag);
     if (b == 0) return;
     int leader = __ffs(b) - 1;
     int base = 0;
     if (lane_id() == leader) base = atomicAdd(tail, __popc(b));
     base = __shfl_sync(MF_FULL, base, leader);
-    if (flag) list[base + __popc(b & lanemask_lt())] = val;
+    if (flag) {
+        int pos = base + __popc(b & lanemask_lt());
+        if (MF_OK_IDX(pos, cap, 90)) list[pos] = val;
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -32,6 +32,7 @@
 #include "mf_solver.cuh"
 
 #include <climits>
+#include <cstring>
 
 // cnt[0..7]: list tails, handed out in rotation; taking bank k zeroes bank
 // k+4 (mod 8), which was last read at least one group barrier earlier (no
@@ -85,6 +86,7 @@ struct QCtx {
     bool leader;
     u64 t_start;
     u64 time_limit;
+    u64 q_begin;
     // per-warp counters (flushed at the end of the query)
     i64 w_arcs, w_verts, w_push;
 
@@ -130,8 +132,10 @@ template <class Claim>
 __device__ bool bfs_levels(QCtx &c, int *Q, int bank, int hi, Claim cl, int *levels_out) {
     int lo = 0, level = 0;
     while (lo < hi) {
+        MF_TRACE(10, level);
         for (int i = lo + c.gw; i < hi; i += c.gW) {
             int v = ldcg(&Q[i]);
+            if (!MF_OK_IDX(v, c.n, 11)) continue;
             int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
             for (int base = b; base < e1; base += 32) {
                 int e = base + c.lane;
@@ -141,7 +145,7 @@ __device__ bool bfs_levels(QCtx &c, int *Q, int bank, int hi, Claim cl, int *lev
                     w = ldro(&c.col[e]);
                     ok = cl(v, e, w, level);
                 }
-                warp_append(ok, w, Q, &c.st.cnt[bank]);
+                warp_append(ok, w, Q, &c.st.cnt[bank], c.n);
             }
             if (c.lane == 0) {
                 c.w_arcs += e1 - b;
@@ -164,6 +168,7 @@ __device__ bool bfs_levels(QCtx &c, int *Q, int bank, int hi, Claim cl, int *lev
 // reachable from s, in which case the flow is 0).
 __device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, int &nv,
                       bool &t_reach) {
+    MF_TRACE(20, s);
     // forward BFS from s over cap > 0
     int bank = c.take_bank();
     if (c.leader) {
@@ -233,7 +238,7 @@ __device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, i
             keep = (ldcg(&qm[v]) == M) || v == s;
             if (keep) mark[v] = M;
         }
-        warp_append(keep, v, c.st.vlist, &c.st.cnt[vb]);
+        warp_append(keep, v, c.st.vlist, &c.st.cnt[vb], c.n);
     }
     if (!c.sync()) return false;
     if (c.leader && !t_reach) {
@@ -251,6 +256,7 @@ __device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, i
 // Fresh residual state over the kept vertices: excess 0; res[e] = cap[e]
 // when the head is kept, else 0 (the arc is outside the induced subgraph).
 __device__ bool init_state(QCtx &c, int nv, unsigned M) {
+    MF_TRACE(30, nv);
     i64 mask_arcs = 0;
     for (int i = c.gw; i < nv; i += c.gW) {
         int v = ldcg(&c.st.vlist[i]);
@@ -275,6 +281,7 @@ __device__ bool init_state(QCtx &c, int nv, unsigned M) {
 
 // Saturate every residual arc out of s (RA:173-200; parallel over arcs).
 __device__ bool preflow(QCtx &c, int s) {
+    MF_TRACE(31, s);
     int b = ldro(&c.row[s]), e1 = ldro(&c.row[s + 1]);
     int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
     for (int e = b + gt; e < e1; e += gT) {
@@ -298,6 +305,7 @@ __device__ bool preflow(QCtx &c, int s) {
 // Returns counts in na / nd (active / deficits).
 __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int blockv, int srcv,
                                bool deficit_seeds, int *L, int &na, int &nd, i64 *&ab) {
+    MF_TRACE(40, nv);
     unsigned cur = ++c.clock;
     int qbk = c.take_bank();
     const int n = c.n;
@@ -316,7 +324,7 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
                 c.st.h[v] = 0;
             }
         }
-        warp_append(seed, v, c.st.qa, &c.st.cnt[qbk]);
+        warp_append(seed, v, c.st.qa, &c.st.cnt[qbk], c.n);
     }
     int hi = 0;
     if (!c.sync_tail(qbk, hi)) return false;
@@ -335,6 +343,7 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
     if (!bfs_levels(c, c.st.qa, qbk, hi, relab, nullptr)) return false;
 
     // sweep: heights of unreached vertices, active list, counts
+    MF_TRACE(41, 0);
     int lbk = c.take_bank();
     ab = c.take_abank();
     i64 l_sum = 0, l_high = 0, l_def = 0;
@@ -362,7 +371,7 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
             }
             if (ev < 0 && v != srcv && v != blockv) ++l_def;
         }
-        warp_append(act, v, L, &c.st.cnt[lbk]);
+        warp_append(act, v, L, &c.st.cnt[lbk], c.n);
     }
     l_sum = warp_sum_i64(l_sum);
     l_def = warp_sum_i64(l_def);
@@ -405,8 +414,20 @@ __device__ __forceinline__ bool enlist(QCtx &c, int w, unsigned rstamp) {
 __device__ void discharge_vertex(QCtx &c, int v, int K, int sinkv, int blockv, int *N, int nbk,
                                  unsigned rstamp, i64 *ab) {
     const int n = c.n;
-    int hv = ldcg(&c.st.h[v]);
-    i64 ev = ldcg(&c.st.ex[v]);
+    MF_TRACE(50, v);
+    // Height and excess steer warp-wide branches below: read them once on
+    // lane 0 and broadcast.  Under independent thread scheduling the lanes
+    // of a warp need not load at the same moment, and another warp may change
+    // h[v] / ex[v] in between; per-lane copies could then disagree and split
+    // the warp across full-mask shuffles.
+    int hv = 0;
+    i64 ev = 0;
+    if (c.lane == 0) {
+        hv = ldcg(&c.st.h[v]);
+        ev = ldcg(&c.st.ex[v]);
+    }
+    hv = __shfl_sync(MF_FULL, hv, 0);
+    ev = __shfl_sync(MF_FULL, ev, 0);
     int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
     i64 pushes = 0, arcs = 0;
     for (int cyc = 0; cyc < K; ++cyc) {
@@ -440,7 +461,7 @@ __device__ void discharge_vertex(QCtx &c, int v, int K, int sinkv, int blockv, i
             }
             if (r - d > 0) minh = min(minh, hw);
             bool add = act && enlist(c, w, rstamp);
-            warp_append(add, w, N, &c.st.cnt[nbk]);
+            warp_append(add, w, N, &c.st.cnt[nbk], c.n);
             arcs += min(32, e1 - base);
             if (rem == 0) break;
         }
@@ -455,8 +476,9 @@ __device__ void discharge_vertex(QCtx &c, int v, int K, int sinkv, int blockv, i
         ev = ldcg(&c.st.ex[v]);
         ev = __shfl_sync(MF_FULL, ev, 0);
     }
+    MF_TRACE(51, v);
     bool again = (c.lane == 0) && ev > 0 && hv < n && enlist(c, v, rstamp);
-    warp_append(again, v, N, &c.st.cnt[nbk]);
+    warp_append(again, v, N, &c.st.cnt[nbk], c.n);
     if (c.lane == 0) {
         c.w_arcs += arcs;
         c.w_verts += 1;
@@ -472,6 +494,7 @@ __device__ void discharge_vertex(QCtx &c, int v, int K, int sinkv, int blockv, i
 __device__ void path_push_vertex(QCtx &c, int v, int max_path, int sinkv, int blockv, int *N,
                                  int nbk, unsigned rstamp, unsigned pstamp, i64 *ab) {
     const int n = c.n;
+    MF_TRACE(60, v);
     bool own = false;
     if (c.lane == 0) own = atomicMax(&c.st.claim[v], pstamp) < pstamp;
     own = __shfl_sync(MF_FULL, own, 0);
@@ -561,6 +584,7 @@ __device__ void path_push_vertex(QCtx &c, int v, int max_path, int sinkv, int bl
 // top-K regions with a non-zero count become hot.  CTA 0 of the group
 // bitonic-sorts (count desc, region asc) in shared memory.
 __device__ bool select_hot(QCtx &c, const int *N, int nN, int hot_k) {
+    MF_TRACE(70, nN);
     const int R = c.R;
     int *hot = c.st.hot;
     int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
@@ -615,12 +639,15 @@ __device__ bool select_hot(QCtx &c, const int *N, int nN, int hot_k) {
 __device__ bool rm_pass(QCtx &c, int nv, unsigned M, int hlo, int hhi, int s, int t, int *N,
                         int nbk, unsigned rstamp, i64 *ab) {
     const int n = c.n;
+    MF_TRACE(80, nv);
     i64 fixed = 0;
     for (int i = c.gw; i < nv; i += c.gW) {
         int v = ldcg(&c.st.vlist[i]);
         if (v == s || v == t) continue;
         if (!ldcg(&c.st.ract[ldro(&c.rof[v])])) continue;
-        int hv = ldcg(&c.st.h[v]);
+        int hv = 0;
+        if (c.lane == 0) hv = ldcg(&c.st.h[v]);
+        hv = __shfl_sync(MF_FULL, hv, 0);
         if (hv < hlo || hv > hhi || hv >= n) continue;
         int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
         i64 gained = 0;
@@ -651,7 +678,7 @@ __device__ bool rm_pass(QCtx &c, int nv, unsigned M, int hlo, int hhi, int s, in
             add = old <= 0 && old + gained > 0 && enlist(c, v, rstamp);
             if (!add && old > 0) add = enlist(c, v, rstamp);
         }
-        warp_append(add, v, N, &c.st.cnt[nbk]);
+        warp_append(add, v, N, &c.st.cnt[nbk], c.n);
         if (c.lane == 0) {
             c.w_arcs += e1 - b;
             c.w_verts += 1;
@@ -722,6 +749,7 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
             if (c.leader && c.time_limit && globaltimer_ns() - c.t_start > c.time_limit)
                 atomicCAS(c.err, 0, MFD_TIMEOUT);
             // ---- one discharge round over L -> N
+            MF_TRACE(45, (int)round);
             unsigned rstamp = ++c.clock;
             int nbk = c.take_bank();
             i64 *rb = c.take_abank();
@@ -768,8 +796,11 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
                 }
                 qo.pp_rounds++;
             } else {
-                for (int i = c.gw; i < na; i += c.gW)
-                    discharge_vertex(c, ldcg(&L[i]), K, sinkv, blockv, N, nbk, rstamp, rb);
+                for (int i = c.gw; i < na; i += c.gW) {
+                    int v = ldcg(&L[i]);
+                    if (!MF_OK_IDX(v, n, 12)) continue;
+                    discharge_vertex(c, v, K, sinkv, blockv, N, nbk, rstamp, rb);
+                }
             }
             // clear region scratch for this round's optional passes
             {
@@ -779,7 +810,9 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
                     c.st.ract[r] = 0;
                 }
             }
+            MF_TRACE(46, (int)round);
             if (!c.sync()) return false;
+            MF_TRACE(47, (int)round);
             int nN = ldcg(&c.st.cnt[nbk]);
             i64 sum = ldcg(&rb[A_SUMEX]);
             i64 high = ldcg(&rb[A_HIGH]);
@@ -999,7 +1032,7 @@ __device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int
             v = ldcg(&c.st.qb[i]);
             add = ldcg(&claim[v]) != O;
         }
-        warp_append(add, v, c.st.vlist, &c.st.cnt[addb]);
+        warp_append(add, v, c.st.vlist, &c.st.cnt[addb], c.n);
     }
     if (!c.sync()) return false;
     nv = ldcg(&c.st.cnt[addb]);
@@ -1065,6 +1098,7 @@ __device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int
 
 // ---------------------------------------------------------------------------
 __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
+    MF_TRACE(2, q);
     QOut qo = {};
     int status = MFD_OK;
     const KOpts &o = p.o;
@@ -1141,6 +1175,7 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
             if (!c.sync()) return;
         }
     }
+    MF_TRACE(90, q);
     c.flush_warp_counts();
     if (!c.sync()) return;
     if (c.leader) {
@@ -1152,6 +1187,8 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
         qo.arcs_ex = tot[T_ARCS];
         qo.verts_ex = tot[T_VERTS];
         qo.pushes = tot[T_PUSH];
+        qo.t_begin = c.q_begin;
+        qo.t_done = globaltimer_ns();
         p.out[q] = qo;
         c.st.meta[0] = (int)M;
         c.st.meta[1] = nv;
@@ -1179,6 +1216,7 @@ __global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
     c.time_limit = p.time_limit_ns;
     DSlot gslot = p.slots[gid];
     c.bar = gslot.bar;
+    MF_TRACE(1, gid);
     for (;;) {
         // take a query (group leader), broadcast through the group slot
         int *qcell = gslot.cnt + CNT_Q;
@@ -1240,9 +1278,11 @@ __global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
         c.cap = g.cap;
         c.st = p.slots[si];
         c.clock = ldcg(c.st.clock);
+        c.q_begin = globaltimer_ns();
         if (s < 0 || t < 0 || s >= g.n || t >= g.n || s == t) {
             if (c.leader) {
                 QOut z = {};
+                z.t_begin = z.t_done = c.q_begin;
                 p.out[q] = z;
             }
         } else {
@@ -1259,8 +1299,39 @@ __global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
     }
 }
 
+#ifdef MF_CHECKS
+
+static unsigned *h_chk_trace = nullptr;
+static int *h_chk_bad = nullptr;
+static int h_chk_warps = 0;
+extern "C" int mf_chk_host_buffers(unsigned **trace, int **bad, int *nwarps) {
+    *trace = h_chk_trace;
+    *bad = h_chk_bad;
+    *nwarps = h_chk_warps;
+    return h_chk_trace ? 0 : 1;
+}
+static void mf_chk_install(int warps) {
+    if (h_chk_trace && warps <= h_chk_warps) {
+        memset(h_chk_trace, 0, sizeof(unsigned) * 4 * h_chk_warps);
+        return;
+    }
+    cudaHostAlloc((void **)&h_chk_trace, sizeof(unsigned) * 4 * warps, cudaHostAllocMapped);
+    cudaHostAlloc((void **)&h_chk_bad, sizeof(int) * 4, cudaHostAllocMapped);
+    memset(h_chk_trace, 0, sizeof(unsigned) * 4 * warps);
+    memset(h_chk_bad, 0, sizeof(int) * 4);
+    h_chk_warps = warps;
+    MfChk c;
+    cudaHostGetDevicePointer((void **)&c.trace, h_chk_trace, 0);
+    cudaHostGetDevicePointer((void **)&c.bad, h_chk_bad, 0);
+    cudaMemcpyToSymbol(g_chk, &c, sizeof(c));
+}
+#endif
+
 void mf_launch_kernel(const KParams &p, int grid, int threads, cudaStream_t st, bool cooperative,
                       cudaError_t *err) {
+#ifdef MF_CHECKS
+    mf_chk_install(grid * threads / 32);
+#endif
     void *args[] = {(void *)&p};
     if (cooperative)
         *err = cudaLaunchCooperativeKernel((void *)mf_kernel, dim3(grid), dim3(threads), args, 0, st);

@@ -69,6 +69,8 @@ struct QOut {
     i64 deficit_phases;
     i64 cut;
     i64 mask_arcs;
+    u64 t_begin;   // globaltimer ns when the group took the query
+    u64 t_done;    // globaltimer ns when its answer was written
     int mask_n;
     int status;
 };

@@ -136,21 +136,30 @@ def write_case(name, fn):
 
 
 def run_ref(d, timeout=300):
+    """Run the reference program in static and dynamic mode; keep its result
+    files and its per-query log lines (prune / upload sizes)."""
     if not os.path.exists(O.REF_BIN):
         raise SystemExit("reference build missing: run oracle/build_ref.sh first")
-    out = tempfile.mkdtemp()
-    try:
-        r = subprocess.run(["timeout", str(timeout), O.REF_BIN, d, out, "static"], capture_output=True,
-                           text=True)
-        if r.returncode != 0:
-            print("reference failed on %s (rc %d): %s" % (d, r.returncode, r.stderr[-400:]))
-            return False
-        shutil.copy(os.path.join(out, "res_mt.txt"), os.path.join(d, "ref_res_mt.txt"))
-        with open(os.path.join(d, "ref_stderr_tail.txt"), "w") as f:
-            f.write("\n".join(r.stderr.splitlines()[-5:]) + "\n")
-        return True
-    finally:
-        shutil.rmtree(out, ignore_errors=True)
+    ok = True
+    for mode, res_name, out_name in (("static", "res_mt.txt", "ref_res_mt.txt"),
+                                     ("dynamic", "res_dynamic.txt", "ref_res_dynamic.txt")):
+        out = tempfile.mkdtemp()
+        try:
+            r = subprocess.run(["timeout", str(timeout), O.REF_BIN, d, out, mode], capture_output=True,
+                               text=True)
+            if r.returncode != 0:
+                print("reference %s failed on %s (rc %d): %s" % (mode, d, r.returncode, r.stderr[-400:]))
+                ok = False
+                continue
+            shutil.copy(os.path.join(out, res_name), os.path.join(d, out_name))
+            keep = [l for l in r.stderr.splitlines()
+                    if l.startswith("[QueryPrune") or l.startswith("[Static]") or l.startswith("[Dynamic] Query")
+                    or l.startswith("Graph (") or l.startswith("Exceeded")]
+            with open(os.path.join(d, "ref_log_%s.txt" % mode), "w") as f:
+                f.write("\n".join(keep) + "\n")
+        finally:
+            shutil.rmtree(out, ignore_errors=True)
+    return ok
 
 
 def main():
