@@ -1194,7 +1194,6 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
         c.st.meta[1] = nv;
         c.st.meta[2] = s;
         c.st.meta[3] = t;
-        *c.st.clock = c.clock;
     }
     c.sync();
 }
@@ -1287,6 +1286,9 @@ __global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
             }
         } else {
             solve_query(c, p, q, s, t);
+            // every path through solve_query consumed stamps: persist the
+            // clock so the slot's next query never reuses one
+            if (c.leader) *c.st.clock = c.clock;
         }
         if (*(volatile int *)p.err) return;
         if (p.ring_tail && c.leader) {
