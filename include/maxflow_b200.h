@@ -150,6 +150,26 @@ int mf_solve_residual(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, in
 int mf_certify(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, int64_t *flow,
                mf_stats *stats);
 
+/* Allocation-free solve.  No counterpart in the reference (its every solve
+ * allocates per-query state, RA:1336-1372).  For callers that may not
+ * allocate device memory where they need a flow — a framework that owns the
+ * device memory pool, a service that reserves everything at start-up and
+ * must not let cudaMalloc synchronize the device on the request path, a
+ * plugin handed only device pointers.  The caller passes a paired-arc CSR
+ * already in device memory (d_row: n+1 offsets; d_col/d_rev/d_cap: arcs
+ * entries, any vertex order, rev pairing each arc with its reverse) and gets
+ * the exact max flow from s to t in *flow (host).  Scratch is a fixed
+ * file-scope device array of about 11 MB sized for n <= 65536 vertices and
+ * arcs <= 1048576; larger graphs are rejected with MF_ERR_ARG.  The call
+ * makes no cudaMalloc / cudaFree or other allocating call.  Its first call on
+ * a device resolves the array's device address and zeroes it; make that first
+ * call before any stream capture.  Every call shares the array and it keeps
+ * the last call's contents, so calls that overlap on the GPU race: serialize
+ * them.  stream: a cudaStream_t (NULL = default stream); stats may be NULL. */
+int mf_solve_csr_noalloc(int n, long long arcs, const int32_t *d_row, const int32_t *d_col,
+                         const int32_t *d_rev, const int64_t *d_cap, int32_t s, int32_t t,
+                         const mf_opts *opts, void *stream, int64_t *flow, mf_stats *stats);
+
 /* ---- dynamic capacities ----------------------------------------------- */
 
 /* Apply nb capacity changes: arc u->v (first matching forward arc, caller

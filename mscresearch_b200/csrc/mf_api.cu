@@ -552,6 +552,10 @@ void host_csr(int n, i64 m, const int32_t *u, const int32_t *v, const int64_t *c
 
 }  // namespace
 
+// Sets the text returned by mf_last_error_string() on the calling thread
+// (used by entry points implemented in other translation units).
+void mf_set_last_error(const char *msg) { g_err = msg ? msg : ""; }
+
 // ===========================================================================
 extern "C" {
 
