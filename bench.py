@@ -105,11 +105,11 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_workload(rank=0):
+def make_workload(rank=0, scale=SCALE, nhub=NHUB, nuni=NUNI):
     import mscresearch_b200 as mf
-    u, v, c = mf.gen_rmat(SCALE, DRAWS, 0.57, 0.19, 0.19, 1, 1000, GRAPH_SEED)
-    n = 1 << SCALE
-    s, t = mf.gen_queries_hub(n, u, v, NHUB, NUNI, QUERY_SEED + 1000 * rank)
+    u, v, c = mf.gen_rmat(scale, 16 << scale, 0.57, 0.19, 0.19, 1, 1000, GRAPH_SEED)
+    n = 1 << scale
+    s, t = mf.gen_queries_hub(n, u, v, nhub, nuni, QUERY_SEED + 1000 * rank)
     return n, u, v, c, s, t
 
 
@@ -173,7 +173,7 @@ def run_engine(args):
     import torch
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     import mscresearch_b200 as mf
-    n, u, v, c, s, t = make_workload(rank)
+    n, u, v, c, s, t = make_workload(rank, args.scale, args.nhub, args.nuni)
     g = mf.Graph.from_edges(n, u, v, c, R=R)
     _, arcs, _ = g.info
     o = mf.opts(group_ctas=args.group)
@@ -204,13 +204,15 @@ def run_engine(args):
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_step = dist_max(float(np.mean(e2e_ms)), world)
     # ---- plain per-query solver on the same queries (drop-in path)
-    plain_ms, plain_flows = [], []
-    for a, b in zip(s, t):
-        f, st = g.solve(a, b)
-        plain_ms.append(st.time_ms)
-        plain_flows.append(f)
-    plain_total = dist_max(float(np.sum(plain_ms)), world)
-    assert list(plain_flows) == list(flows), "plain and batched answers differ"
+    plain_ms, plain_flows, plain_st = [], [], []
+    if not args.no_plain:
+        for a, b in zip(s, t):
+            f, st = g.solve(a, b)
+            plain_ms.append(st.time_ms)
+            plain_flows.append(f)
+            plain_st.append(st)
+        assert list(plain_flows) == list(flows), "plain and batched answers differ"
+    plain_total = dist_max(float(np.sum(plain_ms)), world) if plain_ms else None
     # ---- served: Poisson arrivals at ~60% of batched capacity
     served = None
     if args.serve:
@@ -232,7 +234,7 @@ def run_engine(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
         "data": "synthetic (seeded R-MAT 2^20, 2^24 draws, caps U[1,1000]; 128 hub + 128 uniform queries)",
-        "config": {"workload": WORKLOAD, "n": n, "edges": len(u), "arcs": arcs, "queries_per_gpu": nq,
+        "config": {"workload": "rmat%d_%dq" % (args.scale, nq), "n": n, "edges": len(u), "arcs": arcs, "queries_per_gpu": nq,
                    "R": R, "prune": "fwd(s) & bwd(t)", "group_ctas": o.group_ctas,
                    "l2": "inputs larger than L2 (graph %.2f GB, residual slot %.2f GB)" % (
                        arcs * 20 / 1e9, arcs * 8 / 1e9),
@@ -245,8 +247,8 @@ def run_engine(args):
                      "peak_kind": kind, "alg_bytes_per_launch": alg_bytes},
         "batched": {"qps": round(value, 3), "p50_ms": pct(finish, 50), "p99_ms": pct(finish, 99),
                     "edges_per_s": edges / (np.mean(dev_ms) / 1e3)},
-        "plain": {"qps": round(total_q / (plain_total / 1e3), 3), "p50_ms": pct(plain_ms, 50),
-                  "p99_ms": pct(plain_ms, 99)},
+        "plain": {"qps": round(total_q / (plain_total / 1e3), 3) if plain_total else None,
+                  "p50_ms": pct(plain_ms, 50), "p99_ms": pct(plain_ms, 99)},
         "clocks": clk.summary(),
     }
     if served:
@@ -257,6 +259,18 @@ def run_engine(args):
         res["cpu_baseline"] = cb
     if rank == 0:
         print(json.dumps(res), flush=True)
+    if args.dump and rank == 0:
+        keys = ["flow", "mask_vertices", "mask_arcs", "rounds", "global_relabels", "arcs_examined",
+                "vertices_examined", "pushes", "path_push_rounds", "hot_sweeps", "rm_fixed", "service_ms",
+                "finish_ms"]
+        with open(args.dump, "w") as f:
+            for i, x in enumerate(stats_last):
+                row = {k: getattr(x, k) for k in keys}
+                row.update(q=i, s=int(s[i]), t=int(t[i]), plain_ms=plain_ms[i] if plain_ms else None)
+                if plain_st:
+                    row.update(plain_rounds=plain_st[i].rounds, plain_relabels=plain_st[i].global_relabels,
+                               plain_arcs=plain_st[i].arcs_examined)
+                f.write(json.dumps(row) + "\n")
     g.close()
     if world > 1:
         import torch.distributed as dist
@@ -364,6 +378,11 @@ def main():
     ap.add_argument("--ref-queries-per-step", type=int, default=2)
     ap.add_argument("--ref-timeout", type=int, default=900)
     ap.add_argument("--check", action="store_true")
+    ap.add_argument("--scale", type=int, default=SCALE)
+    ap.add_argument("--nhub", type=int, default=NHUB)
+    ap.add_argument("--nuni", type=int, default=NUNI)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--dump", default=None, help="write per-query stats (jsonl)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
