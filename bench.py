@@ -39,7 +39,7 @@ METRIC = "exact max-flow queries/sec + p50/p99 latency, batched vs plain, same B
 WORKLOAD = "rmat20_256q"
 SCALE, DRAWS, NHUB, NUNI, R = 20, 1 << 24, 128, 128, 128
 GRAPH_SEED, QUERY_SEED = 1, 2
-QOUT_BYTES = 120  # device per-query record copied back by mf_solve_batch
+QOUT_BYTES = 152  # device per-query record copied back by mf_solve_batch
 
 
 def peaks():
@@ -262,14 +262,15 @@ def run_engine(args):
     if args.dump and rank == 0:
         keys = ["flow", "mask_vertices", "mask_arcs", "rounds", "global_relabels", "arcs_examined",
                 "vertices_examined", "pushes", "path_push_rounds", "hot_sweeps", "rm_fixed", "service_ms",
-                "finish_ms"]
+                "finish_ms", "prune_ms", "relabel_ms", "rounds_ms", "relabel_arcs"]
         with open(args.dump, "w") as f:
             for i, x in enumerate(stats_last):
                 row = {k: getattr(x, k) for k in keys}
                 row.update(q=i, s=int(s[i]), t=int(t[i]), plain_ms=plain_ms[i] if plain_ms else None)
                 if plain_st:
                     row.update(plain_rounds=plain_st[i].rounds, plain_relabels=plain_st[i].global_relabels,
-                               plain_arcs=plain_st[i].arcs_examined)
+                               plain_arcs=plain_st[i].arcs_examined, plain_prune_ms=plain_st[i].prune_ms,
+                               plain_relabel_ms=plain_st[i].relabel_ms, plain_rounds_ms=plain_st[i].rounds_ms)
                 f.write(json.dumps(row) + "\n")
     g.close()
     if world > 1:

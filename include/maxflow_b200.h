@@ -87,6 +87,10 @@ typedef struct mf_stats {
     double service_ms;        /* device time from the query's start to its answer */
     double finish_ms;         /* batched calls: device time from the launch's first
                                  query start to this query's answer */
+    double prune_ms;          /* device time in prune + init + preflow */
+    double relabel_ms;        /* device time in global relabels */
+    double rounds_ms;         /* device time in discharge rounds */
+    long long relabel_arcs;   /* arc examinations inside global relabels */
 } mf_stats;
 
 void mf_opts_default(mf_opts *o);

@@ -62,6 +62,10 @@ class MfStats(C.Structure):
         ("time_ms", C.c_double),
         ("service_ms", C.c_double),
         ("finish_ms", C.c_double),
+        ("prune_ms", C.c_double),
+        ("relabel_ms", C.c_double),
+        ("rounds_ms", C.c_double),
+        ("relabel_arcs", C.c_longlong),
     ]
 
 

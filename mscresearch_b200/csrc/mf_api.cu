@@ -67,7 +67,7 @@ int dev_info(DevInfo &d, int threads) {
     return MF_OK;
 }
 
-size_t slot_bytes(int n, i64 arcs) {
+size_t slot_bytes(int n, i64 arcs, int nhub) {
     size_t b = 0;
     auto add = [&](size_t x) { b += (x + 255) & ~(size_t)255; };
     add(sizeof(i64) * (size_t)std::max<i64>(arcs, 1));  // res
@@ -75,17 +75,19 @@ size_t slot_bytes(int n, i64 arcs) {
     for (int i = 0; i < 7; ++i) add(sizeof(int) * (size_t)n);  // h mark qmark claim vlist qa qb
     add(sizeof(int) * 1024);                             // hot
     add(sizeof(int) * 1024);                             // ract
-    add(sizeof(int) * 16);                               // cnt
+    add(sizeof(int) * 32);                               // cnt
     add(sizeof(i64) * 128);                              // acc
     add(sizeof(GroupBar));
     add(sizeof(unsigned));                               // clock
     add(sizeof(int) * 8);                                // meta
+    add(sizeof(HubWork) * (size_t)std::max(nhub, 1));    // hubw
     return b;
 }
 
 struct SlotPool {
     int n = 0;
     i64 arcs = 0;
+    int nhub = 0;
     std::vector<void *> bases;
     std::vector<DSlot> host;
     DSlot *dev = nullptr;
@@ -93,7 +95,7 @@ struct SlotPool {
 
     int grow(int want) {
         while ((int)host.size() < want) {
-            size_t bytes = slot_bytes(n, arcs);
+            size_t bytes = slot_bytes(n, arcs, nhub);
             void *base = nullptr;
             cudaError_t e = cudaMalloc(&base, bytes);
             if (e != cudaSuccess) {
@@ -120,11 +122,13 @@ struct SlotPool {
             s.qb = (int *)take(sizeof(int) * (size_t)n);
             s.hot = (int *)take(sizeof(int) * 1024);
             s.ract = (int *)take(sizeof(int) * 1024);
-            s.cnt = (int *)take(sizeof(int) * 16);
+            s.cnt = (int *)take(sizeof(int) * 32);
             s.acc = (i64 *)take(sizeof(i64) * 128);
             s.bar = (GroupBar *)take(sizeof(GroupBar));
             s.clock = (unsigned *)take(sizeof(unsigned));
             s.meta = (int *)take(sizeof(int) * 8);
+            s.hubw = (HubWork *)take(sizeof(HubWork) * (size_t)std::max(nhub, 1));
+            s.nhub = std::max(nhub, 1);
             bases.push_back(base);
             host.push_back(s);
         }
@@ -199,6 +203,7 @@ struct mf_graph {
     i64 arcs = 0;
     int R = 0;
     int avg_deg = 0;
+    int nhub = 0;  // vertices with more than HUB_T arcs
     std::vector<int> new_id;  // caller id -> internal id
     std::vector<int> old_id;  // internal id -> caller id
     std::vector<double> score_caller;
@@ -411,7 +416,7 @@ int launch(mf_graph *g, SlotPool &pool, int nq, const int *s_int, const int *t_i
         if ((int)pool.host.size() < nslots) {
             size_t fr = 0, tot = 0;
             CK(cudaMemGetInfo(&fr, &tot));
-            size_t per = slot_bytes(pool.n, pool.arcs);
+            size_t per = slot_bytes(pool.n, pool.arcs, pool.nhub);
             int fit = (int)pool.host.size() + (int)((fr * 0.85) / (double)per);
             if (fit < 1) return fail(MF_ERR_NOMEM, "admission: no HBM for a residual slot (%zu bytes)", per);
             nslots = std::min(nslots, fit);
@@ -486,6 +491,10 @@ int launch(mf_graph *g, SlotPool &pool, int nq, const int *s_int, const int *t_i
 void fill_stats(mf_stats *st, const QOut &q, double ms, u64 launch_t0) {
     memset(st, 0, sizeof(*st));
     st->service_ms = (double)(q.t_done - q.t_begin) * 1e-6;
+    st->prune_ms = (double)q.t_prune * 1e-6;
+    st->relabel_ms = (double)q.t_relabel * 1e-6;
+    st->rounds_ms = (double)q.t_rounds * 1e-6;
+    st->relabel_arcs = q.arcs_relabel;
     st->finish_ms = launch_t0 ? (double)(q.t_done - launch_t0) * 1e-6 : 0.0;
     st->flow = q.flow;
     st->status = status_from_err(q.status);
@@ -640,8 +649,15 @@ int mf_graph_create_from_edges(int n, long long m, const int32_t *u, const int32
         mf_graph_destroy(g);
         return rc;
     }
+    {
+        int nh = 0;
+        for (int x = 0; x < n; ++x)
+            if (row[x + 1] - row[x] > HUB_T) ++nh;
+        g->nhub = nh;
+    }
     g->pool.n = n;
     g->pool.arcs = g->arcs;
+    g->pool.nhub = g->nhub;
     *out = g;
     return MF_OK;
 }
@@ -915,12 +931,13 @@ int mf_session_create(mf_graph *g, int nq, const int32_t *s, const int32_t *t, c
     else mf_opts_default(&ss->opts);
     ss->pool.n = g->n;
     ss->pool.arcs = g->arcs;
+    ss->pool.nhub = g->nhub;
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
-    if ((double)slot_bytes(g->n, g->arcs) * nq > 0.9 * (double)fr) {
+    if ((double)slot_bytes(g->n, g->arcs, g->nhub) * nq > 0.9 * (double)fr) {
         delete ss;
         return fail(MF_ERR_NOMEM, "admission: %d resident queries need %.1f GB, %.1f GB free", nq,
-                    slot_bytes(g->n, g->arcs) * (double)nq / 1e9, fr / 1e9);
+                    slot_bytes(g->n, g->arcs, g->nhub) * (double)nq / 1e9, fr / 1e9);
     }
     int rc = ss->pool.grow(nq);
     if (rc) {
@@ -1080,7 +1097,7 @@ int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int ma
     mf_server *sv = new mf_server();
     if (opts) sv->opts = *opts;
     else mf_opts_default(&sv->opts);
-    int nmax = 0;
+    int nmax = 0, hmax = 0;
     i64 amax = 0, arcs_sum = 0, n_sum = 0;
     std::vector<DGraph> dg(ngraphs);
     for (int i = 0; i < ngraphs; ++i) {
@@ -1092,6 +1109,7 @@ int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int ma
         sv->graphs.push_back(g);
         nmax = std::max(nmax, g->n);
         amax = std::max(amax, g->arcs);
+        hmax = std::max(hmax, g->nhub);
         arcs_sum += g->arcs;
         n_sum += g->n;
         dg[i] = DGraph{g->n, g->R, g->arcs, g->row, g->col, g->rev, g->cap, g->region_of};
@@ -1108,7 +1126,7 @@ int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int ma
     int groups = std::max(1, di.sms * di.bps / sv->G);
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
-    size_t per = slot_bytes(nmax, amax);
+    size_t per = slot_bytes(nmax, amax, hmax);
     int fit = (int)((fr * 0.85) / (double)per);
     int ns = std::min(groups, fit);
     if (max_slots > 0) ns = std::min(ns, max_slots);
@@ -1119,6 +1137,7 @@ int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int ma
     sv->nslots = ns;
     sv->pool.n = nmax;
     sv->pool.arcs = amax;
+    sv->pool.nhub = hmax;
     rc = sv->pool.grow(ns);
     if (rc) {
         sv->pool.release();

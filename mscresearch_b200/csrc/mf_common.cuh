@@ -127,22 +127,26 @@ __device__ __forceinline__ void warp_append(bool flag, int val, int *list, int *
 struct GroupBar {
     unsigned arrive;
     unsigned gen;
-    int snap;      // value captured by the last arriver (gsync_snap)
-    int pad;
+    int snap;      // values captured by the last arriver (gsync_snap)
+    int snap2;
 };
 
-// gsync_snap additionally returns, to every thread of the group, the value
-// of *src at the moment the last CTA arrived: all appends made before the
-// barrier are counted and none made after it (a CTA that leaves the barrier
-// early may already be appending to *src).
+// gsync_snap additionally returns, to every thread of the group, the values
+// of *src and *src2 at the moment the last CTA arrived: all appends made
+// before the barrier are counted and none made after it (a CTA that leaves
+// the barrier early may already be appending).
 __device__ __forceinline__ bool gsync_impl(int G, GroupBar *bar, int *err, u64 limit_ns,
-                                           const int *src, int *snap_out) {
+                                           const int *src, const int *src2, int *snap_out,
+                                           int *snap2_out) {
     __shared__ int s_ok;
-    __shared__ int s_snap;
+    __shared__ int s_snap, s_snap2;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        if (G == 1 && src) s_snap = *(volatile const int *)src;
+        if (G == 1 && src) {
+            s_snap = *(volatile const int *)src;
+            s_snap2 = *(volatile const int *)src2;
+        }
         if (G > 1) {
             volatile unsigned *vgen = &bar->gen;
             unsigned gen0 = *vgen;
@@ -152,6 +156,7 @@ __device__ __forceinline__ bool gsync_impl(int G, GroupBar *bar, int *err, u64 l
                 if (src) {
                     __threadfence();
                     *(volatile int *)&bar->snap = *(volatile const int *)src;
+                    *(volatile int *)&bar->snap2 = *(volatile const int *)src2;
                 }
                 atomicExch(&bar->arrive, 0u);
                 __threadfence();
@@ -173,23 +178,30 @@ __device__ __forceinline__ bool gsync_impl(int G, GroupBar *bar, int *err, u64 l
                 }
             }
             __threadfence();
-            if (src) s_snap = *(volatile int *)&bar->snap;
+            if (src) {
+                s_snap = *(volatile int *)&bar->snap;
+                s_snap2 = *(volatile int *)&bar->snap2;
+            }
         }
         if (*(volatile int *)err) ok = 0;
         s_ok = ok;
     }
     __syncthreads();
-    if (snap_out) *snap_out = s_snap;
+    if (snap_out) {
+        *snap_out = s_snap;
+        *snap2_out = s_snap2;
+    }
     return s_ok != 0;
 }
 
 __device__ __forceinline__ bool gsync(int G, GroupBar *bar, int *err, u64 limit_ns) {
-    return gsync_impl(G, bar, err, limit_ns, nullptr, nullptr);
+    return gsync_impl(G, bar, err, limit_ns, nullptr, nullptr, nullptr, nullptr);
 }
 
 __device__ __forceinline__ bool gsync_snap(int G, GroupBar *bar, int *err, u64 limit_ns,
-                                           const int *src, int *snap_out) {
-    return gsync_impl(G, bar, err, limit_ns, src, snap_out);
+                                           const int *src, const int *src2, int *snap_out,
+                                           int *snap2_out) {
+    return gsync_impl(G, bar, err, limit_ns, src, src2, snap_out, snap2_out);
 }
 
 // ---------------------------------------------------------------------------

@@ -49,11 +49,14 @@ constexpr size_t OFF_QB = OFF_QA + na_align(sizeof(int) * NA_MAX_N);
 constexpr size_t OFF_HOT = OFF_QB + na_align(sizeof(int) * NA_MAX_N);
 constexpr size_t OFF_RACT = OFF_HOT + na_align(sizeof(int) * 1024);
 constexpr size_t OFF_CNT = OFF_RACT + na_align(sizeof(int) * 1024);
-constexpr size_t OFF_ACC = OFF_CNT + na_align(sizeof(int) * 16);
+constexpr size_t OFF_ACC = OFF_CNT + na_align(sizeof(int) * 32);
 constexpr size_t OFF_BAR = OFF_ACC + na_align(sizeof(i64) * 128);
 constexpr size_t OFF_CLOCK = OFF_BAR + na_align(sizeof(GroupBar));
 constexpr size_t OFF_META = OFF_CLOCK + na_align(sizeof(unsigned));
-constexpr size_t NA_BYTES = OFF_META + na_align(sizeof(int) * 8);
+// a hub has more than HUB_T arcs, so at most NA_MAX_ARCS / (HUB_T + 1) exist
+constexpr int NA_MAX_HUBS = (int)(NA_MAX_ARCS / (HUB_T + 1)) + 1;
+constexpr size_t OFF_HUBW = OFF_META + na_align(sizeof(int) * 8);
+constexpr size_t NA_BYTES = OFF_HUBW + na_align(sizeof(HubWork) * NA_MAX_HUBS);
 
 }  // namespace
 
@@ -150,6 +153,8 @@ extern "C" int mf_solve_csr_noalloc(int n, long long arcs, const int32_t *d_row,
     sl.bar = (GroupBar *)(b + OFF_BAR);
     sl.clock = (unsigned *)(b + OFF_CLOCK);
     sl.meta = (int *)(b + OFF_META);
+    sl.hubw = (HubWork *)(b + OFF_HUBW);
+    sl.nhub = NA_MAX_HUBS;
     int ctl[4] = {0, 0, s, t};  // err, q_next, s, t
     GroupBar bar0 = {0, 0, 0, 0};
     cudaError_t e = cudaMemcpyAsync(b + OFF_GRAPH, &g, sizeof g, cudaMemcpyHostToDevice, st);

@@ -10,9 +10,9 @@
 //     and deficit vertices, warp-ballot
 //     frontier compaction) .................. init_height_level_frontier + bfs_expand_frontier
 //                                             RA:203-233, 322-348, driver RA:1499-1581
-//   discharge (warp per active vertex,
-//     ballot/shuffle arc scan, multi-push
-//     with native 64-bit atomics) ........... staticMaxFlow_kernel_14_region RA:432-515
+//   discharge (lane / warp / group per vertex
+//     by degree, ballot/shuffle arc scans,
+//     native 64-bit atomics) ................ staticMaxFlow_kernel_14_region RA:432-515
 //   active worklist + counts ................ build_active_list_and_count RA:664-695
 //   hot-region extra sweep .................. count_region_active_kernel + hot pass RA:283-318, 1899-1984
 //   sparse-phase path push .................. try_push_along_path / _with_path_push RA:773-955
@@ -20,24 +20,35 @@
 //   stagnation / adaptive K, GR frequency ... RA:1845-1891
 //   termination + read excess(t) ............ RA:1988, 2114, 2202-2204
 //
+// Load balance.  Every frontier and worklist holds each vertex at most once
+// and is split by degree: vertices with at most HUB_T arcs fill the list
+// from the front, "hubs" fill it from the back of the same array.  BFS levels
+// give each warp 32 front vertices and spread their combined arcs over the
+// lanes; hub arcs are cut into 32-arc chunks spread over all warps of the
+// group.  Discharge runs one vertex per lane for vertices with at most
+// SMALL_T arcs, one vertex per warp above that, and hubs chunked over the
+// whole group with the excess handed out through an atomic budget.
+//
 // Exactness.  Every kernel keeps residuals non-negative and pairwise
-// conserved with atomic updates; only the owner of a vertex (one warp per
-// vertex per pass, ownership stamps for path push) lowers its excess.  RM is
-// the only step that creates negative excess (deficits), as in the
-// reference; deficits are relabel seeds, and if any remain when no active
-// vertex is left the solver drains them back from the sink (phase B) before
-// resuming.  A solve ends only when an exact global relabel finds no vertex
-// with positive excess that can reach the sink and no deficit: the preflow
-// is then maximum and excess(t) is the max-flow value.
+// conserved with atomic updates; only the owner of a vertex (one lane or
+// warp per vertex per pass, the budget for hubs, ownership stamps for path
+// push) lowers its excess.  RM is the only step that creates negative excess
+// (deficits), as in the reference; deficits are relabel seeds, and if any
+// remain when no active vertex is left the solver drains them back from the
+// sink (phase B) before resuming.  A solve ends only when an exact global
+// relabel finds no vertex with positive excess that can reach the sink and
+// no deficit: the preflow is then maximum and excess(t) is the max-flow value.
 #include "mf_solver.cuh"
 
 #include <climits>
 #include <cstring>
 
-// cnt[0..7]: list tails, handed out in rotation; taking bank k zeroes bank
-// k+4 (mod 8), which was last read at least one group barrier earlier (no
-// code path takes more than three banks between two barriers).
+// cnt[0..7]: front tails of the list banks, cnt[16..23]: their back (hub)
+// tails.  Banks are handed out in rotation; taking bank k zeroes bank k+4
+// (mod 8), last read at least one group barrier earlier (no code path takes
+// more than three banks between two barriers).
 #define NBANKS 8
+#define CNT_BACK 16
 #define CNT_Q 8      // query handed to the group
 #define CNT_FLAG 9   // misc uniform flag
 #define CNT_RS 10    // serving: request source / sink / graph
@@ -64,12 +75,16 @@
 #define T_VERTS 1
 #define T_PUSH 2
 #define T_MASKARCS 3
+#define T_RARCS 4
+
+#define SMALL_T 32  // at most this many arcs: one lane per vertex in discharge
+#define MAX_WARPS 32
 
 enum Phase { PH_A = 0, PH_B = 1, PH_C = 2 };
 
 struct QCtx {
     // group geometry
-    int G, crank, gw, gW, lane, wpc;
+    int G, crank, gw, gW, lane, wpc, warp;
     GroupBar *bar;
     int *err;
     u64 lim;
@@ -79,6 +94,7 @@ struct QCtx {
     const i64 *cap;
     // slot
     DSlot st;
+    int vf;  // kept vertices in the front part of vlist (the rest are at the back)
     // uniform control
     unsigned clock;
     int seq;   // list-bank sequence
@@ -87,17 +103,23 @@ struct QCtx {
     u64 t_start;
     u64 time_limit;
     u64 q_begin;
+    u64 tm_relabel, tm_rounds;  // leader: accumulated phase times
     // per-warp counters (flushed at the end of the query)
     i64 w_arcs, w_verts, w_push;
 
     __device__ bool sync() { return gsync(G, bar, err, lim); }
-    // barrier that also returns the list tail cnt[bank] as of the barrier
-    __device__ bool sync_tail(int bank, int &tail) {
-        return gsync_snap(G, bar, err, lim, &st.cnt[bank], &tail);
+    // barrier that also returns the front and back tails of list bank `bank`
+    // as of the barrier
+    __device__ bool sync_tails(int bank, int &ft, int &bt) {
+        return gsync_snap(G, bar, err, lim, &st.cnt[bank], &st.cnt[CNT_BACK + bank], &ft, &bt);
     }
     __device__ int take_bank() {
         int b = seq & (NBANKS - 1);
-        if (leader) st.cnt[(seq + 4) & (NBANKS - 1)] = 0;
+        if (leader) {
+            int z = (seq + 4) & (NBANKS - 1);
+            st.cnt[z] = 0;
+            st.cnt[CNT_BACK + z] = 0;
+        }
         ++seq;
         return b;
     }
@@ -121,51 +143,155 @@ struct QCtx {
         }
         w_arcs = w_verts = w_push = 0;
     }
+    __device__ __forceinline__ int deg(int v) const { return ldro(&row[v + 1]) - ldro(&row[v]); }
+    // i-th kept vertex (front part, then back part)
+    __device__ __forceinline__ int vat(int i) const {
+        return ldcg(i < vf ? &st.vlist[i] : &st.vlist[n - 1 - (i - vf)]);
+    }
 };
 
+// entry k of a list's back part
+__device__ __forceinline__ int back_at(const QCtx &c, const int *L, int k) { return ldcg(&L[c.n - 1 - k]); }
+
 // ---------------------------------------------------------------------------
-// Level-synchronous frontier BFS over a growing queue Q[0..tail).  The
-// frontier at level L is Q[lo,hi); claimed vertices are appended with warp
-// ballot + prefix ranks (one atomicAdd per warp).  Functor cl(v, e, w) returns
-// true when arc e = v->w claims w (it performs the claim itself).
+// Class-aware warp-aggregated append: flagged lanes add w to list L, at the
+// front (cnt[bank]) or, when w has more than HUB_T arcs, at the back
+// (cnt[CNT_BACK + bank], stored at L[n-1-k]).  One atomicAdd per class per
+// warp.  All 32 lanes must call it.
+__device__ __forceinline__ void append2(QCtx &c, bool flag, int w, int *L, int bank) {
+    unsigned any = __ballot_sync(MF_FULL, flag);
+    if (any == 0) return;
+    bool hub = false;
+    if (flag) hub = c.deg(w) > HUB_T;
+    unsigned fm = __ballot_sync(MF_FULL, flag && !hub);
+    unsigned bm = any & ~fm;
+    if (fm) {
+        int ld = __ffs(fm) - 1, base = 0;
+        if (c.lane == ld) base = atomicAdd(&c.st.cnt[bank], __popc(fm));
+        base = __shfl_sync(MF_FULL, base, ld);
+        if (flag && !hub) {
+            int pos = base + __popc(fm & lanemask_lt());
+            if (MF_OK_IDX(pos, c.n, 91)) L[pos] = w;
+        }
+    }
+    if (bm) {
+        int ld = __ffs(bm) - 1, base = 0;
+        if (c.lane == ld) base = atomicAdd(&c.st.cnt[CNT_BACK + bank], __popc(bm));
+        base = __shfl_sync(MF_FULL, base, ld);
+        if (flag && hub) {
+            int k = base + __popc(bm & lanemask_lt());
+            if (MF_OK_IDX(k, c.n, 92)) L[c.n - 1 - k] = w;
+        }
+    }
+}
+
+// Single-lane append (no warp collectives).
+__device__ __forceinline__ void append1(QCtx &c, int w, int *L, int bank) {
+    if (c.deg(w) > HUB_T) {
+        int k = atomicAdd(&c.st.cnt[CNT_BACK + bank], 1);
+        if (MF_OK_IDX(k, c.n, 93)) L[c.n - 1 - k] = w;
+    } else {
+        int k = atomicAdd(&c.st.cnt[bank], 1);
+        if (MF_OK_IDX(k, c.n, 94)) L[k] = w;
+    }
+}
+
+__device__ __forceinline__ int warp_incl_scan_int(int x) {
+    const int lane = lane_id();
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(MF_FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+// ---------------------------------------------------------------------------
+// Level-synchronous frontier BFS over a growing two-ended queue Q: the
+// frontier at a level is Q[flo,fhi) plus back entries [blo,bhi).  Functor
+// cl(v, e, w, level) returns true when arc e = v->w claims w (it performs
+// the claim itself).
+__shared__ int s_lbs_v[MAX_WARPS][32];
+__shared__ int s_lbs_b[MAX_WARPS][32];
+__shared__ int s_lbs_x[MAX_WARPS][32];
+
 template <class Claim>
-__device__ bool bfs_levels(QCtx &c, int *Q, int bank, int hi, Claim cl, int *levels_out) {
-    int lo = 0, level = 0;
-    while (lo < hi) {
+__device__ bool bfs_levels(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl) {
+    int flo = 0, blo = 0, level = 0;
+    int *sv = s_lbs_v[c.warp], *sb = s_lbs_b[c.warp], *sx = s_lbs_x[c.warp];
+    while (flo < fhi || blo < bhi) {
         MF_TRACE(10, level);
-        for (int i = lo + c.gw; i < hi; i += c.gW) {
-            int v = ldcg(&Q[i]);
-            if (!MF_OK_IDX(v, c.n, 11)) continue;
+        // front: 32 vertices per warp, arcs balanced over the lanes
+        for (int base = flo + c.gw * 32; base < fhi; base += c.gW * 32) {
+            int i = base + c.lane;
+            int v = 0, b = 0, d = 0;
+            if (i < fhi) {
+                v = ldcg(&Q[i]);
+                if (MF_OK_IDX(v, c.n, 11)) {
+                    b = ldro(&c.row[v]);
+                    d = ldro(&c.row[v + 1]) - b;
+                }
+            }
+            int incl = warp_incl_scan_int(d);
+            int total = __shfl_sync(MF_FULL, incl, 31);
+            sv[c.lane] = v;
+            sb[c.lane] = b;
+            sx[c.lane] = incl - d;
+            __syncwarp();
+            for (int k = 0; k < total; k += 32) {
+                int j = k + c.lane;
+                bool ok = false;
+                int w = 0;
+                if (j < total) {
+                    int o = 0;
+#pragma unroll
+                    for (int step = 16; step > 0; step >>= 1)
+                        if (sx[o + step] <= j) o += step;
+                    int e = sb[o] + (j - sx[o]);
+                    w = ldro(&c.col[e]);
+                    ok = cl(sv[o], e, w, level);
+                }
+                append2(c, ok, w, Q, bank);
+            }
+            __syncwarp();
+            if (c.lane == 0) {
+                c.w_arcs += total;
+                c.w_verts += min(32, fhi - base);
+            }
+        }
+        // back: hub arcs in 32-arc chunks over all warps of the group
+        for (int k = blo; k < bhi; ++k) {
+            int v = back_at(c, Q, k);
             int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
-            for (int base = b; base < e1; base += 32) {
-                int e = base + c.lane;
+            int nch = (e1 - b + 31) >> 5;
+            for (int ch = c.gw; ch < nch; ch += c.gW) {
+                int e = b + ch * 32 + c.lane;
                 bool ok = false;
                 int w = 0;
                 if (e < e1) {
                     w = ldro(&c.col[e]);
                     ok = cl(v, e, w, level);
                 }
-                warp_append(ok, w, Q, &c.st.cnt[bank], c.n);
+                append2(c, ok, w, Q, bank);
+                if (c.lane == 0) c.w_arcs += min(32, e1 - (b + ch * 32));
             }
-            if (c.lane == 0) {
-                c.w_arcs += e1 - b;
-                c.w_verts += 1;
-            }
+            if (c.lane == 0 && c.gw == 0) c.w_verts += 1;
         }
-        int tail = 0;
-        if (!c.sync_tail(bank, tail)) return false;
-        lo = hi;
-        hi = tail;
+        int ft = 0, bt = 0;
+        if (!c.sync_tails(bank, ft, bt)) return false;
+        flo = fhi;
+        fhi = ft;
+        blo = bhi;
+        bhi = bt;
         ++level;
     }
-    if (levels_out) *levels_out = level;
     return true;
 }
 
 // ---------------------------------------------------------------------------
 // Prune.  Stamps: S (forward reach), M = S+1 (kept), U (undirected, mode 0).
-// Leaves the kept vertices in vlist[0..nv) and returns nv (0 if t is not
-// reachable from s, in which case the flow is 0).
+// Leaves the kept vertices in vlist (front c.vf entries, back nv - c.vf) and
+// returns nv (0 if t is not reachable from s, in which case the flow is 0).
 __device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, int &nv,
                       bool &t_reach) {
     MF_TRACE(20, s);
@@ -173,10 +299,10 @@ __device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, i
     int bank = c.take_bank();
     if (c.leader) {
         c.st.mark[s] = S;
-        c.st.qa[0] = s;
-        c.st.cnt[bank] = 1;
+        append1(c, s, c.st.qa, bank);
     }
-    if (!c.sync()) return false;
+    int f0 = 0, b0 = 0;
+    if (!c.sync_tails(bank, f0, b0)) return false;
     unsigned *mark = c.st.mark;
     const i64 *cap = c.cap;
     auto fwd = [&](int v, int e, int w, int) -> bool {
@@ -184,32 +310,33 @@ __device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, i
         if (ldcg(&mark[w]) >= S) return false;
         return atomicMax(&mark[w], S) < S;
     };
-    if (!bfs_levels(c, c.st.qa, bank, 1, fwd, nullptr)) return false;
-    int nf = ldcg(&c.st.cnt[bank]);
+    if (!bfs_levels(c, c.st.qa, bank, f0, b0, fwd)) return false;
+    int nff = ldcg(&c.st.cnt[bank]), nfb = ldcg(&c.st.cnt[CNT_BACK + bank]);
     t_reach = ldcg(&mark[t]) >= S;
 
     int vb = c.take_bank();
     if (mode == 1) {
         if (!t_reach) {
             nv = 0;
+            c.vf = 0;
             return true;
         }
-        // backward BFS from t over arcs whose reverse (y->x) has capacity,
+        // backward BFS from t over arcs whose reverse (w->v) has capacity,
         // restricted to forward-reached vertices
         if (c.leader) {
             mark[t] = M;
-            c.st.vlist[0] = t;
-            c.st.cnt[vb] = 1;
+            append1(c, t, c.st.vlist, vb);
         }
-        if (!c.sync()) return false;
+        if (!c.sync_tails(vb, f0, b0)) return false;
         const int *rev = c.rev;
         auto bwd = [&](int v, int e, int w, int) -> bool {
             if (ldcg(&mark[w]) != S) return false;
             if (ldro(&cap[ldro(&rev[e])]) <= 0) return false;
             return atomicCAS(&mark[w], S, M) == S;
         };
-        if (!bfs_levels(c, c.st.vlist, vb, 1, bwd, nullptr)) return false;
-        nv = ldcg(&c.st.cnt[vb]);
+        if (!bfs_levels(c, c.st.vlist, vb, f0, b0, bwd)) return false;
+        c.vf = ldcg(&c.st.cnt[vb]);
+        nv = c.vf + ldcg(&c.st.cnt[CNT_BACK + vb]);
         return true;
     }
     // mode 0: undirected component of t (all arcs) with qmark stamp U = M
@@ -219,36 +346,36 @@ __device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, i
     unsigned *qm = c.st.qmark;
     if (c.leader) {
         qm[t] = M;
-        c.st.qb[0] = t;
-        c.st.cnt[ub] = 1;
+        append1(c, t, c.st.qb, ub);
     }
-    if (!c.sync()) return false;
+    if (!c.sync_tails(ub, f0, b0)) return false;
     auto und = [&](int v, int e, int w, int) -> bool {
         if (ldcg(&qm[w]) >= M) return false;
         return atomicMax(&qm[w], M) < M;
     };
-    if (!bfs_levels(c, c.st.qb, ub, 1, und, nullptr)) return false;
-    // intersect: sweep the forward list (s is its first entry)
+    if (!bfs_levels(c, c.st.qb, ub, f0, b0, und)) return false;
+    // intersect: sweep the forward list (both parts); s is in it
+    int nf = nff + nfb;
     for (int base = c.gw * 32; base < nf; base += c.gW * 32) {
         int i = base + c.lane;
         bool keep = false;
         int v = 0;
         if (i < nf) {
-            v = ldcg(&c.st.qa[i]);
+            v = ldcg(i < nff ? &c.st.qa[i] : &c.st.qa[c.n - 1 - (i - nff)]);
             keep = (ldcg(&qm[v]) == M) || v == s;
             if (keep) mark[v] = M;
         }
-        warp_append(keep, v, c.st.vlist, &c.st.cnt[vb], c.n);
+        append2(c, keep, v, c.st.vlist, vb);
     }
     if (!c.sync()) return false;
     if (c.leader && !t_reach) {
         // t is always kept (RA:1443-1444) even when s cannot reach it
-        int k = atomicAdd(&c.st.cnt[vb], 1);
-        c.st.vlist[k] = t;
+        append1(c, t, c.st.vlist, vb);
         mark[t] = M;
     }
     if (!c.sync()) return false;
-    nv = ldcg(&c.st.cnt[vb]);
+    c.vf = ldcg(&c.st.cnt[vb]);
+    nv = c.vf + ldcg(&c.st.cnt[CNT_BACK + vb]);
     return true;
 }
 
@@ -259,7 +386,7 @@ __device__ bool init_state(QCtx &c, int nv, unsigned M) {
     MF_TRACE(30, nv);
     i64 mask_arcs = 0;
     for (int i = c.gw; i < nv; i += c.gW) {
-        int v = ldcg(&c.st.vlist[i]);
+        int v = c.vat(i);
         int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
         if (c.lane == 0) {
             c.st.ex[v] = 0;
@@ -301,10 +428,11 @@ __device__ bool preflow(QCtx &c, int s) {
 // negative-excess vertices).  Backward BFS over residual arcs through kept
 // vertices; the blocked vertex is never labeled.  Afterwards unreached kept
 // vertices get height n, and the active list (excess > 0, height < n, not
-// the phase sink or blocked vertex) is compacted into L.
-// Returns counts in na / nd (active / deficits).
+// the phase sink or blocked vertex) is compacted into L (front / back).
+// Returns counts in naf / nab (active front / back) and nd (deficits).
 __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int blockv, int srcv,
-                               bool deficit_seeds, int *L, int &na, int &nd, i64 *&ab) {
+                               bool deficit_seeds, int *L, int lbk, int &naf, int &nab, int &nd,
+                               i64 *&ab) {
     MF_TRACE(40, nv);
     unsigned cur = ++c.clock;
     int qbk = c.take_bank();
@@ -316,7 +444,7 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
         bool seed = false;
         int v = 0;
         if (i < nv) {
-            v = ldcg(&c.st.vlist[i]);
+            v = c.vat(i);
             if (v == sinkv) seed = true;
             else if (deficit_seeds && v != blockv && v != srcv && ldcg(&c.st.ex[v]) < 0) seed = true;
             if (seed) {
@@ -324,10 +452,10 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
                 c.st.h[v] = 0;
             }
         }
-        warp_append(seed, v, c.st.qa, &c.st.cnt[qbk], c.n);
+        append2(c, seed, v, c.st.qa, qbk);
     }
-    int hi = 0;
-    if (!c.sync_tail(qbk, hi)) return false;
+    int f0 = 0, b0 = 0;
+    if (!c.sync_tails(qbk, f0, b0)) return false;
     const int *rev = c.rev;
     i64 *res = c.st.res;
     int *h = c.st.h;
@@ -340,20 +468,18 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
         h[w] = level + 1;
         return true;
     };
-    if (!bfs_levels(c, c.st.qa, qbk, hi, relab, nullptr)) return false;
+    if (!bfs_levels(c, c.st.qa, qbk, f0, b0, relab)) return false;
 
     // sweep: heights of unreached vertices, active list, counts
     MF_TRACE(41, 0);
-    int lbk = c.take_bank();
     ab = c.take_abank();
-    i64 l_sum = 0, l_high = 0, l_def = 0;
-    int l_hmin = INT_MAX, l_hmax = -1;
+    i64 l_sum = 0, l_def = 0;
     for (int base = c.gw * 32; base < nv; base += c.gW * 32) {
         int i = base + c.lane;
         bool act = false;
         int v = 0;
         if (i < nv) {
-            v = ldcg(&c.st.vlist[i]);
+            v = c.vat(i);
             int hv;
             if (ldcg(&mark[v]) != cur) {
                 h[v] = n;
@@ -365,13 +491,10 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
             if (ev > 0 && hv < n && v != sinkv && v != blockv) {
                 act = true;
                 l_sum += ev;
-                if (hv > 0) l_hmin = min(l_hmin, hv);
-                l_hmax = max(l_hmax, hv);
-                l_high += (hv > 0);
             }
             if (ev < 0 && v != srcv && v != blockv) ++l_def;
         }
-        warp_append(act, v, L, &c.st.cnt[lbk], c.n);
+        append2(c, act, v, L, lbk);
     }
     l_sum = warp_sum_i64(l_sum);
     l_def = warp_sum_i64(l_def);
@@ -379,12 +502,8 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
         if (l_sum) atomic_add_i64(&ab[A_SUMEX], l_sum);
         if (l_def) atomic_add_i64(&ab[A_NDEF], l_def);
     }
-    if (!c.sync()) return false;
-    na = ldcg(&c.st.cnt[lbk]);
+    if (!c.sync_tails(lbk, naf, nab)) return false;
     nd = (int)ldcg(&ab[A_NDEF]);
-    (void)l_high;
-    (void)l_hmin;
-    (void)l_hmax;
     return true;
 }
 
@@ -403,14 +522,14 @@ __device__ __forceinline__ bool enlist(QCtx &c, int w, unsigned rstamp) {
     return atomicMax(&c.st.qmark[w], rstamp) < rstamp;
 }
 
-// Discharge one vertex with a whole warp for up to K cycles.  Each cycle
-// scans v's arcs 32 at a time: lanes read residual + head height, a ballot
-// finds downhill residual arcs, a 64-bit inclusive shuffle scan splits the
-// remaining excess over them in arc order, and every lane pushes its share
-// with native 64-bit atomics.  If excess remains after all arcs, v is
-// relabeled to 1 + the lowest height over arcs that still have residual
-// (n when none).  Newly active heads and v itself (if still active) are
-// appended to N.
+// Warp-cooperative discharge of one vertex (medium degree) for up to K
+// cycles.  Each cycle scans v's arcs 32 at a time: lanes read residual +
+// head height, a ballot finds downhill residual arcs, a 64-bit inclusive
+// shuffle scan splits the remaining excess over them in arc order, and every
+// lane pushes its share with native 64-bit atomics.  If excess remains after
+// all arcs, v is relabeled to 1 + the lowest height over arcs that still
+// have residual (n when none).  Newly active heads and v itself (if still
+// active) are appended to N.
 __device__ void discharge_vertex(QCtx &c, int v, int K, int sinkv, int blockv, int *N, int nbk,
                                  unsigned rstamp, i64 *ab) {
     const int n = c.n;
@@ -461,7 +580,7 @@ __device__ void discharge_vertex(QCtx &c, int v, int K, int sinkv, int blockv, i
             }
             if (r - d > 0) minh = min(minh, hw);
             bool add = act && enlist(c, w, rstamp);
-            warp_append(add, w, N, &c.st.cnt[nbk], c.n);
+            append2(c, add, w, N, nbk);
             arcs += min(32, e1 - base);
             if (rem == 0) break;
         }
@@ -473,17 +592,204 @@ __device__ void discharge_vertex(QCtx &c, int v, int K, int sinkv, int blockv, i
             if (c.lane == 0) c.st.h[v] = hv;
         }
         __syncwarp();
-        ev = ldcg(&c.st.ex[v]);
+        if (c.lane == 0) ev = ldcg(&c.st.ex[v]);
         ev = __shfl_sync(MF_FULL, ev, 0);
     }
     MF_TRACE(51, v);
     bool again = (c.lane == 0) && ev > 0 && hv < n && enlist(c, v, rstamp);
-    warp_append(again, v, N, &c.st.cnt[nbk], c.n);
+    append2(c, again, v, N, nbk);
     if (c.lane == 0) {
         c.w_arcs += arcs;
         c.w_verts += 1;
         c.w_push += pushes;
         if (arcs) atomic_add_i64(&ab[A_WORK], arcs);
+    }
+}
+
+// Discharge of the front part L[0, nf): each warp takes 32 entries.  Lanes
+// whose vertex has at most SMALL_T arcs discharge it themselves, in lockstep
+// over arc slots (greedy pushes to downhill arcs in arc order, per-lane
+// relabel, warp-aggregated appends); the warp then discharges the other
+// (medium) vertices one at a time, cooperatively, with its cycles capped so
+// that one vertex scans at most about K x 32 arcs per round.  hot != NULL
+// restricts the pass to vertices of hot regions.
+__device__ void discharge_front(QCtx &c, const int *L, int nf, int K, int sinkv, int blockv,
+                                int *N, int nbk, unsigned rstamp, i64 *ab, const int *hot) {
+    const int n = c.n;
+    for (int base = c.gw * 32; base < nf; base += c.gW * 32) {
+        int i = base + c.lane;
+        int v = -1, b = 0, d = 0;
+        if (i < nf) {
+            v = ldcg(&L[i]);
+            if (!MF_OK_IDX(v, n, 12)) v = -1;
+            else if (hot && !ldcg(&hot[ldro(&c.rof[v])])) v = -1;
+        }
+        if (v >= 0) {
+            b = ldro(&c.row[v]);
+            d = ldro(&c.row[v + 1]) - b;
+        }
+        bool small = v >= 0 && d <= SMALL_T;
+        // ---- one vertex per lane
+        i64 ev = 0;
+        int hv = n;
+        if (small) {
+            hv = ldcg(&c.st.h[v]);
+            ev = ldcg(&c.st.ex[v]);
+        }
+        bool act = small && ev > 0 && hv < n;
+        i64 arcs = 0, pushes = 0;
+        for (int cyc = 0; cyc < K; ++cyc) {
+            if (!__any_sync(MF_FULL, act)) break;
+            int md = __reduce_max_sync(MF_FULL, act ? d : 0);
+            i64 rem = ev;
+            int minh = MF_INF_H;
+            bool scan = act;
+            for (int j = 0; j < md; ++j) {
+                bool add = false;
+                int w = 0;
+                if (scan && j < d) {
+                    int e = b + j;
+                    i64 r = ldcg(&c.st.res[e]);
+                    ++arcs;
+                    if (r > 0) {
+                        w = ldro(&c.col[e]);
+                        int hw = ldcg(&c.st.h[w]);
+                        i64 dd = 0;
+                        if (hw < hv) {
+                            dd = min(r, rem);
+                            add = push_arc(c, e, w, dd, sinkv, blockv);
+                            rem -= dd;
+                            ++pushes;
+                        }
+                        if (r - dd > 0) minh = min(minh, hw);
+                        if (rem == 0) scan = false;
+                    }
+                }
+                if (add) add = enlist(c, w, rstamp);
+                append2(c, add, w, N, nbk);
+            }
+            if (act) {
+                i64 pushed = ev - rem;
+                if (pushed) atomic_add_i64(&c.st.ex[v], -pushed);
+                if (rem > 0) {
+                    hv = (minh >= n - 1) ? n : minh + 1;
+                    c.st.h[v] = hv;
+                }
+                ev = ldcg(&c.st.ex[v]);
+                act = ev > 0 && hv < n;
+            }
+        }
+        bool again = small && ev > 0 && hv < n && enlist(c, v, rstamp);
+        append2(c, again, v, N, nbk);
+        arcs = warp_sum_i64(arcs);
+        pushes = warp_sum_i64(pushes);
+        if (c.lane == 0) {
+            c.w_arcs += arcs;
+            c.w_push += pushes;
+            c.w_verts += min(32, nf - base);
+            if (arcs) atomic_add_i64(&ab[A_WORK], arcs);
+        }
+        // ---- medium vertices: one warp each
+        unsigned med = __ballot_sync(MF_FULL, v >= 0 && d > SMALL_T);
+        while (med) {
+            int o = __ffs(med) - 1;
+            med &= med - 1;
+            int vo = __shfl_sync(MF_FULL, v, o);
+            int dv = __shfl_sync(MF_FULL, d, o);
+            int Kv = max(1, min(K, (K * 32) / max(dv, 1)));
+            discharge_vertex(c, vo, Kv, sinkv, blockv, N, nbk, rstamp, ab);
+        }
+    }
+}
+
+// Hubs of L's back part, one cycle per round, spread over all warps of the
+// group.  Set-up (before a group barrier): per hub, budget = its excess,
+// minh = INF, done = 0, hv = its height.  Each warp then takes 32-arc chunks
+// of each hub: it sums the downhill residual of its chunk, claims that much
+// from the hub's budget with one atomicAdd (getting the whole amount, the
+// rest, or nothing), spreads the claim over the chunk's downhill arcs in arc
+// order, and folds the lowest height over arcs left with residual into
+// minh.  The warp that finishes a hub's last chunk relabels it when budget
+// is left (then every downhill arc was saturated, so minh >= its height) and
+// re-lists it if it is still active.
+__device__ bool hub_setup(QCtx &c, const int *L, int nb, const int *hot) {
+    int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+    for (int k = gt; k < nb; k += gT) {
+        int v = back_at(c, L, k);
+        HubWork hw;
+        hw.budget = ldcg(&c.st.ex[v]);
+        hw.minh = MF_INF_H;
+        hw.done = 0;
+        hw.hv = ldcg(&c.st.h[v]);
+        bool skip = hw.budget <= 0 || hw.hv >= c.n || (hot && !ldcg(&hot[ldro(&c.rof[v])]));
+        hw.nch = skip ? 0 : (c.deg(v) + 31) >> 5;
+        if (MF_OK_IDX(k, c.st.nhub, 95)) c.st.hubw[k] = hw;
+    }
+    return c.sync();
+}
+
+__device__ void discharge_hubs(QCtx &c, const int *L, int nb, int sinkv, int blockv, int *N, int nbk,
+                               unsigned rstamp, i64 *ab) {
+    const int n = c.n;
+    for (int k = 0; k < nb; ++k) {
+        HubWork *hw = &c.st.hubw[k];
+        int nch = ldcg(&hw->nch);
+        if (nch == 0) continue;
+        int v = back_at(c, L, k);
+        int hv = ldcg(&hw->hv);
+        int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+        for (int ch = c.gw; ch < nch; ch += c.gW) {
+            int e = b + ch * 32 + c.lane;
+            i64 r = 0;
+            int w = 0, hwt = MF_INF_H;
+            if (e < e1) {
+                r = ldcg(&c.st.res[e]);
+                if (r > 0) {
+                    w = ldro(&c.col[e]);
+                    hwt = ldcg(&c.st.h[w]);
+                }
+            }
+            bool adm = r > 0 && hwt < hv;
+            i64 x = adm ? r : 0;
+            i64 incl = warp_incl_scan_i64(x);
+            i64 tot = __shfl_sync(MF_FULL, incl, 31);
+            i64 take = 0;
+            if (tot > 0) {
+                if (c.lane == 0) {
+                    i64 old = atomic_add_i64(&hw->budget, -tot);
+                    take = old >= tot ? tot : (old > 0 ? old : 0);
+                }
+                take = __shfl_sync(MF_FULL, take, 0);
+            }
+            i64 dd = 0;
+            bool act = false;
+            if (adm && take > incl - x) dd = min(r, take - (incl - x));
+            if (dd > 0) act = push_arc(c, e, w, dd, sinkv, blockv);
+            if (act) act = enlist(c, w, rstamp);
+            append2(c, act, w, N, nbk);
+            int mh = __reduce_min_sync(MF_FULL, (r - dd > 0) ? hwt : MF_INF_H);
+            if (c.lane == 0) {
+                if (take) atomic_add_i64(&c.st.ex[v], -take);
+                if (mh != MF_INF_H) atomicMin(&hw->minh, mh);
+                c.w_arcs += min(32, e1 - (b + ch * 32));
+                c.w_push += take ? 1 : 0;
+                __threadfence();
+                if (atomicAdd(&hw->done, 1) == nch - 1) {
+                    // last chunk of this hub: relabel if excess was left over
+                    __threadfence();
+                    i64 left = atomic_add_i64(&hw->budget, 0);
+                    int hnew = hv;
+                    if (left > 0) {
+                        int m = atomicAdd(&hw->minh, 0);
+                        hnew = (m >= n - 1) ? n : m + 1;
+                        c.st.h[v] = hnew;
+                    }
+                    i64 ev = ldcg(&c.st.ex[v]);
+                    if (ev > 0 && hnew < n && enlist(c, v, rstamp)) append1(c, v, N, nbk);
+                    c.w_verts += 1;
+                }
+            }
+        }
     }
 }
 
@@ -504,12 +810,15 @@ __device__ void path_push_vertex(QCtx &c, int v, int max_path, int sinkv, int bl
     i64 arcs = 0, pushes = 0;
     while (hops < max_path && steps < 2 * max_path + 8) {
         ++steps;
-        i64 ec = ldcg(&c.st.ex[cur]);
+        i64 ec = 0;
+        int hc = 0;
+        if (c.lane == 0) {
+            ec = ldcg(&c.st.ex[cur]);
+            hc = ldcg(&c.st.h[cur]);
+        }
         ec = __shfl_sync(MF_FULL, ec, 0);
-        if (ec <= 0 || cur == sinkv) break;
-        int hc = ldcg(&c.st.h[cur]);
         hc = __shfl_sync(MF_FULL, hc, 0);
-        if (hc >= n) break;
+        if (ec <= 0 || cur == sinkv || hc >= n) break;
         int b = ldro(&c.row[cur]), e1 = ldro(&c.row[cur + 1]);
         int best_e = INT_MAX, minh = MF_INF_H;
         for (int base = b; base < e1; base += 32) {
@@ -539,16 +848,12 @@ __device__ void path_push_vertex(QCtx &c, int v, int max_path, int sinkv, int bl
                     atomic_add_i64(&c.st.ex[cur], -d);
                     ++pushes;
                 }
-                if (ec - d > 0 && enlist(c, cur, rstamp)) {
-                    int k = atomicAdd(&c.st.cnt[nbk], 1);
-                    N[k] = cur;
-                }
+                if (ec - d > 0 && enlist(c, cur, rstamp)) append1(c, cur, N, nbk);
                 if (w != sinkv && w != blockv && atomicMax(&c.st.claim[w], pstamp) < pstamp) {
                     cont = true;
                     nxt = w;
                 } else if (act && enlist(c, w, rstamp)) {
-                    int k = atomicAdd(&c.st.cnt[nbk], 1);
-                    N[k] = w;
+                    append1(c, w, N, nbk);
                 }
             }
             cont = __shfl_sync(MF_FULL, cont, 0);
@@ -567,10 +872,8 @@ __device__ void path_push_vertex(QCtx &c, int v, int max_path, int sinkv, int bl
     }
     if (c.lane == 0 && cur >= 0) {
         i64 ec = ldcg(&c.st.ex[cur]);
-        if (ec > 0 && ldcg(&c.st.h[cur]) < n && cur != sinkv && enlist(c, cur, rstamp)) {
-            int k = atomicAdd(&c.st.cnt[nbk], 1);
-            N[k] = cur;
-        }
+        if (ec > 0 && ldcg(&c.st.h[cur]) < n && cur != sinkv && enlist(c, cur, rstamp))
+            append1(c, cur, N, nbk);
     }
     if (c.lane == 0) {
         c.w_arcs += arcs;
@@ -583,12 +886,15 @@ __device__ void path_push_vertex(QCtx &c, int v, int max_path, int sinkv, int bl
 // Hot-region selection (RA:1902-1946): per-region counts of the worklist,
 // top-K regions with a non-zero count become hot.  CTA 0 of the group
 // bitonic-sorts (count desc, region asc) in shared memory.
-__device__ bool select_hot(QCtx &c, const int *N, int nN, int hot_k) {
-    MF_TRACE(70, nN);
+__device__ bool select_hot(QCtx &c, const int *N, int nNf, int nNb, int hot_k) {
+    MF_TRACE(70, nNf);
     const int R = c.R;
     int *hot = c.st.hot;
     int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
-    for (int i = gt; i < nN; i += gT) atomicAdd(&hot[ldro(&c.rof[ldcg(&N[i])])], 1);
+    for (int i = gt; i < nNf + nNb; i += gT) {
+        int v = i < nNf ? ldcg(&N[i]) : back_at(c, N, i - nNf);
+        atomicAdd(&hot[ldro(&c.rof[v])], 1);
+    }
     if (!c.sync()) return false;
     if (c.crank == 0) {
         __shared__ long long keys[1024];
@@ -619,8 +925,6 @@ __device__ bool select_hot(QCtx &c, const int *N, int nN, int hot_k) {
             long long k = keys[i];
             int r = (int)(k & 0xffff);
             int cntv = INT_MAX - (int)(k >> 16);
-            // reuse hot[] as the flag array: hot iff rank < hot_k and count > 0
-            // (written after all reads above, separated by __syncthreads)
             keys[i] = ((long long)r << 1) | ((i < hot_k && cntv > 0) ? 1 : 0);
         }
         __syncthreads();
@@ -633,16 +937,16 @@ __device__ bool select_hot(QCtx &c, const int *N, int nN, int hot_k) {
 }
 
 // RM (RA:605-657): for kept vertices in active regions with height in the
-// band, every arc v->w with h(w) > h(v)+1, excess(w) <= 0 and residual on
-// w->v has that residual moved from w to v (saturating the steep arc w->v).
-// Residuals updated atomically; w may go negative (a deficit).
+// band, every arc v->w to a kept w with h(w) > h(v)+1, excess(w) <= 0 and
+// residual on w->v has that residual moved from w to v (saturating the steep
+// arc w->v).  Residuals updated atomically; w may go negative (a deficit).
 __device__ bool rm_pass(QCtx &c, int nv, unsigned M, int hlo, int hhi, int s, int t, int *N,
                         int nbk, unsigned rstamp, i64 *ab) {
     const int n = c.n;
     MF_TRACE(80, nv);
     i64 fixed = 0;
     for (int i = c.gw; i < nv; i += c.gW) {
-        int v = ldcg(&c.st.vlist[i]);
+        int v = c.vat(i);
         if (v == s || v == t) continue;
         if (!ldcg(&c.st.ract[ldro(&c.rof[v])])) continue;
         int hv = 0;
@@ -674,11 +978,10 @@ __device__ bool rm_pass(QCtx &c, int nv, unsigned M, int hlo, int hhi, int s, in
         gained = warp_sum_i64(gained);
         bool add = false;
         if (c.lane == 0 && gained > 0) {
-            i64 old = atomic_add_i64(&c.st.ex[v], gained);
-            add = old <= 0 && old + gained > 0 && enlist(c, v, rstamp);
-            if (!add && old > 0) add = enlist(c, v, rstamp);
+            atomic_add_i64(&c.st.ex[v], gained);
+            add = enlist(c, v, rstamp);
         }
-        warp_append(add, v, N, &c.st.cnt[nbk], c.n);
+        append2(c, add, v, N, nbk);
         if (c.lane == 0) {
             c.w_arcs += e1 - b;
             c.w_verts += 1;
@@ -690,10 +993,10 @@ __device__ bool rm_pass(QCtx &c, int nv, unsigned M, int hlo, int hhi, int s, in
 }
 
 // ---------------------------------------------------------------------------
-// The push-relabel driver for one phase set (RA:1450-2115, device-resident):
-// relabel -> rounds of discharge (+ hot sweep, path push, RM, stagnation
-// control) -> relabel ... until a relabel finds nothing to do.
-// final_phase == PH_A: max preflow for (s,t); PH_C: return excess to s.
+// The push-relabel driver (RA:1450-2115, device-resident): relabel -> rounds
+// of discharge (+ hot sweep, path push, RM, stagnation control) -> relabel
+// ... until a relabel finds nothing to do.  start_phase PH_A: maximum preflow
+// for (s,t); PH_C: return excess to s.
 __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsigned M,
                            int start_phase, QOut &qo, int &status) {
     const int n = c.n;
@@ -707,18 +1010,21 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
     int pp_stable = 0, p_count = 64, pp_iter = 0;
     i64 round = 0;
     i64 mask_arcs = ldcg(&c.st.acc[ACC_TOT + T_MASKARCS]);
-    int *L = c.st.qb, *N = c.st.qa;
     for (;;) {
         int sinkv = (phase == PH_A) ? t : (phase == PH_B ? -1 : s);
         int blockv = (phase == PH_C) ? t : s;
         bool defseeds = (phase != PH_C);
-        int na = 0, nd = 0;
+        int naf = 0, nab = 0, nd = 0;
         i64 *ab = nullptr;
-        L = c.st.qb;
-        N = c.st.qa;
-        if (!global_relabel(c, nv, M, sinkv, blockv, s, defseeds, L, na, nd, ab)) return false;
+        int *L = c.st.qb, *N = c.st.qa;
+        int lbk = c.take_bank();
+        u64 t0 = globaltimer_ns();
+        i64 a0 = c.w_arcs;
+        if (!global_relabel(c, nv, M, sinkv, blockv, s, defseeds, L, lbk, naf, nab, nd, ab)) return false;
+        c.tm_relabel += globaltimer_ns() - t0;
+        if (c.lane == 0 && c.w_arcs > a0) atomic_add_i64(&c.st.acc[ACC_TOT + T_RARCS], c.w_arcs - a0);
         qo.relabels++;
-        if (na == 0) {
+        if (naf + nab == 0) {
             if (phase == PH_A) {
                 if (nd == 0) return true;
                 phase = PH_B;
@@ -739,7 +1045,8 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
         i64 work_since = 0;
         int rounds_since = 0;
         bool force_gr = false;
-        while (na > 0) {
+        u64 tr0 = globaltimer_ns();
+        while (naf + nab > 0) {
             if (round >= o.iter_max) {
                 status = MFD_ITER_LIMIT;
                 return true;
@@ -750,6 +1057,7 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
                 atomicCAS(c.err, 0, MFD_TIMEOUT);
             // ---- one discharge round over L -> N
             MF_TRACE(45, (int)round);
+            int na = naf + nab;
             unsigned rstamp = ++c.clock;
             int nbk = c.take_bank();
             i64 *rb = c.take_abank();
@@ -764,7 +1072,7 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
             i64 l_sum = 0, l_high = 0;
             int l_hmin = INT_MAX, l_hmax = -1;
             for (int i = c.gw * 32 + c.lane; i < na; i += c.gW * 32) {
-                int v = ldcg(&L[i]);
+                int v = i < naf ? ldcg(&L[i]) : back_at(c, L, i - naf);
                 i64 ev = ldcg(&c.st.ex[v]);
                 int hv = ldcg(&c.st.h[v]);
                 if (ev > 0 && hv < n) {
@@ -786,9 +1094,10 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
             }
             if (use_pp) {
                 unsigned pstamp = ++c.clock;
-                for (int i = c.gw; i < na; i += c.gW)
-                    path_push_vertex(c, ldcg(&L[i]), o.max_path, sinkv, blockv, N, nbk, rstamp,
-                                     pstamp, rb);
+                for (int i = c.gw; i < na; i += c.gW) {
+                    int v = i < naf ? ldcg(&L[i]) : back_at(c, L, i - naf);
+                    path_push_vertex(c, v, o.max_path, sinkv, blockv, N, nbk, rstamp, pstamp, rb);
+                }
                 pp_stable = 0;
                 if (++pp_iter >= 4) {
                     pp_iter = 0;
@@ -796,11 +1105,9 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
                 }
                 qo.pp_rounds++;
             } else {
-                for (int i = c.gw; i < na; i += c.gW) {
-                    int v = ldcg(&L[i]);
-                    if (!MF_OK_IDX(v, n, 12)) continue;
-                    discharge_vertex(c, v, K, sinkv, blockv, N, nbk, rstamp, rb);
-                }
+                if (nab > 0 && !hub_setup(c, L, nab, nullptr)) return false;
+                discharge_front(c, L, naf, K, sinkv, blockv, N, nbk, rstamp, rb, nullptr);
+                if (nab > 0) discharge_hubs(c, L, nab, sinkv, blockv, N, nbk, rstamp, rb);
             }
             // clear region scratch for this round's optional passes
             {
@@ -811,9 +1118,9 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
                 }
             }
             MF_TRACE(46, (int)round);
-            if (!c.sync()) return false;
+            int nNf = 0, nNb = 0;
+            if (!c.sync_tails(nbk, nNf, nNb)) return false;
             MF_TRACE(47, (int)round);
-            int nN = ldcg(&c.st.cnt[nbk]);
             i64 sum = ldcg(&rb[A_SUMEX]);
             i64 high = ldcg(&rb[A_HIGH]);
             int hmin = (int)ldcg(&rb[A_HMIN]), hmax = (int)ldcg(&rb[A_HMAX]);
@@ -844,29 +1151,30 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
                 calm = 0;
             }
             // hot-region extra sweep over the next worklist (RA:1899-1984)
-            if (o.use_hot && !use_pp && !hotspot && nN >= 64 && (round % 2) == 1 && c.R > 1) {
-                if (!select_hot(c, N, nN, o.hot_k)) return false;
-                for (int i = c.gw; i < nN; i += c.gW) {
-                    int v = ldcg(&N[i]);
-                    if (ldcg(&c.st.hot[ldro(&c.rof[v])]))
-                        discharge_vertex(c, v, K, sinkv, blockv, N, nbk, rstamp, rb);
-                }
-                if (!c.sync()) return false;
-                nN = ldcg(&c.st.cnt[nbk]);
+            if (o.use_hot && !use_pp && !hotspot && nNf + nNb >= 64 && (round % 2) == 1 && c.R > 1) {
+                if (!select_hot(c, N, nNf, nNb, o.hot_k)) return false;
+                if (nNb > 0 && !hub_setup(c, N, nNb, c.st.hot)) return false;
+                discharge_front(c, N, nNf, K, sinkv, blockv, N, nbk, rstamp, rb, c.st.hot);
+                if (nNb > 0) discharge_hubs(c, N, nNb, sinkv, blockv, N, nbk, rstamp, rb);
+                if (!c.sync_tails(nbk, nNf, nNb)) return false;
                 work_since += ldcg(&rb[A_WORK]) - work_round;
                 qo.hot_sweeps++;
             }
             // RM (RA:1991-2097)
-            bool do_rm = o.use_rm && start_phase != PH_C && nN > 0 && (round % rm_freq) == 0 &&
+            bool do_rm = o.use_rm && start_phase != PH_C && nNf + nNb > 0 && (round % rm_freq) == 0 &&
                          (o.force_rm || frac_high >= 0.5f);
             if (do_rm) {
                 int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
-                for (int i = gt; i < nN; i += gT) c.st.ract[ldro(&c.rof[ldcg(&N[i])])] = 1;
+                for (int i = gt; i < nNf + nNb; i += gT) {
+                    int v = i < nNf ? ldcg(&N[i]) : back_at(c, N, i - nNf);
+                    c.st.ract[ldro(&c.rof[v])] = 1;
+                }
                 if (!c.sync()) return false;
                 int hlo = max(0, (hmin == INT_MAX ? 0 : hmin) - 4);
                 int hhi = min(n - 1, (hmax < 0 ? n - 1 : hmax) + 4);
                 if (!rm_pass(c, nv, M, hlo, hhi, s, t, N, nbk, rstamp, rb)) return false;
-                nN = ldcg(&c.st.cnt[nbk]);
+                nNf = ldcg(&c.st.cnt[nbk]);
+                nNb = ldcg(&c.st.cnt[CNT_BACK + nbk]);
                 i64 fixed = ldcg(&rb[A_FIXED]);
                 qo.rm_fixed += fixed;
                 double frac_fix = (double)fixed / (double)max((i64)1, mask_arcs);
@@ -878,12 +1186,14 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
             int *tmp = L;
             L = N;
             N = tmp;
-            na = nN;
+            naf = nNf;
+            nab = nNb;
             bool gr_due = force_gr || rounds_since >= gr_freq ||
                           (o.gr_alpha > 0.0 && (double)work_since >= o.gr_alpha * (double)mask_arcs);
             if (gr_due) break;
         }
-        // relabel (either na == 0 -> exact termination check, or due)
+        c.tm_rounds += globaltimer_ns() - tr0;
+        // relabel (either nothing is active -> exact termination check, or due)
     }
 }
 
@@ -896,7 +1206,7 @@ __device__ bool certify(QCtx &c, int s, int t, int nv, unsigned M, i64 flow, QOu
     i64 *ab = c.take_abank();
     i64 bad = 0;
     for (int i = c.gw; i < nv; i += c.gW) {
-        int v = ldcg(&c.st.vlist[i]);
+        int v = c.vat(i);
         if (c.lane == 0 && v != s && v != t && ldcg(&c.st.ex[v]) != 0) ++bad;
         int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
         for (int e = b + c.lane; e < e1; e += 32) {
@@ -916,10 +1226,10 @@ __device__ bool certify(QCtx &c, int s, int t, int nv, unsigned M, i64 flow, QOu
     int bk = c.take_bank();
     if (c.leader) {
         c.st.qmark[t] = Z;
-        c.st.qa[0] = t;
-        c.st.cnt[bk] = 1;
+        append1(c, t, c.st.qa, bk);
     }
-    if (!c.sync()) return false;
+    int f0 = 0, b0 = 0;
+    if (!c.sync_tails(bk, f0, b0)) return false;
     unsigned *qm = c.st.qmark, *mark = c.st.mark;
     const int *rev = c.rev;
     const i64 *cap = c.cap;
@@ -932,7 +1242,7 @@ __device__ bool certify(QCtx &c, int s, int t, int nv, unsigned M, i64 flow, QOu
         if (r <= 0) return false;
         return atomicMax(&qm[w], Z) < Z;
     };
-    if (!bfs_levels(c, c.st.qa, bk, 1, cut_bfs, nullptr)) return false;
+    if (!bfs_levels(c, c.st.qa, bk, f0, b0, cut_bfs)) return false;
     // cut capacity over all vertices
     i64 cut = 0;
     for (int v = c.gw; v < c.n; v += c.gW) {
@@ -970,30 +1280,31 @@ __device__ bool write_full_residual(QCtx &c, unsigned M, i64 *out) {
 
 // ---------------------------------------------------------------------------
 // Warm start after capacity updates (mode KM_REPAIR).  The slot keeps the
-// previous solve's residual, excess and kept set (meta: M_old, nv_old).
-// 1. old kept vertices get claim stamp O; 2. re-prune on the new capacities;
-// new kept = old kept U new prune; 3. vertices new to the kept set get fresh
-// state and their arc pairs with kept vertices are reopened; 4. each updated
-// arc inside the kept set adjusts its residual, cancelling flow above the
-// new capacity (tail gains excess, head loses it); 5. s re-saturates.
+// previous solve's residual, excess and kept set (meta: M_old, nv_old,
+// vf_old).  1. old kept vertices get claim stamp O; 2. re-prune on the new
+// capacities; new kept = old kept U new prune; 3. vertices new to the kept
+// set get fresh state and their arc pairs with kept vertices are reopened;
+// 4. each updated arc inside the kept set adjusts its residual, cancelling
+// flow above the new capacity (tail gains excess, head loses it); 5. s
+// re-saturates.
 __device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int &nv, bool &t_reach) {
     int *meta = c.st.meta;
-    unsigned M_old = (unsigned)ldcg(&meta[0]);
+    int vf_old = ldcg(&meta[4]);
     int nv_old = ldcg(&meta[1]);
+    c.vf = vf_old;
     unsigned O = ++c.clock;
     for (int i = c.crank * blockDim.x + threadIdx.x; i < nv_old; i += c.G * blockDim.x)
-        c.st.claim[ldcg(&c.st.vlist[i])] = O;
+        c.st.claim[c.vat(i)] = O;
     if (!c.sync()) return false;
     unsigned S = ++c.clock;
     unsigned Mn = ++c.clock;
-    // prune into qb-list of vertices new to the kept set (vlist kept as-is)
     int bank = c.take_bank();
     if (c.leader) {
         c.st.mark[s] = S;
-        c.st.qa[0] = s;
-        c.st.cnt[bank] = 1;
+        append1(c, s, c.st.qa, bank);
     }
-    if (!c.sync()) return false;
+    int f0 = 0, b0 = 0;
+    if (!c.sync_tails(bank, f0, b0)) return false;
     unsigned *mark = c.st.mark, *claim = c.st.claim;
     const i64 *cap = c.cap;
     const int *rev = c.rev;
@@ -1002,47 +1313,52 @@ __device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int
         if (ldcg(&mark[w]) >= S) return false;
         return atomicMax(&mark[w], S) < S;
     };
-    if (!bfs_levels(c, c.st.qa, bank, 1, fwd, nullptr)) return false;
+    if (!bfs_levels(c, c.st.qa, bank, f0, b0, fwd)) return false;
     t_reach = ldcg(&mark[t]) >= S;
     int nb = c.take_bank();
     int addb = c.take_bank();
+    int nbf = 0, nbb = 0;
     if (t_reach) {
         if (c.leader) {
             mark[t] = Mn;
-            c.st.qb[0] = t;
-            c.st.cnt[nb] = 1;
+            append1(c, t, c.st.qb, nb);
         }
-        if (!c.sync()) return false;
+        if (!c.sync_tails(nb, f0, b0)) return false;
         auto bwd = [&](int v, int e, int w, int) -> bool {
             if (ldcg(&mark[w]) != S) return false;
             if (ldro(&cap[ldro(&rev[e])]) <= 0) return false;
             return atomicCAS(&mark[w], S, Mn) == S;
         };
-        if (!bfs_levels(c, c.st.qb, nb, 1, bwd, nullptr)) return false;
+        if (!bfs_levels(c, c.st.qb, nb, f0, b0, bwd)) return false;
+        nbf = ldcg(&c.st.cnt[nb]);
+        nbb = ldcg(&c.st.cnt[CNT_BACK + nb]);
     }
-    int nnew_bfs = t_reach ? ldcg(&c.st.cnt[nb]) : 0;
-    // new kept vertices = bwd-reached not in the old set -> appended to vlist
-    if (c.leader) c.st.cnt[addb] = nv_old;
+    // vertices new to the kept set (bwd-reached, not old) go to the front of
+    // vlist after the old front part; the old back part stays where it is
+    if (c.leader) c.st.cnt[addb] = vf_old;
     if (!c.sync()) return false;
+    int nnew_bfs = nbf + nbb;
     for (int base = c.gw * 32; base < nnew_bfs; base += c.gW * 32) {
         int i = base + c.lane;
         bool add = false;
         int v = 0;
         if (i < nnew_bfs) {
-            v = ldcg(&c.st.qb[i]);
+            v = ldcg(i < nbf ? &c.st.qb[i] : &c.st.qb[c.n - 1 - (i - nbf)]);
             add = ldcg(&claim[v]) != O;
         }
         warp_append(add, v, c.st.vlist, &c.st.cnt[addb], c.n);
     }
     if (!c.sync()) return false;
-    nv = ldcg(&c.st.cnt[addb]);
+    int vf_new = ldcg(&c.st.cnt[addb]);
+    int nadd = vf_new - vf_old;
+    c.vf = vf_new;
+    nv = nv_old + nadd;
     // every kept vertex (old and new) gets the current mask stamp
-    for (int i = c.crank * blockDim.x + threadIdx.x; i < nv; i += c.G * blockDim.x)
-        mark[ldcg(&c.st.vlist[i])] = Mn;
+    for (int i = c.crank * blockDim.x + threadIdx.x; i < nv; i += c.G * blockDim.x) mark[c.vat(i)] = Mn;
     if (!c.sync()) return false;
     // fresh state for new vertices; reopen their arc pairs
     i64 add_arcs = 0;
-    for (int i = nv_old + c.gw; i < nv; i += c.gW) {
+    for (int i = vf_old + c.gw; i < vf_new; i += c.gW) {
         int v = ldcg(&c.st.vlist[i]);
         int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
         if (c.lane == 0) {
@@ -1103,7 +1419,10 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
     int status = MFD_OK;
     const KOpts &o = p.o;
     if (c.leader) {
-        for (int i = 0; i < NBANKS; ++i) c.st.cnt[i] = 0;
+        for (int i = 0; i < NBANKS; ++i) {
+            c.st.cnt[i] = 0;
+            c.st.cnt[CNT_BACK + i] = 0;
+        }
         for (int i = 0; i < 4 * ACC_BANK; ++i) c.st.acc[i] = 0;
         for (int b = 0; b < 4; ++b) {
             c.st.acc[b * ACC_BANK + A_HMIN] = INT_MAX;
@@ -1113,6 +1432,8 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
     }
     c.seq = 0;
     c.aseq = 0;
+    c.vf = 0;
+    c.tm_relabel = c.tm_rounds = 0;
     if (!c.sync()) return;
     unsigned M = 0;
     int nv = 0;
@@ -1141,11 +1462,13 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
         }
     }
     i64 flow = 0;
+    u64 t_pruned = globaltimer_ns();
     if (t_reach && nv > 0) {
         if (p.mode == KM_HEIGHTS) {
-            int na = 0, nd = 0;
+            int naf = 0, nab = 0, nd = 0;
             i64 *ab = nullptr;
-            if (!global_relabel(c, nv, M, t, s, s, true, c.st.qb, na, nd, ab)) return;
+            int lbk = c.take_bank();
+            if (!global_relabel(c, nv, M, t, s, s, true, c.st.qb, lbk, naf, nab, nd, ab)) return;
             int *hd = (int *)p.dbg;
             int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
             for (int v = gt; v < c.n; v += gT)
@@ -1189,11 +1512,16 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
         qo.pushes = tot[T_PUSH];
         qo.t_begin = c.q_begin;
         qo.t_done = globaltimer_ns();
+        qo.t_prune = t_pruned - c.q_begin;
+        qo.t_relabel = c.tm_relabel;
+        qo.t_rounds = c.tm_rounds;
+        qo.arcs_relabel = tot[T_RARCS];
         p.out[q] = qo;
         c.st.meta[0] = (int)M;
         c.st.meta[1] = nv;
         c.st.meta[2] = s;
         c.st.meta[3] = t;
+        c.st.meta[4] = c.vf;
     }
     c.sync();
 }
@@ -1204,7 +1532,8 @@ __global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
     c.crank = blockIdx.x % p.G;
     int gid = blockIdx.x / p.G;
     c.wpc = blockDim.x >> 5;
-    c.gw = c.crank * c.wpc + (threadIdx.x >> 5);
+    c.warp = threadIdx.x >> 5;
+    c.gw = c.crank * c.wpc + c.warp;
     c.gW = p.G * c.wpc;
     c.lane = threadIdx.x & 31;
     c.err = p.err;
@@ -1302,7 +1631,6 @@ __global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
 }
 
 #ifdef MF_CHECKS
-
 static unsigned *h_chk_trace = nullptr;
 static int *h_chk_bad = nullptr;
 static int h_chk_warps = 0;

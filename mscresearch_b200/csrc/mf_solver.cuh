@@ -14,6 +14,19 @@ struct DGraph {
     const int *region_of;  // n
 };
 
+// Vertices with more arcs than this are "hubs": worklists keep them at the
+// back and their arcs are processed in 32-arc chunks by all warps of a group.
+#define HUB_T 512
+
+// Per-hub state of one chunked discharge pass.
+struct HubWork {
+    i64 budget;  // excess not yet handed out to chunks
+    int minh;    // lowest head height over arcs left with residual
+    int done;    // chunks finished
+    int hv;      // hub height at set-up
+    int nch;     // chunks (0 = nothing to do)
+};
+
 // Working state of one residual slot.  All arrays are full-size for the
 // graph the slot serves; stamps make resets unnecessary between queries.
 struct DSlot {
@@ -28,11 +41,13 @@ struct DSlot {
     int *qb;           // n: worklist
     int *hot;          // 1024: region counts / hot flags
     int *ract;         // 1024: active-region flags
-    int *cnt;          // 16 ints: rotating list tails + control words
+    int *cnt;          // 32 ints: rotating list tails (front, back) + control words
     i64 *acc;          // 64 i64: rotating round accumulators + query totals
     GroupBar *bar;     // group barrier
     unsigned *clock;   // persistent stamp clock
-    int *meta;         // per-slot query meta (mask stamp, nv, s, t) for warm starts
+    int *meta;         // per-slot query meta (mask stamp, nv, s, t, front count) for warm starts
+    HubWork *hubw;     // nhub entries
+    int nhub;          // capacity of hubw (hub vertices of the largest graph served)
 };
 
 // Options as seen by the kernel (resolved on the host).
@@ -71,6 +86,10 @@ struct QOut {
     i64 mask_arcs;
     u64 t_begin;   // globaltimer ns when the group took the query
     u64 t_done;    // globaltimer ns when its answer was written
+    u64 t_prune;   // ns in prune + init + preflow
+    u64 t_relabel; // ns in global relabels
+    u64 t_rounds;  // ns in discharge rounds (incl. hot sweep, path push, RM)
+    i64 arcs_relabel; // arc examinations inside global relabels
     int mask_n;
     int status;
 };
