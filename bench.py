@@ -39,7 +39,7 @@ METRIC = "exact max-flow queries/sec + p50/p99 latency, batched vs plain, same B
 WORKLOAD = "rmat20_256q"
 SCALE, DRAWS, NHUB, NUNI, R = 20, 1 << 24, 128, 128, 128
 GRAPH_SEED, QUERY_SEED = 1, 2
-QOUT_BYTES = 152  # device per-query record copied back by mf_solve_batch
+QOUT_BYTES = 160  # device per-query record copied back by mf_solve_batch
 
 
 def peaks():

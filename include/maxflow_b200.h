@@ -45,7 +45,9 @@ typedef struct mf_graph mf_graph;
 /* Solver options.  mf_opts_default() fills the defaults; fields mirror the
  * reference's knobs (RA:1459-1484, RA:1936, RA:2644-2648). */
 typedef struct mf_opts {
-    int kernel_cycles;     /* K: discharge cycles per active vertex per round (RA:1467); 0 = max(4, avg degree) */
+    int kernel_cycles;     /* K: discharge cycles per active vertex per round (RA:1467 uses max(4, avg
+                              degree) with one push per cycle; each cycle here pushes to every
+                              downhill arc); 0 = 4 */
     int gr_freq;           /* rounds between global relabels at most (GR_FREQ0, RA:1466) */
     double gr_work_alpha;  /* also relabel once scanned arcs exceed alpha x mask arcs (0 = off) */
     int prune_mode;        /* 0: RA:1391-1445 mask (fwd(s) & undirected comp(t)); 1: fwd(s) & bwd(t) (default) */
@@ -65,6 +67,8 @@ typedef struct mf_opts {
     int threads;           /* threads per CTA (0 = 512) */
     int certify;           /* 1 = return excess to the source and check the certificate */
     int verbose;           /* 1 = per-query log lines on stderr */
+    int use_kept_cache;    /* 1 = queries with s and t in the graph's cached strongly connected
+                              component take it as their kept set (prune_mode 1 only) */
 } mf_opts;
 
 /* Per-query statistics (all counts exact device counters). */

@@ -158,11 +158,12 @@ class Graph:
         _check(rc)
         return f.value, st
 
-    def prune_mask(self, s, t, mode=1):
+    def prune_mask(self, s, t, mode=1, use_kept_cache=1):
         n = self.info[0]
         m = np.zeros(n, np.uint8)
         kept = C.c_int()
-        _check(lib.mf_debug_prune_mask(self._h, int(s), int(t), C.byref(opts(prune_mode=mode)),
+        _check(lib.mf_debug_prune_mask(self._h, int(s), int(t),
+                                       C.byref(opts(prune_mode=mode, use_kept_cache=use_kept_cache)),
                                        _p(m, C.c_uint8), C.byref(kept)))
         return m
 

@@ -40,6 +40,7 @@ class MfOpts(C.Structure):
         ("threads", C.c_int),
         ("certify", C.c_int),
         ("verbose", C.c_int),
+        ("use_kept_cache", C.c_int),
     ]
 
 

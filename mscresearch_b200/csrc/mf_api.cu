@@ -204,6 +204,15 @@ struct mf_graph {
     int R = 0;
     int avg_deg = 0;
     int nhub = 0;  // vertices with more than HUB_T arcs
+    int pivot = 0;  // internal id of the highest-degree vertex (kept-set cache pivot)
+    // kept-set cache (see DGraph)
+    unsigned char *kc_in = nullptr;
+    int *kc_img = nullptr;
+    i64 *kc_res = nullptr;
+    int kc_f = 0, kc_b = 0;
+    i64 kc_arcs = 0;
+    bool kc_valid = false;
+    bool kc_tried = false;
     std::vector<int> new_id;  // caller id -> internal id
     std::vector<int> old_id;  // internal id -> caller id
     std::vector<double> score_caller;
@@ -243,7 +252,19 @@ struct mf_session {
 
 namespace {
 
+void free_kept_cache(mf_graph *g) {
+    cudaFree(g->kc_in);
+    cudaFree(g->kc_img);
+    cudaFree(g->kc_res);
+    g->kc_in = nullptr;
+    g->kc_img = nullptr;
+    g->kc_res = nullptr;
+    g->kc_valid = false;
+    g->kc_tried = false;
+}
+
 void free_graph_arrays(mf_graph *g) {
+    free_kept_cache(g);
     cudaFree(g->row);
     cudaFree(g->col);
     cudaFree(g->rev);
@@ -256,6 +277,33 @@ void free_graph_arrays(mf_graph *g) {
     g->cap = nullptr;
     g->fwd = nullptr;
     g->d_graph = nullptr;
+}
+
+DGraph make_dgraph(const mf_graph *g) {
+    DGraph dg{};
+    dg.n = g->n;
+    dg.R = g->R;
+    dg.arcs = g->arcs;
+    dg.row = g->row;
+    dg.col = g->col;
+    dg.rev = g->rev;
+    dg.cap = g->cap;
+    dg.region_of = g->region_of;
+    if (g->kc_valid) {
+        dg.kc_in = g->kc_in;
+        dg.kc_img = g->kc_img;
+        dg.kc_res = g->kc_res;
+        dg.kc_f = g->kc_f;
+        dg.kc_b = g->kc_b;
+        dg.kc_arcs = g->kc_arcs;
+    }
+    return dg;
+}
+
+int upload_dgraph(mf_graph *g) {
+    DGraph dg = make_dgraph(g);
+    CK(cudaMemcpy(g->d_graph, &dg, sizeof(DGraph), cudaMemcpyHostToDevice));
+    return MF_OK;
 }
 
 // Partition + reorder the device CSR given in (row,col,cap,rev,fwd), whose
@@ -313,10 +361,16 @@ int partition_into(mf_graph *g, int R, int *row, int *col, i64 *cap, int *rev, u
     g->new_id.swap(new_id);
     g->old_id.swap(old_id);
     g->R = R;
-    DGraph dg{n, R, arcs, g->row, g->col, g->rev, g->cap, g->region_of};
+    int best = 0;
+    {
+        std::vector<int> rw(n + 1);
+        CK(cudaMemcpy(rw.data(), g->row, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+        for (int x = 1; x < n; ++x)
+            if (rw[x + 1] - rw[x] > rw[best + 1] - rw[best]) best = x;
+    }
+    g->pivot = best;
     CK(cudaMalloc(&g->d_graph, sizeof(DGraph)));
-    CK(cudaMemcpy(g->d_graph, &dg, sizeof(DGraph), cudaMemcpyHostToDevice));
-    return MF_OK;
+    return upload_dgraph(g);
 }
 
 int ensure_launch_buffers(mf_graph *g, int nq, int nslots) {
@@ -353,7 +407,8 @@ int ensure_launch_buffers(mf_graph *g, int nq, int nslots) {
 
 KOpts resolve_opts(const mf_opts &o, int avg_deg) {
     KOpts k;
-    k.K = o.kernel_cycles > 0 ? o.kernel_cycles : std::max(4, avg_deg);
+    k.K = o.kernel_cycles > 0 ? o.kernel_cycles : 4;
+    (void)avg_deg;
     k.gr_freq = std::max(1, o.gr_freq);
     k.gr_alpha = o.gr_work_alpha;
     k.prune_mode = o.prune_mode;
@@ -368,6 +423,7 @@ KOpts resolve_opts(const mf_opts &o, int avg_deg) {
     k.stagnate = std::max(1, o.stagnate_rounds);
     k.force_rm = o.force_rm;
     k.force_pp = o.force_path_push;
+    k.use_cache = o.use_kept_cache;
     k.iter_max = o.iter_max > 0 ? o.iter_max : 20000000;
     return k;
 }
@@ -588,6 +644,7 @@ void mf_opts_default(mf_opts *o) {
     o->threads = 512;
     o->certify = 0;
     o->verbose = 0;
+    o->use_kept_cache = 1;
 }
 
 const char *mf_last_error_string(void) { return g_err.c_str(); }
@@ -731,6 +788,69 @@ int mf_graph_export(const mf_graph *g, int32_t *row, int32_t *col, int64_t *cap,
     return MF_OK;
 }
 
+// kc_res[e] = cap[e] if both ends of e are in the component, else 0;
+// kc_arcs = arcs out of component vertices.
+__global__ void k_kept_res(int n, const int *row, const int *col, const i64 *cap,
+                           const unsigned char *in, i64 *res, unsigned long long *arcs) {
+    int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    int nw = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long mine = 0;
+    for (int v = w; v < n; v += nw) {
+        bool iv = in[v];
+        int b = row[v], e1 = row[v + 1];
+        for (int e = b + lane; e < e1; e += 32) res[e] = (iv && in[col[e]]) ? cap[e] : 0;
+        if (iv && lane == 0) mine += (unsigned long long)(e1 - b);
+    }
+    if (lane == 0 && mine) atomicAdd(arcs, mine);
+}
+
+// Builds the kept-set cache once per graph state (prune mode 1 only): the
+// strongly connected component of the highest-degree vertex, found by the
+// solver's own prune with s = t = pivot.
+static int ensure_kept_cache(mf_graph *g, const mf_opts &o) {
+    if (g->kc_valid || g->kc_tried || o.prune_mode != 1 || !o.use_kept_cache) return MF_OK;
+    g->kc_tried = true;
+    int n = g->n;
+    KcOut ko{};
+    CK(cudaMalloc(&g->kc_in, n));
+    CK(cudaMalloc(&g->kc_img, sizeof(int) * (size_t)n));
+    CK(cudaMalloc(&g->kc_res, sizeof(i64) * (size_t)std::max<i64>(g->arcs, 1)));
+    CK(cudaMemset(g->kc_in, 0, n));
+    ko.img = g->kc_img;
+    ko.in = g->kc_in;
+    KcOut *dko = nullptr;
+    CK(cudaMalloc(&dko, sizeof(KcOut)));
+    CK(cudaMemcpy(dko, &ko, sizeof(KcOut), cudaMemcpyHostToDevice));
+    int piv = g->pivot;
+    QOut out;
+    int rc = launch(g, g->pool, 1, &piv, &piv, false, o, KM_KEPTSET, dko, nullptr, 0, 0, &out);
+    cudaFree(dko);
+    if (rc) {
+        free_kept_cache(g);
+        g->kc_tried = true;
+        return rc;
+    }
+    g->kc_f = out.kept_front;
+    g->kc_b = out.mask_n - out.kept_front;
+    unsigned long long *darcs = nullptr;
+    CK(cudaMalloc(&darcs, sizeof(unsigned long long)));
+    CK(cudaMemset(darcs, 0, sizeof(unsigned long long)));
+    k_kept_res<<<g->dev.sms * 8, 256, 0, g->stream>>>(n, g->row, g->col, g->cap, g->kc_in, g->kc_res, darcs);
+    unsigned long long ka = 0;
+    CK(cudaMemcpyAsync(&ka, darcs, sizeof(ka), cudaMemcpyDeviceToHost, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    cudaFree(darcs);
+    g->kc_arcs = (i64)ka;
+    g->kc_valid = out.mask_n >= 2;
+    if (!g->kc_valid) {
+        bool tried = true;
+        free_kept_cache(g);
+        g->kc_tried = tried;
+        return MF_OK;
+    }
+    return upload_dgraph(g);
+}
+
 static int solve_common(mf_graph *g, int nq, const int32_t *s, const int32_t *t, const mf_opts *opts,
                         int64_t *flows, mf_stats *stats, int mode, void *dbg, bool single) {
     if (!g) return fail(MF_ERR_ARG, "graph is NULL");
@@ -741,6 +861,8 @@ static int solve_common(mf_graph *g, int nq, const int32_t *s, const int32_t *t,
     else mf_opts_default(&o);
     std::vector<int> si(nq), ti(nq);
     for (int i = 0; i < nq; ++i) to_internal(g, s[i], t[i], si[i], ti[i]);
+    int rc0 = ensure_kept_cache(g, o);
+    if (rc0) return rc0;
     std::vector<QOut> outs(nq);
     int G = single ? 0 : (o.group_ctas > 0 ? o.group_ctas : 2);
     int rc = launch(g, g->pool, nq, si.data(), ti.data(), false, o, mode, dbg, nullptr, 0, G, outs.data());
@@ -893,6 +1015,12 @@ static int resolve_updates(mf_graph *g, int nb, const int32_t *u, const int32_t 
 static int apply_updates(mf_graph *g, const std::vector<ArcUpdate> &ups, ArcUpdate **d_out) {
     *d_out = nullptr;
     if (ups.empty()) return MF_OK;
+    // capacities change reachability: drop the kept-set cache (rebuilt lazily)
+    if (g->kc_valid || g->kc_tried) {
+        free_kept_cache(g);
+        int rc = upload_dgraph(g);
+        if (rc) return rc;
+    }
     ArcUpdate *d = nullptr;
     CK(cudaMalloc(&d, sizeof(ArcUpdate) * ups.size()));
     CK(cudaMemcpy(d, ups.data(), sizeof(ArcUpdate) * ups.size(), cudaMemcpyHostToDevice));
@@ -1112,7 +1240,12 @@ int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int ma
         hmax = std::max(hmax, g->nhub);
         arcs_sum += g->arcs;
         n_sum += g->n;
-        dg[i] = DGraph{g->n, g->R, g->arcs, g->row, g->col, g->rev, g->cap, g->region_of};
+        int rc0 = ensure_kept_cache(g, sv->opts);
+        if (rc0) {
+            delete sv;
+            return rc0;
+        }
+        dg[i] = make_dgraph(g);
     }
     sv->ko = resolve_opts(sv->opts, (int)(arcs_sum / std::max<i64>(1, n_sum)));
     DevInfo di;

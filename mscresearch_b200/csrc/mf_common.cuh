@@ -24,6 +24,7 @@ typedef unsigned long long u64;
 // L2-coherent loads (cg) so that no SM serves a stale L1 line.
 __device__ __forceinline__ int ldro(const int *p) { return __ldg(p); }
 __device__ __forceinline__ i64 ldro(const i64 *p) { return __ldg(p); }
+__device__ __forceinline__ unsigned char ldro_u8(const unsigned char *p) { return __ldg(p); }
 __device__ __forceinline__ int ldcg(const int *p) { return __ldcg(p); }
 __device__ __forceinline__ unsigned ldcg(const unsigned *p) { return __ldcg(p); }
 __device__ __forceinline__ i64 ldcg(const i64 *p) { return __ldcg(p); }

@@ -92,6 +92,7 @@ struct QCtx {
     int n, R;
     const int *row, *col, *rev, *rof;
     const i64 *cap;
+    const DGraph *gr;
     // slot
     DSlot st;
     int vf;  // kept vertices in the front part of vlist (the rest are at the back)
@@ -1443,7 +1444,45 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
     } else {
         unsigned S = ++c.clock;
         M = ++c.clock;
-        if (!prune(c, s, t, o.prune_mode, S, M, nv, t_reach)) return;
+        const DGraph &g = *c.gr;
+        bool cached = p.mode != KM_KEPTSET && o.prune_mode == 1 && o.use_cache && g.kc_in &&
+                      ldro_u8(&g.kc_in[s]) && ldro_u8(&g.kc_in[t]);
+        if (cached) {
+            // s and t lie in the cached component: it is the kept set
+            nv = g.kc_f + g.kc_b;
+            c.vf = g.kc_f;
+            t_reach = true;
+            int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+            for (int i = gt; i < nv; i += gT) {
+                int pos = i < g.kc_f ? i : c.n - 1 - (i - g.kc_f);
+                int v = ldro(&g.kc_img[pos]);
+                c.st.vlist[pos] = v;
+                c.st.mark[v] = M;
+                c.st.ex[v] = 0;
+                c.st.h[v] = 0;
+            }
+            if (c.leader) c.st.acc[ACC_TOT + T_MASKARCS] = g.kc_arcs;
+            if (!c.sync()) return;
+        } else if (!prune(c, s, t, o.prune_mode, S, M, nv, t_reach)) {
+            return;
+        }
+        if (p.mode == KM_KEPTSET) {
+            KcOut *ko = (KcOut *)p.dbg;
+            int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+            for (int i = gt; i < nv; i += gT) {
+                int pos = i < c.vf ? i : c.n - 1 - (i - c.vf);
+                int v = ldcg(&c.st.vlist[pos]);
+                ko->img[pos] = v;
+                ko->in[v] = 1;
+            }
+            if (c.leader) {
+                qo.mask_n = nv;
+                qo.kept_front = c.vf;
+                p.out[q] = qo;
+            }
+            c.sync();
+            return;
+        }
         if (p.mode == KM_PRUNE) {
             unsigned char *mk = (unsigned char *)p.dbg;
             int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
@@ -1457,7 +1496,21 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
             return;
         }
         if (t_reach && nv > 0) {
-            if (!init_state(c, nv, M)) return;
+            if (cached) {
+                // initial residuals of the component, copied whole (16-byte
+                // vectors); ex/h were set with the kept list above
+                const longlong2 *src = reinterpret_cast<const longlong2 *>(g.kc_res);
+                longlong2 *dst = reinterpret_cast<longlong2 *>(c.st.res);
+                i64 A = ldro(&c.row[c.n]);
+                i64 nvec = A >> 1;
+                int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+                for (i64 k = gt; k < nvec; k += gT) dst[k] = __ldg(&src[k]);
+                if (gt == 0 && (A & 1)) c.st.res[A - 1] = ldro(&g.kc_res[A - 1]);
+                if (c.lane == 0 && c.gw == 0) c.w_verts += nv;
+                if (!c.sync()) return;
+            } else if (!init_state(c, nv, M)) {
+                return;
+            }
             if (!preflow(c, s)) return;
         }
     }
@@ -1604,10 +1657,11 @@ __global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
         c.rev = g.rev;
         c.rof = g.region_of;
         c.cap = g.cap;
+        c.gr = &p.graphs[gi];
         c.st = p.slots[si];
         c.clock = ldcg(c.st.clock);
         c.q_begin = globaltimer_ns();
-        if (s < 0 || t < 0 || s >= g.n || t >= g.n || s == t) {
+        if (s < 0 || t < 0 || s >= g.n || t >= g.n || (s == t && p.mode != KM_KEPTSET)) {
             if (c.leader) {
                 QOut z = {};
                 z.t_begin = z.t_done = c.q_begin;

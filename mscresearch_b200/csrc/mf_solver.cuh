@@ -12,6 +12,16 @@ struct DGraph {
     const int *rev;        // arcs
     const i64 *cap;        // arcs (current capacities)
     const int *region_of;  // n
+    // Kept-set cache: the strongly connected component of a pivot vertex.
+    // For s and t both in it, fwd(s) & bwd(t) is exactly that component, so
+    // a query can take its kept list (vlist layout: front kc_f entries, back
+    // kc_b entries) and initial residuals (kc_res: cap, arcs to heads outside
+    // the component 0) instead of pruning.  kc_in == NULL: no cache.
+    const unsigned char *kc_in;  // n: 1 = in the component
+    const int *kc_img;           // n: kept list image
+    const i64 *kc_res;           // arcs: initial residuals
+    int kc_f, kc_b;
+    i64 kc_arcs;                 // arcs out of the component's vertices
 };
 
 // Vertices with more arcs than this are "hubs": worklists keep them at the
@@ -67,6 +77,7 @@ struct KOpts {
     int stagnate;
     int force_rm;
     int force_pp;
+    int use_cache;
     i64 iter_max;
 };
 
@@ -92,6 +103,8 @@ struct QOut {
     i64 arcs_relabel; // arc examinations inside global relabels
     int mask_n;
     int status;
+    int kept_front;  // kept vertices in vlist's front part
+    int pad;
 };
 
 // One capacity change, resolved to an arc (region-ordered index).
@@ -109,6 +122,14 @@ enum KMode {
     KM_CERTIFY = 3,     // solve + return excess to source + certificate checks
     KM_RESIDUAL = 4,    // solve, then write full-graph residuals into dbg (i64 per arc)
     KM_REPAIR = 5,      // warm start from the slot's kept state after capacity updates
+    KM_KEPTSET = 6,     // prune from a pivot (s == t): the pivot's SCC; kept list image and
+                        // membership written to the KcOut in dbg
+};
+
+// Output of KM_KEPTSET.
+struct KcOut {
+    int *img;             // n: kept list image (vlist layout)
+    unsigned char *in;    // n: membership (caller zeroes it)
 };
 
 struct KParams {

@@ -92,11 +92,11 @@ def rmat14():
     eg.close()
 
 
-@pytest.mark.parametrize("mode", [0, 1])
-def test_prune_masks_match_oracle(rmat14, mode):
+@pytest.mark.parametrize("mode,cache", [(0, 1), (1, 1), (1, 0)])
+def test_prune_masks_match_oracle(rmat14, mode, cache):
     n, u, v, c, g, s, t, eg = rmat14
     for a, b in list(zip(s, t))[:10] + [(0, 1), (5, 5)]:
-        m = eg.prune_mask(a, b, mode)
+        m = eg.prune_mask(a, b, mode, cache)
         if a == b:
             assert m.sum() == 0
             continue
@@ -158,7 +158,10 @@ def test_device_certificate(rmat14):
     dict(use_rm=0, use_path_push=0, use_hot_sweep=0, gr_freq=1, gr_work_alpha=0.0),
     dict(kernel_cycles=64, gr_freq=100000, gr_work_alpha=0.0),
     dict(prune_mode=0),
-], ids=["rm", "path_push", "hot", "relabel_every_round", "rare_relabel", "ref_prune"])
+    dict(use_kept_cache=0),
+    dict(kernel_cycles=32),
+], ids=["rm", "path_push", "hot", "relabel_every_round", "rare_relabel", "ref_prune", "no_kept_cache",
+        "k32"])
 def test_heuristics_stay_exact(rmat14, kw):
     n, u, v, c, g, s, t, eg = rmat14
     exp = oracle_flows(g, s, t)
