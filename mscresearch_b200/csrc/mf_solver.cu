@@ -159,17 +159,18 @@ __device__ __forceinline__ int back_at(const QCtx &c, const int *L, int k) { ret
 // front (cnt[bank]) or, when w has more than HUB_T arcs, at the back
 // (cnt[CNT_BACK + bank], stored at L[n-1-k]).  One atomicAdd per class per
 // warp.  All 32 lanes must call it.
-__device__ __forceinline__ void append2(QCtx &c, bool flag, int w, int *L, int bank) {
-    unsigned any = __ballot_sync(MF_FULL, flag);
+__device__ __forceinline__ void append2(QCtx &c, bool flag, int w, int *L, int bank,
+                                        unsigned mask = MF_FULL) {
+    unsigned any = __ballot_sync(mask, flag);
     if (any == 0) return;
     bool hub = false;
     if (flag) hub = c.deg(w) > HUB_T;
-    unsigned fm = __ballot_sync(MF_FULL, flag && !hub);
+    unsigned fm = __ballot_sync(mask, flag && !hub);
     unsigned bm = any & ~fm;
     if (fm) {
         int ld = __ffs(fm) - 1, base = 0;
         if (c.lane == ld) base = atomicAdd(&c.st.cnt[bank], __popc(fm));
-        base = __shfl_sync(MF_FULL, base, ld);
+        base = __shfl_sync(mask, base, ld);
         if (flag && !hub) {
             int pos = base + __popc(fm & lanemask_lt());
             if (MF_OK_IDX(pos, c.n, 91)) L[pos] = w;
@@ -178,7 +179,7 @@ __device__ __forceinline__ void append2(QCtx &c, bool flag, int w, int *L, int b
     if (bm) {
         int ld = __ffs(bm) - 1, base = 0;
         if (c.lane == ld) base = atomicAdd(&c.st.cnt[CNT_BACK + bank], __popc(bm));
-        base = __shfl_sync(MF_FULL, base, ld);
+        base = __shfl_sync(mask, base, ld);
         if (flag && hub) {
             int k = base + __popc(bm & lanemask_lt());
             if (MF_OK_IDX(k, c.n, 92)) L[c.n - 1 - k] = w;
@@ -523,39 +524,42 @@ __device__ __forceinline__ bool enlist(QCtx &c, int w, unsigned rstamp) {
     return atomicMax(&c.st.qmark[w], rstamp) < rstamp;
 }
 
-// Warp-cooperative discharge of one vertex (medium degree) for up to K
-// cycles.  Each cycle scans v's arcs 32 at a time: lanes read residual +
+// Cooperative discharge of one vertex by a tile of TW lanes (TW = 8 or 32;
+// the tile is lanes [tb, tb+TW) of the warp, mask its lane mask) for up to
+// K cycles.  Each cycle scans v's arcs TW at a time: lanes read residual +
 // head height, a ballot finds downhill residual arcs, a 64-bit inclusive
 // shuffle scan splits the remaining excess over them in arc order, and every
 // lane pushes its share with native 64-bit atomics.  If excess remains after
 // all arcs, v is relabeled to 1 + the lowest height over arcs that still
 // have residual (n when none).  Newly active heads and v itself (if still
 // active) are appended to N.
-__device__ void discharge_vertex(QCtx &c, int v, int K, int sinkv, int blockv, int *N, int nbk,
-                                 unsigned rstamp, i64 *ab) {
+template <int TW>
+__device__ void discharge_tile(QCtx &c, int v, int K, int sinkv, int blockv, int *N, int nbk,
+                               unsigned rstamp, i64 *ab, unsigned mask, int tb) {
     const int n = c.n;
+    const int tl = c.lane - tb;  // lane within the tile
     MF_TRACE(50, v);
-    // Height and excess steer warp-wide branches below: read them once on
-    // lane 0 and broadcast.  Under independent thread scheduling the lanes
-    // of a warp need not load at the same moment, and another warp may change
-    // h[v] / ex[v] in between; per-lane copies could then disagree and split
-    // the warp across full-mask shuffles.
+    // Height and excess steer tile-wide branches below: read them once on
+    // the tile's first lane and broadcast.  Under independent thread
+    // scheduling the lanes need not load at the same moment, and another warp
+    // may change h[v] / ex[v] in between; per-lane copies could then disagree
+    // and split the tile across its shuffles.
     int hv = 0;
     i64 ev = 0;
-    if (c.lane == 0) {
+    if (tl == 0) {
         hv = ldcg(&c.st.h[v]);
         ev = ldcg(&c.st.ex[v]);
     }
-    hv = __shfl_sync(MF_FULL, hv, 0);
-    ev = __shfl_sync(MF_FULL, ev, 0);
+    hv = __shfl_sync(mask, hv, 0, TW);
+    ev = __shfl_sync(mask, ev, 0, TW);
     int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
     i64 pushes = 0, arcs = 0;
     for (int cyc = 0; cyc < K; ++cyc) {
         if (ev <= 0 || hv >= n) break;
         i64 rem = ev;
         int minh = MF_INF_H;
-        for (int base = b; base < e1; base += 32) {
-            int e = base + c.lane;
+        for (int base = b; base < e1; base += TW) {
+            int e = base + tl;
             i64 r = 0;
             int w = 0, hw = MF_INF_H;
             if (e < e1) {
@@ -566,40 +570,45 @@ __device__ void discharge_vertex(QCtx &c, int v, int K, int sinkv, int blockv, i
                 }
             }
             bool adm = r > 0 && hw < hv;
-            unsigned am = __ballot_sync(MF_FULL, adm);
+            unsigned am = __ballot_sync(mask, adm);
             i64 d = 0;
             bool act = false;
             if (am) {
                 i64 x = adm ? r : 0;
-                i64 incl = warp_incl_scan_i64(x);
+                i64 incl = x;
+#pragma unroll
+                for (int o = 1; o < TW; o <<= 1) {
+                    i64 y = __shfl_up_sync(mask, incl, o, TW);
+                    if (tl >= o) incl += y;
+                }
                 i64 excl = incl - x;
                 if (adm && rem > excl) d = min(r, rem - excl);
                 if (d > 0) act = push_arc(c, e, w, d, sinkv, blockv);
-                i64 tot = __shfl_sync(MF_FULL, incl, 31);
+                i64 tot = __shfl_sync(mask, incl, TW - 1, TW);
                 rem -= min(tot, rem);
-                pushes += __popc(__ballot_sync(MF_FULL, d > 0));
+                pushes += __popc(__ballot_sync(mask, d > 0));
             }
             if (r - d > 0) minh = min(minh, hw);
             bool add = act && enlist(c, w, rstamp);
-            append2(c, add, w, N, nbk);
-            arcs += min(32, e1 - base);
+            append2(c, add, w, N, nbk, mask);
+            arcs += min(TW, e1 - base);
             if (rem == 0) break;
         }
         i64 pushed = ev - rem;
-        if (c.lane == 0 && pushed) atomic_add_i64(&c.st.ex[v], -pushed);
+        if (tl == 0 && pushed) atomic_add_i64(&c.st.ex[v], -pushed);
         if (rem > 0) {
-            int mh = __reduce_min_sync(MF_FULL, minh);
+            int mh = __reduce_min_sync(mask, minh);
             hv = (mh >= n - 1) ? n : mh + 1;
-            if (c.lane == 0) c.st.h[v] = hv;
+            if (tl == 0) c.st.h[v] = hv;
         }
-        __syncwarp();
-        if (c.lane == 0) ev = ldcg(&c.st.ex[v]);
-        ev = __shfl_sync(MF_FULL, ev, 0);
+        __syncwarp(mask);
+        if (tl == 0) ev = ldcg(&c.st.ex[v]);
+        ev = __shfl_sync(mask, ev, 0, TW);
     }
     MF_TRACE(51, v);
-    bool again = (c.lane == 0) && ev > 0 && hv < n && enlist(c, v, rstamp);
-    append2(c, again, v, N, nbk);
-    if (c.lane == 0) {
+    bool again = (tl == 0) && ev > 0 && hv < n && enlist(c, v, rstamp);
+    append2(c, again, v, N, nbk, mask);
+    if (tl == 0) {
         c.w_arcs += arcs;
         c.w_verts += 1;
         c.w_push += pushes;
@@ -607,98 +616,52 @@ __device__ void discharge_vertex(QCtx &c, int v, int K, int sinkv, int blockv, i
     }
 }
 
-// Discharge of the front part L[0, nf): each warp takes 32 entries.  Lanes
-// whose vertex has at most SMALL_T arcs discharge it themselves, in lockstep
-// over arc slots (greedy pushes to downhill arcs in arc order, per-lane
-// relabel, warp-aggregated appends); the warp then discharges the other
-// (medium) vertices one at a time, cooperatively, with its cycles capped so
-// that one vertex scans at most about K x 32 arcs per round.  hot != NULL
-// restricts the pass to vertices of hot regions.
+__device__ __forceinline__ void discharge_vertex(QCtx &c, int v, int K, int sinkv, int blockv, int *N,
+                                                 int nbk, unsigned rstamp, i64 *ab) {
+    discharge_tile<32>(c, v, K, sinkv, blockv, N, nbk, rstamp, ab, MF_FULL, 0);
+}
+
+// Discharge of the front part L[0, nf): each warp takes 32 entries.
+// Vertices with at most SMALL_T arcs go to 8-lane tiles, four at a time (a
+// tile reads 8 consecutive arcs per step); the others get the whole warp,
+// with cycles capped so that one vertex scans at most about K x 32 arcs per
+// round.  hot != NULL restricts the pass to vertices of hot regions.
 __device__ void discharge_front(QCtx &c, const int *L, int nf, int K, int sinkv, int blockv,
                                 int *N, int nbk, unsigned rstamp, i64 *ab, const int *hot) {
     const int n = c.n;
     for (int base = c.gw * 32; base < nf; base += c.gW * 32) {
         int i = base + c.lane;
-        int v = -1, b = 0, d = 0;
+        int v = -1, d = 0;
         if (i < nf) {
             v = ldcg(&L[i]);
             if (!MF_OK_IDX(v, n, 12)) v = -1;
             else if (hot && !ldcg(&hot[ldro(&c.rof[v])])) v = -1;
         }
-        if (v >= 0) {
-            b = ldro(&c.row[v]);
-            d = ldro(&c.row[v + 1]) - b;
-        }
+        if (v >= 0) d = c.deg(v);
         bool small = v >= 0 && d <= SMALL_T;
-        // ---- one vertex per lane
-        i64 ev = 0;
-        int hv = n;
-        if (small) {
-            hv = ldcg(&c.st.h[v]);
-            ev = ldcg(&c.st.ex[v]);
+        unsigned sm = __ballot_sync(MF_FULL, small);
+        unsigned med = __ballot_sync(MF_FULL, v >= 0 && !small);
+        // small vertices: 8-lane tiles, four per step
+        const int tile = c.lane >> 3, tb = tile << 3;
+        const unsigned tmask = 0xffu << tb;
+        while (sm) {
+            // the k-th set bit of sm for k = tile
+            unsigned rest = sm;
+            for (int k = 0; k < tile && rest; ++k) rest &= rest - 1;
+            int src = rest ? __ffs(rest) - 1 : -1;
+            int vt = __shfl_sync(MF_FULL, v, src < 0 ? 0 : src);
+            for (int k = 0; k < 4 && sm; ++k) sm &= sm - 1;
+            if (src >= 0) discharge_tile<8>(c, vt, K, sinkv, blockv, N, nbk, rstamp, ab, tmask, tb);
+            __syncwarp();
         }
-        bool act = small && ev > 0 && hv < n;
-        i64 arcs = 0, pushes = 0;
-        for (int cyc = 0; cyc < K; ++cyc) {
-            if (!__any_sync(MF_FULL, act)) break;
-            int md = __reduce_max_sync(MF_FULL, act ? d : 0);
-            i64 rem = ev;
-            int minh = MF_INF_H;
-            bool scan = act;
-            for (int j = 0; j < md; ++j) {
-                bool add = false;
-                int w = 0;
-                if (scan && j < d) {
-                    int e = b + j;
-                    i64 r = ldcg(&c.st.res[e]);
-                    ++arcs;
-                    if (r > 0) {
-                        w = ldro(&c.col[e]);
-                        int hw = ldcg(&c.st.h[w]);
-                        i64 dd = 0;
-                        if (hw < hv) {
-                            dd = min(r, rem);
-                            add = push_arc(c, e, w, dd, sinkv, blockv);
-                            rem -= dd;
-                            ++pushes;
-                        }
-                        if (r - dd > 0) minh = min(minh, hw);
-                        if (rem == 0) scan = false;
-                    }
-                }
-                if (add) add = enlist(c, w, rstamp);
-                append2(c, add, w, N, nbk);
-            }
-            if (act) {
-                i64 pushed = ev - rem;
-                if (pushed) atomic_add_i64(&c.st.ex[v], -pushed);
-                if (rem > 0) {
-                    hv = (minh >= n - 1) ? n : minh + 1;
-                    c.st.h[v] = hv;
-                }
-                ev = ldcg(&c.st.ex[v]);
-                act = ev > 0 && hv < n;
-            }
-        }
-        bool again = small && ev > 0 && hv < n && enlist(c, v, rstamp);
-        append2(c, again, v, N, nbk);
-        arcs = warp_sum_i64(arcs);
-        pushes = warp_sum_i64(pushes);
-        if (c.lane == 0) {
-            c.w_arcs += arcs;
-            c.w_push += pushes;
-            c.w_verts += min(32, nf - base);
-            if (arcs) atomic_add_i64(&ab[A_WORK], arcs);
-        }
-        // ---- medium vertices: one warp each
-        unsigned med = __ballot_sync(MF_FULL, v >= 0 && d > SMALL_T);
+        // medium vertices: one warp each
         while (med) {
             int o = __ffs(med) - 1;
             med &= med - 1;
             int vo = __shfl_sync(MF_FULL, v, o);
             int dv = __shfl_sync(MF_FULL, d, o);
             int Kv = max(1, min(K, (K * 32) / max(dv, 1)));
-            discharge_vertex(c, vo, Kv, sinkv, blockv, N, nbk, rstamp, ab);
+            discharge_tile<32>(c, vo, Kv, sinkv, blockv, N, nbk, rstamp, ab, MF_FULL, 0);
         }
     }
 }
