@@ -177,6 +177,12 @@ def run_engine(args):
     g = mf.Graph.from_edges(n, u, v, c, R=R)
     _, arcs, _ = g.info
     o = mf.opts(group_ctas=args.group)
+    if args.K:
+        o.kernel_cycles = args.K
+    if args.gr_freq:
+        o.gr_freq = args.gr_freq
+    if args.gr_alpha is not None:
+        o.gr_work_alpha = args.gr_alpha
     nq = len(s)
     # warm-up (also sizes the residual slot pool)
     for _ in range(args.warmup):
@@ -236,6 +242,7 @@ def run_engine(args):
         "data": "synthetic (seeded R-MAT 2^20, 2^24 draws, caps U[1,1000]; 128 hub + 128 uniform queries)",
         "config": {"workload": "rmat%d_%dq" % (args.scale, nq), "n": n, "edges": len(u), "arcs": arcs, "queries_per_gpu": nq,
                    "R": R, "prune": "fwd(s) & bwd(t)", "group_ctas": o.group_ctas,
+                   "K": o.kernel_cycles, "gr_freq": o.gr_freq, "gr_alpha": o.gr_work_alpha,
                    "l2": "inputs larger than L2 (graph %.2f GB, residual slot %.2f GB)" % (
                        arcs * 20 / 1e9, arcs * 8 / 1e9),
                    "parallelism": "query shards, graph replica per GPU"},
@@ -384,6 +391,9 @@ def main():
     ap.add_argument("--nuni", type=int, default=NUNI)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--dump", default=None, help="write per-query stats (jsonl)")
+    ap.add_argument("--K", type=int, default=0, help="discharge cycles (0 = library default)")
+    ap.add_argument("--gr-freq", type=int, default=0, help="max rounds between global relabels")
+    ap.add_argument("--gr-alpha", type=float, default=None, help="relabel after alpha x kept arcs of work")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

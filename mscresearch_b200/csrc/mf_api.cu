@@ -205,6 +205,7 @@ struct mf_graph {
     int avg_deg = 0;
     int nhub = 0;  // vertices with more than HUB_T arcs
     int pivot = 0;  // internal id of the highest-degree vertex (kept-set cache pivot)
+    int *hubs = nullptr;  // device: internal ids of the hubs
     // kept-set cache (see DGraph)
     unsigned char *kc_in = nullptr;
     int *kc_img = nullptr;
@@ -273,6 +274,8 @@ void free_graph_arrays(mf_graph *g) {
     cudaFree(g->region_of);
     cudaFree(g->region_start);
     cudaFree(g->d_graph);
+    cudaFree(g->hubs);
+    g->hubs = nullptr;
     g->row = g->col = g->rev = g->region_of = g->region_start = nullptr;
     g->cap = nullptr;
     g->fwd = nullptr;
@@ -289,6 +292,8 @@ DGraph make_dgraph(const mf_graph *g) {
     dg.rev = g->rev;
     dg.cap = g->cap;
     dg.region_of = g->region_of;
+    dg.hubs = g->hubs;
+    dg.nhub = g->hubs ? g->nhub : 0;
     if (g->kc_valid) {
         dg.kc_in = g->kc_in;
         dg.kc_img = g->kc_img;
@@ -363,10 +368,17 @@ int partition_into(mf_graph *g, int R, int *row, int *col, i64 *cap, int *rev, u
     g->R = R;
     int best = 0;
     {
-        std::vector<int> rw(n + 1);
+        std::vector<int> rw(n + 1), hl;
         CK(cudaMemcpy(rw.data(), g->row, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
         for (int x = 1; x < n; ++x)
             if (rw[x + 1] - rw[x] > rw[best + 1] - rw[best]) best = x;
+        for (int x = 0; x < n; ++x)
+            if (rw[x + 1] - rw[x] > HUB_T) hl.push_back(x);
+        g->nhub = (int)hl.size();
+        if (!hl.empty()) {
+            CK(cudaMalloc(&g->hubs, sizeof(int) * hl.size()));
+            CK(cudaMemcpy(g->hubs, hl.data(), sizeof(int) * hl.size(), cudaMemcpyHostToDevice));
+        }
     }
     g->pivot = best;
     CK(cudaMalloc(&g->d_graph, sizeof(DGraph)));
@@ -705,12 +717,6 @@ int mf_graph_create_from_edges(int n, long long m, const int32_t *u, const int32
     if (rc != MF_OK) {
         mf_graph_destroy(g);
         return rc;
-    }
-    {
-        int nh = 0;
-        for (int x = 0; x < n; ++x)
-            if (row[x + 1] - row[x] > HUB_T) ++nh;
-        g->nhub = nh;
     }
     g->pool.n = n;
     g->pool.arcs = g->arcs;

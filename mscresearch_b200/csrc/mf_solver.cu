@@ -210,77 +210,156 @@ __device__ __forceinline__ int warp_incl_scan_int(int x) {
 
 // ---------------------------------------------------------------------------
 // Level-synchronous frontier BFS over a growing two-ended queue Q: the
-// frontier at a level is Q[flo,fhi) plus back entries [blo,bhi).  Functor
-// cl(v, e, w, level) returns true when arc e = v->w claims w (it performs
-// the claim itself).
+// frontier at a level is Q[flo,fhi) plus back entries [blo,bhi).
 __shared__ int s_lbs_v[MAX_WARPS][32];
 __shared__ int s_lbs_b[MAX_WARPS][32];
 __shared__ int s_lbs_x[MAX_WARPS][32];
 
+// One top-down level.  Functor cl(v, e, w, level) returns true when arc
+// e = v->w claims w (it performs the claim itself).
 template <class Claim>
-__device__ bool bfs_levels(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl) {
-    int flo = 0, blo = 0, level = 0;
+__device__ void td_level(QCtx &c, int *Q, int bank, int flo, int fhi, int blo, int bhi, int level,
+                         Claim cl) {
     int *sv = s_lbs_v[c.warp], *sb = s_lbs_b[c.warp], *sx = s_lbs_x[c.warp];
+    // front: 32 vertices per warp, arcs balanced over the lanes
+    for (int base = flo + c.gw * 32; base < fhi; base += c.gW * 32) {
+        int i = base + c.lane;
+        int v = 0, b = 0, d = 0;
+        if (i < fhi) {
+            v = ldcg(&Q[i]);
+            if (MF_OK_IDX(v, c.n, 11)) {
+                b = ldro(&c.row[v]);
+                d = ldro(&c.row[v + 1]) - b;
+            }
+        }
+        int incl = warp_incl_scan_int(d);
+        int total = __shfl_sync(MF_FULL, incl, 31);
+        sv[c.lane] = v;
+        sb[c.lane] = b;
+        sx[c.lane] = incl - d;
+        __syncwarp();
+        for (int k = 0; k < total; k += 32) {
+            int j = k + c.lane;
+            bool ok = false;
+            int w = 0;
+            if (j < total) {
+                int o = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1)
+                    if (sx[o + step] <= j) o += step;
+                int e = sb[o] + (j - sx[o]);
+                w = ldro(&c.col[e]);
+                ok = cl(sv[o], e, w, level);
+            }
+            append2(c, ok, w, Q, bank);
+        }
+        __syncwarp();
+        if (c.lane == 0) {
+            c.w_arcs += total;
+            c.w_verts += min(32, fhi - base);
+        }
+    }
+    // back: hub arcs in 32-arc chunks over all warps of the group
+    for (int k = blo; k < bhi; ++k) {
+        int v = back_at(c, Q, k);
+        int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+        int nch = (e1 - b + 31) >> 5;
+        for (int ch = c.gw; ch < nch; ch += c.gW) {
+            int e = b + ch * 32 + c.lane;
+            bool ok = false;
+            int w = 0;
+            if (e < e1) {
+                w = ldro(&c.col[e]);
+                ok = cl(v, e, w, level);
+            }
+            append2(c, ok, w, Q, bank);
+            if (c.lane == 0) c.w_arcs += min(32, e1 - (b + ch * 32));
+        }
+        if (c.lane == 0 && c.gw == 0) c.w_verts += 1;
+    }
+}
+
+// One bottom-up level over a universe of candidates: uf(i), i < nuf, gives a
+// vertex of at most HUB_T arcs and ub(k), k < nub, a hub, or -1 when the
+// candidate is already visited.  par(w, e, x, level) tests whether arc
+// e = w->x links w to the search; set(w, level) claims w and returns true
+// (one lane calls it per candidate, so it may store without atomics).  Small
+// candidates are scanned by 8-lane tiles (four per warp step), hubs by whole
+// warps (one hub per warp); both stop at the first parent.
+template <class UF, class UB, class Par, class Set>
+__device__ void bu_level(QCtx &c, int *Q, int bank, int level, int nuf, UF uf, int nub, UB ub, Par par,
+                         Set set) {
+    const int tile = c.lane >> 3, tb = tile << 3, tl = c.lane & 7;
+    const unsigned tmask = 0xffu << tb;
+    i64 arcs = 0;
+    for (int base = c.gw * 32; base < nuf; base += c.gW * 32) {
+        int i = base + c.lane;
+        int w = i < nuf ? uf(i) : -1;
+        unsigned todo = __ballot_sync(MF_FULL, w >= 0);
+        if (c.lane == 0) c.w_verts += min(32, nuf - base);
+        while (todo) {
+            unsigned rest = todo;
+            for (int k = 0; k < tile && rest; ++k) rest &= rest - 1;
+            int src = rest ? __ffs(rest) - 1 : -1;
+            int wt = __shfl_sync(MF_FULL, w, src < 0 ? 0 : src);
+            for (int k = 0; k < 4 && todo; ++k) todo &= todo - 1;
+            bool claimed = false;
+            if (src >= 0) {
+                int b = ldro(&c.row[wt]), e1 = ldro(&c.row[wt + 1]);
+                bool found = false;
+                for (int eb = b; eb < e1 && !found; eb += 8) {
+                    int e = eb + tl;
+                    bool hit = e < e1 && par(wt, e, ldro(&c.col[e]), level);
+                    found = __any_sync(tmask, hit);
+                    if (tl == 0) arcs += min(8, e1 - eb);
+                }
+                if (found && tl == 0) claimed = set(wt, level);
+            }
+            __syncwarp();
+            append2(c, claimed, wt, Q, bank);
+        }
+    }
+    for (int k = c.gw; k < nub; k += c.gW) {
+        int w = 0;
+        if (c.lane == 0) w = ub(k);
+        w = __shfl_sync(MF_FULL, w, 0);
+        bool claimed = false;
+        if (w >= 0) {
+            int b = ldro(&c.row[w]), e1 = ldro(&c.row[w + 1]);
+            unsigned hm = 0;
+            for (int eb = b; eb < e1 && !hm; eb += 32) {
+                int e = eb + c.lane;
+                hm = __ballot_sync(MF_FULL, e < e1 && par(w, e, ldro(&c.col[e]), level));
+                if (c.lane == 0) arcs += min(32, e1 - eb);
+            }
+            if (hm && c.lane == 0) claimed = set(w, level);
+        }
+        append2(c, claimed, w, Q, bank);
+    }
+    arcs = warp_sum_i64(arcs);
+    if (c.lane == 0) c.w_arcs += arcs;
+}
+
+// Direction-optimizing BFS: a level runs top-down while the frontier holds
+// at most a 1/14 share of the unvisited universe (nu - visited), bottom-up
+// otherwise.  Both directions append the newly visited vertices to Q, so
+// the next level can run either way.  nuf = nub = 0: top-down only.
+template <class Claim, class UF, class UB, class Par, class Set>
+__device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, int nuf, UF uf, int nub,
+                        UB ub, Par par, Set set) {
+    int flo = 0, blo = 0, level = 0;
+    const long long nu = (long long)nuf + nub;
+    long long visited = (long long)fhi + bhi;
     while (flo < fhi || blo < bhi) {
         MF_TRACE(10, level);
-        // front: 32 vertices per warp, arcs balanced over the lanes
-        for (int base = flo + c.gw * 32; base < fhi; base += c.gW * 32) {
-            int i = base + c.lane;
-            int v = 0, b = 0, d = 0;
-            if (i < fhi) {
-                v = ldcg(&Q[i]);
-                if (MF_OK_IDX(v, c.n, 11)) {
-                    b = ldro(&c.row[v]);
-                    d = ldro(&c.row[v + 1]) - b;
-                }
-            }
-            int incl = warp_incl_scan_int(d);
-            int total = __shfl_sync(MF_FULL, incl, 31);
-            sv[c.lane] = v;
-            sb[c.lane] = b;
-            sx[c.lane] = incl - d;
-            __syncwarp();
-            for (int k = 0; k < total; k += 32) {
-                int j = k + c.lane;
-                bool ok = false;
-                int w = 0;
-                if (j < total) {
-                    int o = 0;
-#pragma unroll
-                    for (int step = 16; step > 0; step >>= 1)
-                        if (sx[o + step] <= j) o += step;
-                    int e = sb[o] + (j - sx[o]);
-                    w = ldro(&c.col[e]);
-                    ok = cl(sv[o], e, w, level);
-                }
-                append2(c, ok, w, Q, bank);
-            }
-            __syncwarp();
-            if (c.lane == 0) {
-                c.w_arcs += total;
-                c.w_verts += min(32, fhi - base);
-            }
-        }
-        // back: hub arcs in 32-arc chunks over all warps of the group
-        for (int k = blo; k < bhi; ++k) {
-            int v = back_at(c, Q, k);
-            int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
-            int nch = (e1 - b + 31) >> 5;
-            for (int ch = c.gw; ch < nch; ch += c.gW) {
-                int e = b + ch * 32 + c.lane;
-                bool ok = false;
-                int w = 0;
-                if (e < e1) {
-                    w = ldro(&c.col[e]);
-                    ok = cl(v, e, w, level);
-                }
-                append2(c, ok, w, Q, bank);
-                if (c.lane == 0) c.w_arcs += min(32, e1 - (b + ch * 32));
-            }
-            if (c.lane == 0 && c.gw == 0) c.w_verts += 1;
-        }
+        long long fsize = (long long)(fhi - flo) + (bhi - blo);
+        if (nu > visited && fsize * 14 > nu - visited)
+            bu_level(c, Q, bank, level, nuf, uf, nub, ub, par, set);
+        else
+            td_level(c, Q, bank, flo, fhi, blo, bhi, level, cl);
         int ft = 0, bt = 0;
         if (!c.sync_tails(bank, ft, bt)) return false;
+        visited += (long long)(ft - fhi) + (bt - bhi);
         flo = fhi;
         fhi = ft;
         blo = bhi;
@@ -288,6 +367,21 @@ __device__ bool bfs_levels(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl
         ++level;
     }
     return true;
+}
+
+struct NoCand {
+    __device__ int operator()(int) const { return -1; }
+};
+struct NoPar {
+    __device__ bool operator()(int, int, int, int) const { return false; }
+};
+struct NoSet {
+    __device__ bool operator()(int, int) const { return false; }
+};
+
+template <class Claim>
+__device__ bool bfs_levels(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl) {
+    return bfs_dir(c, Q, bank, fhi, bhi, cl, 0, NoCand{}, 0, NoCand{}, NoPar{}, NoSet{});
 }
 
 // ---------------------------------------------------------------------------
@@ -312,7 +406,25 @@ __device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, i
         if (ldcg(&mark[w]) >= S) return false;
         return atomicMax(&mark[w], S) < S;
     };
-    if (!bfs_levels(c, c.st.qa, bank, f0, b0, fwd)) return false;
+    // bottom-up: every vertex, hubs from the graph's hub list
+    const int *hubs = c.gr->hubs;
+    const int nuf = hubs ? c.n : 0, nub = hubs ? c.gr->nhub : 0;
+    const int *rev = c.rev;
+    auto fwd_uf = [&](int i) -> int {
+        return (c.deg(i) <= HUB_T && ldcg(&mark[i]) < S) ? i : -1;
+    };
+    auto fwd_ub = [&](int k) -> int {
+        int w = ldro(&hubs[k]);
+        return ldcg(&mark[w]) < S ? w : -1;
+    };
+    auto fwd_par = [&](int w, int e, int x, int) -> bool {
+        return ldcg(&mark[x]) >= S && ldro(&cap[ldro(&rev[e])]) > 0;
+    };
+    auto fwd_set = [&](int w, int) -> bool {
+        mark[w] = S;
+        return true;
+    };
+    if (!bfs_dir(c, c.st.qa, bank, f0, b0, fwd, nuf, fwd_uf, nub, fwd_ub, fwd_par, fwd_set)) return false;
     int nff = ldcg(&c.st.cnt[bank]), nfb = ldcg(&c.st.cnt[CNT_BACK + bank]);
     t_reach = ldcg(&mark[t]) >= S;
 
@@ -330,13 +442,29 @@ __device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, i
             append1(c, t, c.st.vlist, vb);
         }
         if (!c.sync_tails(vb, f0, b0)) return false;
-        const int *rev = c.rev;
         auto bwd = [&](int v, int e, int w, int) -> bool {
             if (ldcg(&mark[w]) != S) return false;
             if (ldro(&cap[ldro(&rev[e])]) <= 0) return false;
             return atomicCAS(&mark[w], S, M) == S;
         };
-        if (!bfs_levels(c, c.st.vlist, vb, f0, b0, bwd)) return false;
+        // bottom-up universe: the forward-reached list
+        const int *qa = c.st.qa;
+        auto bwd_uf = [&](int i) -> int {
+            int w = ldcg(&qa[i]);
+            return ldcg(&mark[w]) == S ? w : -1;
+        };
+        auto bwd_ub = [&](int k) -> int {
+            int w = back_at(c, qa, k);
+            return ldcg(&mark[w]) == S ? w : -1;
+        };
+        auto bwd_par = [&](int w, int e, int x, int) -> bool {
+            return ldcg(&mark[x]) == M && ldro(&cap[e]) > 0;
+        };
+        auto bwd_set = [&](int w, int) -> bool {
+            mark[w] = M;
+            return true;
+        };
+        if (!bfs_dir(c, c.st.vlist, vb, f0, b0, bwd, nff, bwd_uf, nfb, bwd_ub, bwd_par, bwd_set)) return false;
         c.vf = ldcg(&c.st.cnt[vb]);
         nv = c.vf + ldcg(&c.st.cnt[CNT_BACK + vb]);
         return true;
@@ -355,7 +483,17 @@ __device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, i
         if (ldcg(&qm[w]) >= M) return false;
         return atomicMax(&qm[w], M) < M;
     };
-    if (!bfs_levels(c, c.st.qb, ub, f0, b0, und)) return false;
+    auto und_uf = [&](int i) -> int { return (c.deg(i) <= HUB_T && ldcg(&qm[i]) < M) ? i : -1; };
+    auto und_ub = [&](int k) -> int {
+        int w = ldro(&hubs[k]);
+        return ldcg(&qm[w]) < M ? w : -1;
+    };
+    auto und_par = [&](int w, int e, int x, int) -> bool { return ldcg(&qm[x]) >= M; };
+    auto und_set = [&](int w, int) -> bool {
+        qm[w] = M;
+        return true;
+    };
+    if (!bfs_dir(c, c.st.qb, ub, f0, b0, und, nuf, und_uf, nub, und_ub, und_par, und_set)) return false;
     // intersect: sweep the forward list (both parts); s is in it
     int nf = nff + nfb;
     for (int base = c.gw * 32; base < nf; base += c.gW * 32) {
@@ -425,6 +563,50 @@ __device__ bool preflow(QCtx &c, int s) {
 }
 
 // ---------------------------------------------------------------------------
+// BFS of the global relabel (direction-optimizing, exact levels).  Top-down:
+// frontier vertex v claims an unvisited kept vertex w with residual w->v
+// (stamp CAS, then height).  Bottom-up: an unvisited kept vertex w takes
+// level + 1 when one of its residual arcs reaches a vertex of the current
+// level; it writes the height first and publishes the stamp with a release
+// store, and the parent test reads the stamp with an acquire load before the
+// height, so a vertex claimed in this level (height level + 1) is never
+// taken for a parent.
+__device__ bool relabel_bfs(QCtx &c, int nv, unsigned M, unsigned cur, int blockv, int bank, int fhi,
+                            int bhi) {
+    unsigned *mark = c.st.mark;
+    const int *rev = c.rev;
+    i64 *res = c.st.res;
+    int *h = c.st.h;
+    const int *vl = c.st.vlist;
+    auto relab = [&](int v, int e, int w, int level) -> bool {
+        if (w == blockv) return false;
+        unsigned mw = ldcg(&mark[w]);
+        if (mw < M || mw >= cur) return false;
+        if (ldcg(&res[ldro(&rev[e])]) <= 0) return false;
+        if (atomicCAS(&mark[w], mw, cur) != mw) return false;
+        h[w] = level + 1;
+        return true;
+    };
+    auto uf = [&](int i) -> int {
+        int w = ldcg(&vl[i]);
+        return (w != blockv && ldcg(&mark[w]) != cur) ? w : -1;
+    };
+    auto ub = [&](int k) -> int {
+        int w = back_at(c, vl, k);
+        return (w != blockv && ldcg(&mark[w]) != cur) ? w : -1;
+    };
+    auto par = [&](int w, int e, int x, int level) -> bool {
+        return ldcg(&res[e]) > 0 && ld_acquire_u32(&mark[x]) == cur && ldcg(&h[x]) == level;
+    };
+    auto set = [&](int w, int level) -> bool {
+        h[w] = level + 1;
+        st_release_u32(&mark[w], cur);
+        return true;
+    };
+    return bfs_dir(c, c.st.qa, bank, fhi, bhi, relab, c.vf, uf, nv - c.vf, ub, par, set);
+}
+
+// ---------------------------------------------------------------------------
 // Exact global relabel.  Seeds at height 0: the phase sink (if any) and, in
 // phases A and B, every deficit vertex (RA:224-231 seeds the sink and
 // negative-excess vertices).  Backward BFS over residual arcs through kept
@@ -458,19 +640,8 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
     }
     int f0 = 0, b0 = 0;
     if (!c.sync_tails(qbk, f0, b0)) return false;
-    const int *rev = c.rev;
-    i64 *res = c.st.res;
+    if (!relabel_bfs(c, nv, M, cur, blockv, qbk, f0, b0)) return false;
     int *h = c.st.h;
-    auto relab = [&](int v, int e, int w, int level) -> bool {
-        if (w == blockv) return false;
-        unsigned mw = ldcg(&mark[w]);
-        if (mw < M || mw >= cur) return false;
-        if (ldcg(&res[ldro(&rev[e])]) <= 0) return false;
-        if (atomicCAS(&mark[w], mw, cur) != mw) return false;
-        h[w] = level + 1;
-        return true;
-    };
-    if (!bfs_levels(c, c.st.qa, qbk, f0, b0, relab)) return false;
 
     // sweep: heights of unreached vertices, active list, counts
     MF_TRACE(41, 0);
@@ -628,13 +799,12 @@ __device__ __forceinline__ void discharge_vertex(QCtx &c, int v, int K, int sink
 // round.  hot != NULL restricts the pass to vertices of hot regions.
 __device__ void discharge_front(QCtx &c, const int *L, int nf, int K, int sinkv, int blockv,
                                 int *N, int nbk, unsigned rstamp, i64 *ab, const int *hot) {
-    const int n = c.n;
     for (int base = c.gw * 32; base < nf; base += c.gW * 32) {
         int i = base + c.lane;
         int v = -1, d = 0;
         if (i < nf) {
             v = ldcg(&L[i]);
-            if (!MF_OK_IDX(v, n, 12)) v = -1;
+            if (!MF_OK_IDX(v, c.n, 12)) v = -1;
             else if (hot && !ldcg(&hot[ldro(&c.rof[v])])) v = -1;
         }
         if (v >= 0) d = c.deg(v);
@@ -695,6 +865,7 @@ __device__ bool hub_setup(QCtx &c, const int *L, int nb, const int *hot) {
 __device__ void discharge_hubs(QCtx &c, const int *L, int nb, int sinkv, int blockv, int *N, int nbk,
                                unsigned rstamp, i64 *ab) {
     const int n = c.n;
+    i64 arcs = 0;  // this warp's arc examinations, added to the round's work once
     for (int k = 0; k < nb; ++k) {
         HubWork *hw = &c.st.hubw[k];
         int nch = ldcg(&hw->nch);
@@ -735,7 +906,7 @@ __device__ void discharge_hubs(QCtx &c, const int *L, int nb, int sinkv, int blo
             if (c.lane == 0) {
                 if (take) atomic_add_i64(&c.st.ex[v], -take);
                 if (mh != MF_INF_H) atomicMin(&hw->minh, mh);
-                c.w_arcs += min(32, e1 - (b + ch * 32));
+                arcs += min(32, e1 - (b + ch * 32));
                 c.w_push += take ? 1 : 0;
                 __threadfence();
                 if (atomicAdd(&hw->done, 1) == nch - 1) {
@@ -754,6 +925,10 @@ __device__ void discharge_hubs(QCtx &c, const int *L, int nb, int sinkv, int blo
                 }
             }
         }
+    }
+    if (c.lane == 0 && arcs) {
+        c.w_arcs += arcs;
+        atomic_add_i64(&ab[A_WORK], arcs);
     }
 }
 

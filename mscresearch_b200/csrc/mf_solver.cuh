@@ -12,6 +12,10 @@ struct DGraph {
     const int *rev;        // arcs
     const i64 *cap;        // arcs (current capacities)
     const int *region_of;  // n
+    // Vertices with more than HUB_T arcs (NULL: not available; the prune
+    // then runs its searches top-down only).
+    const int *hubs;
+    int nhub;
     // Kept-set cache: the strongly connected component of a pivot vertex.
     // For s and t both in it, fwd(s) & bwd(t) is exactly that component, so
     // a query can take its kept list (vlist layout: front kc_f entries, back
