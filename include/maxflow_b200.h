@@ -48,7 +48,7 @@ typedef struct mf_opts {
     int kernel_cycles;     /* K: discharge cycles per active vertex per round (RA:1467 uses max(4, avg
                               degree) with one push per cycle; each cycle here pushes to every
                               downhill arc); 0 = 4 */
-    int gr_freq;           /* rounds between global relabels at most (GR_FREQ0, RA:1466) */
+    int gr_freq;           /* rounds between global relabels at most (default 16; RA:1466 uses 128) */
     double gr_work_alpha;  /* also relabel once scanned arcs exceed alpha x mask arcs (0 = off) */
     int prune_mode;        /* 0: RA:1391-1445 mask (fwd(s) & undirected comp(t)); 1: fwd(s) & bwd(t) (default) */
     int path_push_switch;  /* active count at or below which path-push starts (RA:1480) */
@@ -63,7 +63,7 @@ typedef struct mf_opts {
     int force_rm;          /* tests: run RM every rm_freq rounds regardless of frac_high */
     int force_path_push;   /* tests: use path push whenever active <= path_push_switch */
     long long iter_max;    /* round cap per solve (RA:1476) */
-    int group_ctas;        /* CTAs per query group in batched solves (0 = autotuned default) */
+    int group_ctas;        /* CTAs per query group in batched solves (0 = 4) */
     int threads;           /* threads per CTA (0 = 512) */
     int certify;           /* 1 = return excess to the source and check the certificate */
     int verbose;           /* 1 = per-query log lines on stderr */

@@ -639,8 +639,8 @@ extern "C" {
 void mf_opts_default(mf_opts *o) {
     memset(o, 0, sizeof(*o));
     o->kernel_cycles = 0;
-    o->gr_freq = 128;        // GR_FREQ0 (RA:1466)
-    o->gr_work_alpha = 2.0;  // also relabel after ~2 passes over the kept arcs
+    o->gr_freq = 16;         // RA:1466 starts at 128; exact relabels are cheap here
+    o->gr_work_alpha = 0.5;  // also relabel after ~half a pass over the kept arcs
     o->prune_mode = 1;
     o->path_push_switch = 8;  // PATH_PUSH_SWITCH (RA:1480)
     o->max_path_len = 256;    // MAX_PATH_LENGTH (RA:1481)
@@ -870,7 +870,7 @@ static int solve_common(mf_graph *g, int nq, const int32_t *s, const int32_t *t,
     int rc0 = ensure_kept_cache(g, o);
     if (rc0) return rc0;
     std::vector<QOut> outs(nq);
-    int G = single ? 0 : (o.group_ctas > 0 ? o.group_ctas : 2);
+    int G = single ? 0 : (o.group_ctas > 0 ? o.group_ctas : 4);
     int rc = launch(g, g->pool, nq, si.data(), ti.data(), false, o, mode, dbg, nullptr, 0, G, outs.data());
     if (rc) return rc;
     int worst = MF_OK;
@@ -1087,7 +1087,7 @@ static int session_run(mf_session *ss, int mode, const ArcUpdate *d_upd, int nup
                        mf_stats *stats) {
     mf_graph *g = ss->g;
     std::vector<QOut> outs(ss->nq);
-    int G = ss->opts.group_ctas > 0 ? ss->opts.group_ctas : 2;
+    int G = ss->opts.group_ctas > 0 ? ss->opts.group_ctas : 4;
     int rc = launch(g, ss->pool, ss->nq, ss->s.data(), ss->t.data(), true, ss->opts, mode, nullptr,
                     d_upd, nupd, G, outs.data());
     if (rc) return rc;
@@ -1261,7 +1261,7 @@ int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int ma
         delete sv;
         return rc;
     }
-    sv->G = sv->opts.group_ctas > 0 ? sv->opts.group_ctas : 2;
+    sv->G = sv->opts.group_ctas > 0 ? sv->opts.group_ctas : 4;
     int groups = std::max(1, di.sms * di.bps / sv->G);
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);

@@ -62,20 +62,20 @@ extern "C" int mf_autotune(mf_graph *g, int nq, const int32_t *s, const int32_t 
         c.group_ctas = G;
         if ((rc = consider(c))) return rc;
     }
-    const int ks[] = {4, 8, 16, 32};
+    const int ks[] = {2, 4, 8, 16};
     for (int K : ks) {
         mf_opts c = cur;
         c.kernel_cycles = K;
         if ((rc = consider(c))) return rc;
     }
-    const double alphas[] = {0.5, 1.0, 2.0, 4.0};
+    const double alphas[] = {0.25, 0.5, 1.0, 2.0};
     for (double a : alphas) {
         if (a == cur.gr_work_alpha) continue;
         mf_opts c = cur;
         c.gr_work_alpha = a;
         if ((rc = consider(c))) return rc;
     }
-    const int freqs[] = {32, 128, 512};
+    const int freqs[] = {8, 16, 32, 128};
     for (int fq : freqs) {
         if (fq == cur.gr_freq) continue;
         mf_opts c = cur;
