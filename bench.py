@@ -179,6 +179,8 @@ def run_engine(args):
     o = mf.opts(group_ctas=args.group)
     if args.K:
         o.kernel_cycles = args.K
+    if args.threads:
+        o.threads = args.threads
     if args.gr_freq:
         o.gr_freq = args.gr_freq
     if args.gr_alpha is not None:
@@ -242,7 +244,7 @@ def run_engine(args):
         "data": "synthetic (seeded R-MAT 2^20, 2^24 draws, caps U[1,1000]; 128 hub + 128 uniform queries)",
         "config": {"workload": "rmat%d_%dq" % (args.scale, nq), "n": n, "edges": len(u), "arcs": arcs, "queries_per_gpu": nq,
                    "R": R, "prune": "fwd(s) & bwd(t)", "group_ctas": o.group_ctas,
-                   "K": o.kernel_cycles, "gr_freq": o.gr_freq, "gr_alpha": o.gr_work_alpha,
+                   "K": o.kernel_cycles, "threads": o.threads or 512, "gr_freq": o.gr_freq, "gr_alpha": o.gr_work_alpha,
                    "l2": "inputs larger than L2 (graph %.2f GB, residual slot %.2f GB)" % (
                        arcs * 20 / 1e9, arcs * 8 / 1e9),
                    "parallelism": "query shards, graph replica per GPU"},
@@ -392,6 +394,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--dump", default=None, help="write per-query stats (jsonl)")
     ap.add_argument("--K", type=int, default=0, help="discharge cycles (0 = library default)")
+    ap.add_argument("--threads", type=int, default=0, help="threads per CTA (0 = library default)")
     ap.add_argument("--gr-freq", type=int, default=0, help="max rounds between global relabels")
     ap.add_argument("--gr-alpha", type=float, default=None, help="relabel after alpha x kept arcs of work")
     args = ap.parse_args()

@@ -64,7 +64,7 @@ typedef struct mf_opts {
     int force_path_push;   /* tests: use path push whenever active <= path_push_switch */
     long long iter_max;    /* round cap per solve (RA:1476) */
     int group_ctas;        /* CTAs per query group in batched solves (0 = 4) */
-    int threads;           /* threads per CTA (0 = 512) */
+    int threads;           /* threads per CTA: a multiple of 32 in [64, 512] (0 = 512) */
     int certify;           /* 1 = return excess to the source and check the certificate */
     int verbose;           /* 1 = per-query log lines on stderr */
     int use_kept_cache;    /* 1 = queries with s and t in the graph's cached strongly connected

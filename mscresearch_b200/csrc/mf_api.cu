@@ -57,6 +57,8 @@ struct DevInfo {
 };
 
 int dev_info(DevInfo &d, int threads) {
+    if (threads < 64 || threads > 512 || threads % 32)
+        return fail(MF_ERR_ARG, "threads per CTA must be a multiple of 32 in [64, 512] (got %d)", threads);
     int dev = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
@@ -464,8 +466,9 @@ int status_from_err(int e) {
 int launch(mf_graph *g, SlotPool &pool, int nq, const int *s_int, const int *t_int,
            bool per_query_slot, const mf_opts &o, int mode, void *dbg, const ArcUpdate *d_upd,
            int nupd, int G_req, QOut *outs) {
-    if (!g->dev.ok) {
-        int rc = dev_info(g->dev, o.threads > 0 ? o.threads : 512);
+    const int want_threads = o.threads > 0 ? o.threads : 512;
+    if (!g->dev.ok || g->dev.threads != want_threads) {
+        int rc = dev_info(g->dev, want_threads);
         if (rc) return rc;
     }
     const int threads = g->dev.threads;

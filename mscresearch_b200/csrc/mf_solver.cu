@@ -1864,6 +1864,8 @@ void mf_launch_kernel(const KParams &p, int grid, int threads, cudaStream_t st, 
 }
 
 int mf_kernel_max_blocks_per_sm(int threads) {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, mf_kernel) != cudaSuccess || threads > fa.maxThreadsPerBlock) return 0;
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mf_kernel, threads, 0) != cudaSuccess)
         return 0;
