@@ -181,6 +181,9 @@ def run_engine(args):
         o.kernel_cycles = args.K
     if args.threads:
         o.threads = args.threads
+    for kv in args.opt:
+        k, v = kv.split("=", 1)
+        setattr(o, k, type(getattr(o, k))(float(v)) if isinstance(getattr(o, k), float) else int(v))
     if args.gr_freq:
         o.gr_freq = args.gr_freq
     if args.gr_alpha is not None:
@@ -245,6 +248,7 @@ def run_engine(args):
         "config": {"workload": "rmat%d_%dq" % (args.scale, nq), "n": n, "edges": len(u), "arcs": arcs, "queries_per_gpu": nq,
                    "R": R, "prune": "fwd(s) & bwd(t)", "group_ctas": o.group_ctas,
                    "K": o.kernel_cycles, "threads": o.threads or 512, "gr_freq": o.gr_freq, "gr_alpha": o.gr_work_alpha,
+                   "opt": list(args.opt),
                    "l2": "inputs larger than L2 (graph %.2f GB, residual slot %.2f GB)" % (
                        arcs * 20 / 1e9, arcs * 8 / 1e9),
                    "parallelism": "query shards, graph replica per GPU"},
@@ -395,6 +399,8 @@ def main():
     ap.add_argument("--dump", default=None, help="write per-query stats (jsonl)")
     ap.add_argument("--K", type=int, default=0, help="discharge cycles (0 = library default)")
     ap.add_argument("--threads", type=int, default=0, help="threads per CTA (0 = library default)")
+    ap.add_argument("--opt", action="append", default=[], metavar="FIELD=VALUE",
+                    help="set any mf_opts field (repeatable), e.g. --opt use_hot_sweep=0")
     ap.add_argument("--gr-freq", type=int, default=0, help="max rounds between global relabels")
     ap.add_argument("--gr-alpha", type=float, default=None, help="relabel after alpha x kept arcs of work")
     args = ap.parse_args()

@@ -69,6 +69,9 @@ typedef struct mf_opts {
     int verbose;           /* 1 = per-query log lines on stderr */
     int use_kept_cache;    /* 1 = queries with s and t in the graph's cached strongly connected
                               component take it as their kept set (prune_mode 1 only) */
+    int schedule;          /* batched solves: 1 = start the queries expected to cost most first
+                              (s and t in the cached component, then larger min(deg s, deg t));
+                              0 = input order.  Results are in input order either way. */
 } mf_opts;
 
 /* Per-query statistics (all counts exact device counters). */

@@ -41,6 +41,7 @@ class MfOpts(C.Structure):
         ("certify", C.c_int),
         ("verbose", C.c_int),
         ("use_kept_cache", C.c_int),
+        ("schedule", C.c_int),
     ]
 
 

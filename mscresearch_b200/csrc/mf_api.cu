@@ -208,6 +208,8 @@ struct mf_graph {
     int nhub = 0;  // vertices with more than HUB_T arcs
     int pivot = 0;  // internal id of the highest-degree vertex (kept-set cache pivot)
     int *hubs = nullptr;  // device: internal ids of the hubs
+    std::vector<int> deg_host;                // internal id -> arcs
+    std::vector<unsigned char> kc_in_host;    // internal id -> in the cached component
     // kept-set cache (see DGraph)
     unsigned char *kc_in = nullptr;
     int *kc_img = nullptr;
@@ -264,6 +266,7 @@ void free_kept_cache(mf_graph *g) {
     g->kc_res = nullptr;
     g->kc_valid = false;
     g->kc_tried = false;
+    g->kc_in_host.clear();
 }
 
 void free_graph_arrays(mf_graph *g) {
@@ -374,8 +377,11 @@ int partition_into(mf_graph *g, int R, int *row, int *col, i64 *cap, int *rev, u
         CK(cudaMemcpy(rw.data(), g->row, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
         for (int x = 1; x < n; ++x)
             if (rw[x + 1] - rw[x] > rw[best + 1] - rw[best]) best = x;
-        for (int x = 0; x < n; ++x)
+        g->deg_host.resize(n);
+        for (int x = 0; x < n; ++x) {
+            g->deg_host[x] = rw[x + 1] - rw[x];
             if (rw[x + 1] - rw[x] > HUB_T) hl.push_back(x);
+        }
         g->nhub = (int)hl.size();
         if (!hl.empty()) {
             CK(cudaMalloc(&g->hubs, sizeof(int) * hl.size()));
@@ -660,6 +666,7 @@ void mf_opts_default(mf_opts *o) {
     o->certify = 0;
     o->verbose = 0;
     o->use_kept_cache = 1;
+    o->schedule = 1;
 }
 
 const char *mf_last_error_string(void) { return g_err.c_str(); }
@@ -851,6 +858,10 @@ static int ensure_kept_cache(mf_graph *g, const mf_opts &o) {
     cudaFree(darcs);
     g->kc_arcs = (i64)ka;
     g->kc_valid = out.mask_n >= 2;
+    if (g->kc_valid) {
+        g->kc_in_host.resize(n);
+        CK(cudaMemcpy(g->kc_in_host.data(), g->kc_in, n, cudaMemcpyDeviceToHost));
+    }
     if (!g->kc_valid) {
         bool tried = true;
         free_kept_cache(g);
@@ -858,6 +869,29 @@ static int ensure_kept_cache(mf_graph *g, const mf_opts &o) {
         return MF_OK;
     }
     return upload_dgraph(g);
+}
+
+// Queue order for a batch: queries whose s and t are both in the cached
+// component first (their kept set is the whole component), then the rest;
+// within each class, larger min(deg s, deg t) first (the flow, and with it
+// the push work, is bounded by the smaller end).  Invalid queries last.
+static std::vector<int> cost_order(const mf_graph *g, int nq, const int *si, const int *ti, const mf_opts &o) {
+    std::vector<long long> key(nq);
+    bool kc = g->kc_valid && o.use_kept_cache && o.prune_mode == 1 && !g->kc_in_host.empty();
+    for (int i = 0; i < nq; ++i) {
+        int a = si[i], b = ti[i];
+        if (a < 0 || b < 0 || a == b || g->deg_host.empty()) {
+            key[i] = -1;
+            continue;
+        }
+        long long k = std::min(g->deg_host[a], g->deg_host[b]);
+        if (kc && g->kc_in_host[a] && g->kc_in_host[b]) k += 1LL << 40;
+        key[i] = k;
+    }
+    std::vector<int> perm(nq);
+    for (int i = 0; i < nq; ++i) perm[i] = i;
+    std::stable_sort(perm.begin(), perm.end(), [&](int x, int y) { return key[x] > key[y]; });
+    return perm;
 }
 
 static int solve_common(mf_graph *g, int nq, const int32_t *s, const int32_t *t, const mf_opts *opts,
@@ -874,8 +908,25 @@ static int solve_common(mf_graph *g, int nq, const int32_t *s, const int32_t *t,
     if (rc0) return rc0;
     std::vector<QOut> outs(nq);
     int G = single ? 0 : (o.group_ctas > 0 ? o.group_ctas : 4);
+    // batched: queue order by expected cost (largest first), results unpermuted
+    std::vector<int> perm;
+    if (!single && o.schedule && nq > 1 && mode == KM_SOLVE) {
+        perm = cost_order(g, nq, si.data(), ti.data(), o);
+        std::vector<int> s2(nq), t2(nq);
+        for (int i = 0; i < nq; ++i) {
+            s2[i] = si[perm[i]];
+            t2[i] = ti[perm[i]];
+        }
+        si.swap(s2);
+        ti.swap(t2);
+    }
     int rc = launch(g, g->pool, nq, si.data(), ti.data(), false, o, mode, dbg, nullptr, 0, G, outs.data());
     if (rc) return rc;
+    if (!perm.empty()) {
+        std::vector<QOut> o2(nq);
+        for (int i = 0; i < nq; ++i) o2[perm[i]] = outs[i];
+        outs.swap(o2);
+    }
     int worst = MF_OK;
     u64 t0min = ~0ull;
     for (int i = 0; i < nq; ++i) t0min = std::min(t0min, outs[i].t_begin);

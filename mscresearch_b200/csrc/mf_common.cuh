@@ -68,17 +68,6 @@ __device__ __forceinline__ bool mf_ok_idx(long long i, long long lim, int site) 
 #define MF_OK_IDX(i, lim, site) true
 #endif
 
-// Ordered publication: st_release makes every earlier store of the thread
-// visible before the stamp; ld_acquire orders every later load after it.
-__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
 __device__ __forceinline__ i64 atomic_add_i64(i64 *p, i64 v) {
     return (i64)atomicAdd(reinterpret_cast<u64 *>(p), (u64)v);
 }

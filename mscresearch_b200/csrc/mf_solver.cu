@@ -563,14 +563,14 @@ __device__ bool preflow(QCtx &c, int s) {
 }
 
 // ---------------------------------------------------------------------------
-// BFS of the global relabel (direction-optimizing, exact levels).  Top-down:
-// frontier vertex v claims an unvisited kept vertex w with residual w->v
-// (stamp CAS, then height).  Bottom-up: an unvisited kept vertex w takes
-// level + 1 when one of its residual arcs reaches a vertex of the current
-// level; it writes the height first and publishes the stamp with a release
-// store, and the parent test reads the stamp with an acquire load before the
-// height, so a vertex claimed in this level (height level + 1) is never
-// taken for a parent.
+// BFS of the global relabel (direction-optimizing, exact levels).  Every kept
+// vertex enters with height n, the seeds with 0.  Top-down: frontier vertex
+// v claims an unvisited kept vertex w with residual w->v (stamp CAS, then
+// height).  Bottom-up: an unvisited kept vertex w takes level + 1 when one
+// of its residual arcs reaches a vertex whose height is level.  Only the
+// current frontier has that height: a vertex claimed during this level
+// holds n or level + 1, whichever of its stores a reader sees, so the test
+// needs no ordering between the claim's stores.
 __device__ bool relabel_bfs(QCtx &c, int nv, unsigned M, unsigned cur, int blockv, int bank, int fhi,
                             int bhi) {
     unsigned *mark = c.st.mark;
@@ -596,11 +596,11 @@ __device__ bool relabel_bfs(QCtx &c, int nv, unsigned M, unsigned cur, int block
         return (w != blockv && ldcg(&mark[w]) != cur) ? w : -1;
     };
     auto par = [&](int w, int e, int x, int level) -> bool {
-        return ldcg(&res[e]) > 0 && ld_acquire_u32(&mark[x]) == cur && ldcg(&h[x]) == level;
+        return ldcg(&res[e]) > 0 && ldcg(&h[x]) == level;
     };
     auto set = [&](int w, int level) -> bool {
         h[w] = level + 1;
-        st_release_u32(&mark[w], cur);
+        mark[w] = cur;
         return true;
     };
     return bfs_dir(c, c.st.qa, bank, fhi, bhi, relab, c.vf, uf, nv - c.vf, ub, par, set);
@@ -610,8 +610,8 @@ __device__ bool relabel_bfs(QCtx &c, int nv, unsigned M, unsigned cur, int block
 // Exact global relabel.  Seeds at height 0: the phase sink (if any) and, in
 // phases A and B, every deficit vertex (RA:224-231 seeds the sink and
 // negative-excess vertices).  Backward BFS over residual arcs through kept
-// vertices; the blocked vertex is never labeled.  Afterwards unreached kept
-// vertices get height n, and the active list (excess > 0, height < n, not
+// vertices; the blocked vertex is never labeled.  Unreached kept vertices
+// keep height n, and the active list (excess > 0, height < n, not
 // the phase sink or blocked vertex) is compacted into L (front / back).
 // Returns counts in naf / nab (active front / back) and nd (deficits).
 __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int blockv, int srcv,
@@ -631,10 +631,9 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
             v = c.vat(i);
             if (v == sinkv) seed = true;
             else if (deficit_seeds && v != blockv && v != srcv && ldcg(&c.st.ex[v]) < 0) seed = true;
-            if (seed) {
-                mark[v] = cur;
-                c.st.h[v] = 0;
-            }
+            if (seed) mark[v] = cur;
+            // every kept vertex starts the search at height n (unreached)
+            c.st.h[v] = seed ? 0 : n;
         }
         append2(c, seed, v, c.st.qa, qbk);
     }
@@ -653,13 +652,7 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
         int v = 0;
         if (i < nv) {
             v = c.vat(i);
-            int hv;
-            if (ldcg(&mark[v]) != cur) {
-                h[v] = n;
-                hv = n;
-            } else {
-                hv = ldcg(&h[v]);
-            }
+            int hv = ldcg(&h[v]);  // n when the search did not reach v
             i64 ev = ldcg(&c.st.ex[v]);
             if (ev > 0 && hv < n && v != sinkv && v != blockv) {
                 act = true;
