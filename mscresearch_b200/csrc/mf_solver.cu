@@ -49,6 +49,7 @@
 // more than three banks between two barriers).
 #define NBANKS 8
 #define CNT_BACK 16
+#define CNT_HUBCH 30  // total chunks of the current hub pass
 #define CNT_Q 8      // query handed to the group
 #define CNT_FLAG 9   // misc uniform flag
 #define CNT_RS 10    // serving: request source / sink / graph
@@ -402,8 +403,9 @@ __device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, i
     unsigned *mark = c.st.mark;
     const i64 *cap = c.cap;
     auto fwd = [&](int v, int e, int w, int) -> bool {
-        if (ldro(&cap[e]) <= 0) return false;
-        if (ldcg(&mark[w]) >= S) return false;
+        i64 ce = ldro(&cap[e]);
+        unsigned mw = ldcg(&mark[w]);
+        if (ce <= 0 || mw >= S) return false;
         return atomicMax(&mark[w], S) < S;
     };
     // bottom-up: every vertex, hubs from the graph's hub list
@@ -443,8 +445,9 @@ __device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, i
         }
         if (!c.sync_tails(vb, f0, b0)) return false;
         auto bwd = [&](int v, int e, int w, int) -> bool {
-            if (ldcg(&mark[w]) != S) return false;
-            if (ldro(&cap[ldro(&rev[e])]) <= 0) return false;
+            unsigned mw = ldcg(&mark[w]);
+            i64 cr = ldro(&cap[ldro(&rev[e])]);
+            if (mw != S || cr <= 0) return false;
             return atomicCAS(&mark[w], S, M) == S;
         };
         // bottom-up universe: the forward-reached list
@@ -579,10 +582,10 @@ __device__ bool relabel_bfs(QCtx &c, int nv, unsigned M, unsigned cur, int block
     int *h = c.st.h;
     const int *vl = c.st.vlist;
     auto relab = [&](int v, int e, int w, int level) -> bool {
-        if (w == blockv) return false;
+        // stamp and reverse residual are loaded together (one latency)
         unsigned mw = ldcg(&mark[w]);
-        if (mw < M || mw >= cur) return false;
-        if (ldcg(&res[ldro(&rev[e])]) <= 0) return false;
+        i64 rr = ldcg(&res[ldro(&rev[e])]);
+        if (w == blockv || mw < M || mw >= cur || rr <= 0) return false;
         if (atomicCAS(&mark[w], mw, cur) != mw) return false;
         h[w] = level + 1;
         return true;
@@ -722,17 +725,26 @@ __device__ void discharge_tile(QCtx &c, int v, int K, int sinkv, int blockv, int
         if (ev <= 0 || hv >= n) break;
         i64 rem = ev;
         int minh = MF_INF_H;
+        // residual and head of the lane's arc are loaded one step ahead (a
+        // residual read early is never above the current one: only this
+        // tile lowers residuals out of v)
+        i64 r_nx = 0;
+        int w_nx = 0;
+        if (b + tl < e1) {
+            r_nx = ldcg(&c.st.res[b + tl]);
+            w_nx = ldro(&c.col[b + tl]);
+        }
         for (int base = b; base < e1; base += TW) {
             int e = base + tl;
-            i64 r = 0;
-            int w = 0, hw = MF_INF_H;
-            if (e < e1) {
-                r = ldcg(&c.st.res[e]);
-                if (r > 0) {
-                    w = ldro(&c.col[e]);
-                    hw = ldcg(&c.st.h[w]);
-                }
+            i64 r = r_nx;
+            int w = w_nx, hw = MF_INF_H;
+            if (e + TW < e1) {
+                r_nx = ldcg(&c.st.res[e + TW]);
+                w_nx = ldro(&c.col[e + TW]);
+            } else {
+                r_nx = 0;  // the lane has no arc in the next step
             }
+            if (r > 0) hw = ldcg(&c.st.h[w]);
             bool adm = r > 0 && hw < hv;
             unsigned am = __ballot_sync(mask, adm);
             i64 d = 0;
@@ -831,14 +843,19 @@ __device__ void discharge_front(QCtx &c, const int *L, int nf, int K, int sinkv,
 
 // Hubs of L's back part, one cycle per round, spread over all warps of the
 // group.  Set-up (before a group barrier): per hub, budget = its excess,
-// minh = INF, done = 0, hv = its height.  Each warp then takes 32-arc chunks
-// of each hub: it sums the downhill residual of its chunk, claims that much
+// minh = INF, done = 0, hv = its height; the first CTA then lays the hubs'
+// 32-arc chunks out in one index space (exclusive prefix of the chunk
+// counts) and every warp takes an equal contiguous range of it.  Per chunk a
+// warp sums the downhill residual of its chunk, claims that much
 // from the hub's budget with one atomicAdd (getting the whole amount, the
 // rest, or nothing), spreads the claim over the chunk's downhill arcs in arc
 // order, and folds the lowest height over arcs left with residual into
 // minh.  The warp that finishes a hub's last chunk relabels it when budget
 // is left (then every downhill arc was saturated, so minh >= its height) and
 // re-lists it if it is still active.
+__shared__ int s_hscan[MAX_WARPS];
+__shared__ int s_htot;
+
 __device__ bool hub_setup(QCtx &c, const int *L, int nb, const int *hot) {
     int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
     for (int k = gt; k < nb; k += gT) {
@@ -850,7 +867,33 @@ __device__ bool hub_setup(QCtx &c, const int *L, int nb, const int *hot) {
         hw.hv = ldcg(&c.st.h[v]);
         bool skip = hw.budget <= 0 || hw.hv >= c.n || (hot && !ldcg(&hot[ldro(&c.rof[v])]));
         hw.nch = skip ? 0 : (c.deg(v) + 31) >> 5;
+        hw.cstart = 0;
         if (MF_OK_IDX(k, c.st.nhub, 95)) c.st.hubw[k] = hw;
+    }
+    if (!c.sync()) return false;
+    // exclusive prefix of the chunk counts (first CTA of the group)
+    if (c.crank == 0) {
+        const int nw = blockDim.x >> 5;
+        int carry = 0;
+        for (int base = 0; base < nb; base += blockDim.x) {
+            int k = base + threadIdx.x;
+            bool in = k < nb && k < c.st.nhub;
+            int x = in ? ldcg(&c.st.hubw[k].nch) : 0;
+            int incl = warp_incl_scan_int(x);
+            if (c.lane == 31) s_hscan[c.warp] = incl;  // warp totals
+            __syncthreads();
+            if (c.warp == 0) {
+                int y = c.lane < nw ? s_hscan[c.lane] : 0;
+                int yi = warp_incl_scan_int(y);
+                if (c.lane < nw) s_hscan[c.lane] = yi - y;  // warp offsets
+                if (c.lane == 31) s_htot = yi;              // tile total
+            }
+            __syncthreads();
+            if (in) c.st.hubw[k].cstart = carry + s_hscan[c.warp] + incl - x;
+            carry += s_htot;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) c.st.cnt[CNT_HUBCH] = carry;
     }
     return c.sync();
 }
@@ -859,23 +902,39 @@ __device__ void discharge_hubs(QCtx &c, const int *L, int nb, int sinkv, int blo
                                unsigned rstamp, i64 *ab) {
     const int n = c.n;
     i64 arcs = 0;  // this warp's arc examinations, added to the round's work once
-    for (int k = 0; k < nb; ++k) {
-        HubWork *hw = &c.st.hubw[k];
-        int nch = ldcg(&hw->nch);
-        if (nch == 0) continue;
-        int v = back_at(c, L, k);
-        int hv = ldcg(&hw->hv);
-        int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
-        for (int ch = c.gw; ch < nch; ch += c.gW) {
+    nb = min(nb, c.st.nhub);
+    const int T = ldcg(&c.st.cnt[CNT_HUBCH]);
+    // this warp's contiguous share of the (hub, chunk) index space
+    const int j0 = (int)((long long)T * c.gw / c.gW), j1 = (int)((long long)T * (c.gw + 1) / c.gW);
+    if (j0 < j1 && nb > 0) {
+        // the hub holding chunk j0: the last k with cstart <= j0 (it has chunks)
+        int lo = 0, hi = nb - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (ldcg(&c.st.hubw[mid].cstart) <= j0) lo = mid;
+            else hi = mid - 1;
+        }
+        int k = lo;
+        int cs = ldcg(&c.st.hubw[k].cstart), nch = ldcg(&c.st.hubw[k].nch);
+        for (int j = j0; j < j1; ++j) {
+            while (j >= cs + nch && k + 1 < nb) {
+                ++k;
+                cs = ldcg(&c.st.hubw[k].cstart);
+                nch = ldcg(&c.st.hubw[k].nch);
+            }
+            if (j >= cs + nch) break;
+            HubWork *hw = &c.st.hubw[k];
+            int v = back_at(c, L, k);
+            int hv = ldcg(&hw->hv);
+            int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+            int ch = j - cs;
             int e = b + ch * 32 + c.lane;
             i64 r = 0;
             int w = 0, hwt = MF_INF_H;
             if (e < e1) {
                 r = ldcg(&c.st.res[e]);
-                if (r > 0) {
-                    w = ldro(&c.col[e]);
-                    hwt = ldcg(&c.st.h[w]);
-                }
+                w = ldro(&c.col[e]);
+                if (r > 0) hwt = ldcg(&c.st.h[w]);
             }
             bool adm = r > 0 && hwt < hv;
             i64 x = adm ? r : 0;

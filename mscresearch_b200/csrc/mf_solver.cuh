@@ -39,6 +39,7 @@ struct HubWork {
     int done;    // chunks finished
     int hv;      // hub height at set-up
     int nch;     // chunks (0 = nothing to do)
+    int cstart;  // chunks of the hubs before this one (exclusive prefix of nch)
 };
 
 // Working state of one residual slot.  All arrays are full-size for the
