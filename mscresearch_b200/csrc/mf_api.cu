@@ -212,6 +212,7 @@ struct mf_graph {
     std::vector<unsigned char> kc_in_host;    // internal id -> in the cached component
     // kept-set cache (see DGraph)
     unsigned char *kc_in = nullptr;
+    unsigned char *kc_fb = nullptr;
     int *kc_img = nullptr;
     i64 *kc_res = nullptr;
     int kc_f = 0, kc_b = 0;
@@ -259,6 +260,8 @@ namespace {
 
 void free_kept_cache(mf_graph *g) {
     cudaFree(g->kc_in);
+    cudaFree(g->kc_fb);
+    g->kc_fb = nullptr;
     cudaFree(g->kc_img);
     cudaFree(g->kc_res);
     g->kc_in = nullptr;
@@ -301,6 +304,7 @@ DGraph make_dgraph(const mf_graph *g) {
     dg.nhub = g->hubs ? g->nhub : 0;
     if (g->kc_valid) {
         dg.kc_in = g->kc_in;
+        dg.kc_fb = g->kc_fb;
         dg.kc_img = g->kc_img;
         dg.kc_res = g->kc_res;
         dg.kc_f = g->kc_f;
@@ -822,7 +826,8 @@ __global__ void k_kept_res(int n, const int *row, const int *col, const i64 *cap
 
 // Builds the kept-set cache once per graph state (prune mode 1 only): the
 // strongly connected component of the highest-degree vertex, found by the
-// solver's own prune with s = t = pivot.
+// solver's own prune with s = t = pivot, and the pivot's forward / backward
+// closures (F / B bits per vertex).
 static int ensure_kept_cache(mf_graph *g, const mf_opts &o) {
     if (g->kc_valid || g->kc_tried || o.prune_mode != 1 || !o.use_kept_cache) return MF_OK;
     g->kc_tried = true;
@@ -832,8 +837,10 @@ static int ensure_kept_cache(mf_graph *g, const mf_opts &o) {
     CK(cudaMalloc(&g->kc_img, sizeof(int) * (size_t)n));
     CK(cudaMalloc(&g->kc_res, sizeof(i64) * (size_t)std::max<i64>(g->arcs, 1)));
     CK(cudaMemset(g->kc_in, 0, n));
+    CK(cudaMalloc(&g->kc_fb, n));
     ko.img = g->kc_img;
     ko.in = g->kc_in;
+    ko.fb = g->kc_fb;
     KcOut *dko = nullptr;
     CK(cudaMalloc(&dko, sizeof(KcOut)));
     CK(cudaMemcpy(dko, &ko, sizeof(KcOut), cudaMemcpyHostToDevice));

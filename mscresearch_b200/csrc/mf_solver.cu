@@ -386,92 +386,117 @@ __device__ bool bfs_levels(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl
 }
 
 // ---------------------------------------------------------------------------
-// Prune.  Stamps: S (forward reach), M = S+1 (kept), U (undirected, mode 0).
-// Leaves the kept vertices in vlist (front c.vf entries, back nv - c.vf) and
-// returns nv (0 if t is not reachable from s, in which case the flow is 0).
-__device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, int &nv,
-                      bool &t_reach) {
-    MF_TRACE(20, s);
-    // forward BFS from s over cap > 0
-    int bank = c.take_bank();
+// Reachability over arcs with capacity, forward (dir 0: x -> w) or backward
+// (dir 1: w -> x), from x.  Vertices whose stamp st[] is below S are
+// unvisited; reached ones get S and are listed in Q (bank).  Bottom-up
+// levels need the graph's hub list; without it the search is top-down.
+__device__ bool reach_all(QCtx &c, int x, int dir, unsigned *st, unsigned S, int *Q, int bank) {
     if (c.leader) {
-        c.st.mark[s] = S;
-        append1(c, s, c.st.qa, bank);
+        st[x] = S;
+        append1(c, x, Q, bank);
     }
     int f0 = 0, b0 = 0;
     if (!c.sync_tails(bank, f0, b0)) return false;
-    unsigned *mark = c.st.mark;
     const i64 *cap = c.cap;
-    auto fwd = [&](int v, int e, int w, int) -> bool {
-        i64 ce = ldro(&cap[e]);
-        unsigned mw = ldcg(&mark[w]);
+    const int *rev = c.rev;
+    auto td = [&](int v, int e, int w, int) -> bool {
+        i64 ce = ldro(&cap[dir ? ldro(&rev[e]) : e]);
+        unsigned mw = ldcg(&st[w]);
         if (ce <= 0 || mw >= S) return false;
-        return atomicMax(&mark[w], S) < S;
+        return atomicMax(&st[w], S) < S;
     };
-    // bottom-up: every vertex, hubs from the graph's hub list
     const int *hubs = c.gr->hubs;
     const int nuf = hubs ? c.n : 0, nub = hubs ? c.gr->nhub : 0;
-    const int *rev = c.rev;
-    auto fwd_uf = [&](int i) -> int {
-        return (c.deg(i) <= HUB_T && ldcg(&mark[i]) < S) ? i : -1;
-    };
-    auto fwd_ub = [&](int k) -> int {
+    auto uf = [&](int i) -> int { return (c.deg(i) <= HUB_T && ldcg(&st[i]) < S) ? i : -1; };
+    auto ub = [&](int k) -> int {
         int w = ldro(&hubs[k]);
-        return ldcg(&mark[w]) < S ? w : -1;
+        return ldcg(&st[w]) < S ? w : -1;
     };
-    auto fwd_par = [&](int w, int e, int x, int) -> bool {
-        return ldcg(&mark[x]) >= S && ldro(&cap[ldro(&rev[e])]) > 0;
+    auto par = [&](int w, int e, int y, int) -> bool {
+        return ldcg(&st[y]) >= S && ldro(&cap[dir ? e : ldro(&rev[e])]) > 0;
     };
-    auto fwd_set = [&](int w, int) -> bool {
-        mark[w] = S;
+    auto set = [&](int w, int) -> bool {
+        st[w] = S;
         return true;
     };
-    if (!bfs_dir(c, c.st.qa, bank, f0, b0, fwd, nuf, fwd_uf, nub, fwd_ub, fwd_par, fwd_set)) return false;
-    int nff = ldcg(&c.st.cnt[bank]), nfb = ldcg(&c.st.cnt[CNT_BACK + bank]);
-    t_reach = ldcg(&mark[t]) >= S;
+    return bfs_dir(c, Q, bank, f0, b0, td, nuf, uf, nub, ub, par, set);
+}
 
+// Reachability from x in direction dir restricted to the vertices stamped
+// S by an earlier search (listed in U: front nuf entries, back nub), which
+// move to stamp M and are listed in vlist (bank vb).
+__device__ bool reach_within(QCtx &c, int x, int dir, unsigned S, unsigned M, const int *U, int nuf, int nub,
+                             int vb) {
+    unsigned *mark = c.st.mark;
+    if (c.leader) {
+        mark[x] = M;
+        append1(c, x, c.st.vlist, vb);
+    }
+    int f0 = 0, b0 = 0;
+    if (!c.sync_tails(vb, f0, b0)) return false;
+    const i64 *cap = c.cap;
+    const int *rev = c.rev;
+    auto td = [&](int v, int e, int w, int) -> bool {
+        unsigned mw = ldcg(&mark[w]);
+        i64 ce = ldro(&cap[dir ? ldro(&rev[e]) : e]);
+        if (mw != S || ce <= 0) return false;
+        return atomicCAS(&mark[w], S, M) == S;
+    };
+    auto uf = [&](int i) -> int {
+        int w = ldcg(&U[i]);
+        return ldcg(&mark[w]) == S ? w : -1;
+    };
+    auto ub = [&](int k) -> int {
+        int w = back_at(c, U, k);
+        return ldcg(&mark[w]) == S ? w : -1;
+    };
+    auto par = [&](int w, int e, int y, int) -> bool {
+        return ldcg(&mark[y]) == M && ldro(&cap[dir ? e : ldro(&rev[e])]) > 0;
+    };
+    auto set = [&](int w, int) -> bool {
+        mark[w] = M;
+        return true;
+    };
+    if (!bfs_dir(c, c.st.vlist, vb, f0, b0, td, nuf, uf, nub, ub, par, set)) return false;
+    c.vf = ldcg(&c.st.cnt[vb]);
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Prune.  Stamps: S (first search), M = S+1 (kept), U (undirected, mode 0).
+// Leaves the kept vertices in vlist (front c.vf entries, back nv - c.vf) and
+// returns nv (0 if t is not reachable from s, in which case the flow is 0).
+// Mode 1 keeps fwd(s) & bwd(t): a full search from one end, then a search
+// from the other end inside the first one's set.  It starts from s, or from
+// t when fb (the pivot closures) says t is outside F: then bwd(t) cannot
+// meet F and the first search stays small, while fwd(s) may cover F.
+__device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, int &nv, bool &t_reach,
+                      const unsigned char *fb) {
+    MF_TRACE(20, s);
+    unsigned *mark = c.st.mark;
+    int bank = c.take_bank();
     int vb = c.take_bank();
     if (mode == 1) {
+        bool tfirst = fb && !(ldro_u8(&fb[t]) & KC_F);
+        int a = tfirst ? t : s, b = tfirst ? s : t, dir1 = tfirst ? 1 : 0;
+        if (!reach_all(c, a, dir1, mark, S, c.st.qa, bank)) return false;
+        int nff = ldcg(&c.st.cnt[bank]), nfb = ldcg(&c.st.cnt[CNT_BACK + bank]);
+        t_reach = ldcg(&mark[b]) >= S;
         if (!t_reach) {
             nv = 0;
             c.vf = 0;
             return true;
         }
-        // backward BFS from t over arcs whose reverse (w->v) has capacity,
-        // restricted to forward-reached vertices
-        if (c.leader) {
-            mark[t] = M;
-            append1(c, t, c.st.vlist, vb);
-        }
-        if (!c.sync_tails(vb, f0, b0)) return false;
-        auto bwd = [&](int v, int e, int w, int) -> bool {
-            unsigned mw = ldcg(&mark[w]);
-            i64 cr = ldro(&cap[ldro(&rev[e])]);
-            if (mw != S || cr <= 0) return false;
-            return atomicCAS(&mark[w], S, M) == S;
-        };
-        // bottom-up universe: the forward-reached list
-        const int *qa = c.st.qa;
-        auto bwd_uf = [&](int i) -> int {
-            int w = ldcg(&qa[i]);
-            return ldcg(&mark[w]) == S ? w : -1;
-        };
-        auto bwd_ub = [&](int k) -> int {
-            int w = back_at(c, qa, k);
-            return ldcg(&mark[w]) == S ? w : -1;
-        };
-        auto bwd_par = [&](int w, int e, int x, int) -> bool {
-            return ldcg(&mark[x]) == M && ldro(&cap[e]) > 0;
-        };
-        auto bwd_set = [&](int w, int) -> bool {
-            mark[w] = M;
-            return true;
-        };
-        if (!bfs_dir(c, c.st.vlist, vb, f0, b0, bwd, nff, bwd_uf, nfb, bwd_ub, bwd_par, bwd_set)) return false;
-        c.vf = ldcg(&c.st.cnt[vb]);
+        if (!reach_within(c, b, 1 - dir1, S, M, c.st.qa, nff, nfb, vb)) return false;
         nv = c.vf + ldcg(&c.st.cnt[CNT_BACK + vb]);
         return true;
     }
+    // mode 0: forward reach of s
+    if (!reach_all(c, s, 0, mark, S, c.st.qa, bank)) return false;
+    int nff = ldcg(&c.st.cnt[bank]), nfb = ldcg(&c.st.cnt[CNT_BACK + bank]);
+    t_reach = ldcg(&mark[t]) >= S;
+    const int *hubs = c.gr->hubs;
+    const int nuf = hubs ? c.n : 0, nub = hubs ? c.gr->nhub : 0;
     // mode 0: undirected component of t (all arcs) with qmark stamp U = M
     // (qmark stamps come from the same clock, so M is unused there), then
     // kept = forward-reached & undirected-reached, plus s and t.
@@ -481,6 +506,7 @@ __device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, i
         qm[t] = M;
         append1(c, t, c.st.qb, ub);
     }
+    int f0 = 0, b0 = 0;
     if (!c.sync_tails(ub, f0, b0)) return false;
     auto und = [&](int v, int e, int w, int) -> bool {
         if (ldcg(&qm[w]) >= M) return false;
@@ -520,6 +546,122 @@ __device__ bool prune(QCtx &c, int s, int t, int mode, unsigned S, unsigned M, i
     c.vf = ldcg(&c.st.cnt[vb]);
     nv = c.vf + ldcg(&c.st.cnt[CNT_BACK + vb]);
     return true;
+}
+
+// ---------------------------------------------------------------------------
+// Kept set of a query with s in B and t in F that is not inside the cached
+// component: the component plus the extras
+//   X = vertices reachable from s without entering F (mark stamp S),
+//   Y = vertices reaching t without entering B (qmark stamp S),
+//   extras = (X & B) | (Y & F) | (X & Y).
+// (A path from s can only leave F's complement for good, and a path into t
+// only leave B's, so fwd(s) = F | X and bwd(t) = B | Y.)  Lists the image
+// then the extras in vlist with mark = M, ex = h = 0; the caller copies the
+// image's residuals and then fixes the extras' arcs (fix_extra_arcs).
+__device__ bool prune_ext(QCtx &c, int s, int t, unsigned S, unsigned M, int &nv) {
+    const DGraph &g = *c.gr;
+    const unsigned char *fb = g.kc_fb;
+    unsigned *mark = c.st.mark, *qm = c.st.qmark;
+    const i64 *cap = c.cap;
+    const int *rev = c.rev;
+    int xb = c.take_bank(), yb = c.take_bank(), vb = c.take_bank();
+    if (c.leader) {
+        if (!(ldro_u8(&fb[s]) & KC_F)) {
+            mark[s] = S;
+            append1(c, s, c.st.qa, xb);
+        }
+        if (!(ldro_u8(&fb[t]) & KC_B)) {
+            qm[t] = S;
+            append1(c, t, c.st.qb, yb);
+        }
+        c.st.cnt[vb] = g.kc_f;  // the extras follow the image
+        c.st.cnt[CNT_BACK + vb] = g.kc_b;
+        c.st.acc[ACC_TOT + T_MASKARCS] = g.kc_arcs;
+    }
+    int f0 = 0, b0 = 0;
+    if (!c.sync_tails(xb, f0, b0)) return false;
+    int yf0 = ldcg(&c.st.cnt[yb]), yb0 = ldcg(&c.st.cnt[CNT_BACK + yb]);
+    auto xs = [&](int v, int e, int w, int) -> bool {
+        i64 ce = ldro(&cap[e]);
+        unsigned mw = ldcg(&mark[w]);
+        if (ce <= 0 || mw >= S || (ldro_u8(&fb[w]) & KC_F)) return false;
+        return atomicMax(&mark[w], S) < S;
+    };
+    if (!bfs_levels(c, c.st.qa, xb, f0, b0, xs)) return false;
+    auto ys = [&](int v, int e, int w, int) -> bool {
+        i64 cr = ldro(&cap[ldro(&rev[e])]);
+        unsigned qw = ldcg(&qm[w]);
+        if (cr <= 0 || qw >= S || (ldro_u8(&fb[w]) & KC_B)) return false;
+        return atomicMax(&qm[w], S) < S;
+    };
+    if (!bfs_levels(c, c.st.qb, yb, yf0, yb0, ys)) return false;
+    const int nxf = ldcg(&c.st.cnt[xb]), nx = nxf + ldcg(&c.st.cnt[CNT_BACK + xb]);
+    const int nyf = ldcg(&c.st.cnt[yb]), ny = nyf + ldcg(&c.st.cnt[CNT_BACK + yb]);
+    // image of the component
+    const int nimg = g.kc_f + g.kc_b;
+    int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+    for (int i = gt; i < nimg; i += gT) {
+        int pos = i < g.kc_f ? i : c.n - 1 - (i - g.kc_f);
+        int v = ldro(&g.kc_img[pos]);
+        c.st.vlist[pos] = v;
+        mark[v] = M;
+        c.st.ex[v] = 0;
+        c.st.h[v] = 0;
+    }
+    // extras
+    i64 xarcs = 0;
+    for (int base = c.gw * 32; base < nx + ny; base += c.gW * 32) {
+        int i = base + c.lane;
+        bool add = false;
+        int v = 0;
+        if (i < nx) {
+            v = i < nxf ? ldcg(&c.st.qa[i]) : back_at(c, c.st.qa, i - nxf);
+            add = (ldro_u8(&fb[v]) & KC_B) || ldcg(&qm[v]) == S;
+        } else if (i < nx + ny) {
+            int j = i - nx;
+            v = j < nyf ? ldcg(&c.st.qb[j]) : back_at(c, c.st.qb, j - nyf);
+            add = (ldro_u8(&fb[v]) & KC_F) != 0;
+        }
+        if (add) {
+            mark[v] = M;
+            c.st.ex[v] = 0;
+            c.st.h[v] = 0;
+            xarcs += c.deg(v);
+        }
+        append2(c, add, v, c.st.vlist, vb);
+    }
+    xarcs = warp_sum_i64(xarcs);
+    if (c.lane == 0 && xarcs) atomic_add_i64(&c.st.acc[ACC_TOT + T_MASKARCS], xarcs);
+    int nf = 0, nb = 0;
+    if (!c.sync_tails(vb, nf, nb)) return false;
+    c.vf = nf;
+    nv = nf + nb;
+    return true;
+}
+
+// Initial residuals on the arcs of the extras (vlist front entries from
+// kc_f, back entries from kc_b): an arc between two kept vertices starts at
+// its capacity, an arc from an extra to a dropped vertex at 0.  The image's
+// residuals must be in place (they hold 0 on arcs into the extras).
+__device__ bool fix_extra_arcs(QCtx &c, unsigned M, int nv) {
+    const DGraph &g = *c.gr;
+    const int xf = c.vf - g.kc_f;             // front extras
+    const int nb = (nv - c.vf) - g.kc_b;      // back extras
+    for (int i = c.gw; i < xf + nb; i += c.gW) {
+        int v = i < xf ? ldcg(&c.st.vlist[g.kc_f + i]) : back_at(c, c.st.vlist, g.kc_b + (i - xf));
+        int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+        for (int e = b + c.lane; e < e1; e += 32) {
+            int w = ldro(&c.col[e]);
+            bool kw = ldcg(&c.st.mark[w]) >= M;
+            c.st.res[e] = kw ? ldro(&c.cap[e]) : 0;
+            if (kw) {
+                int r = ldro(&c.rev[e]);
+                c.st.res[r] = ldro(&c.cap[r]);
+            }
+        }
+        if (c.lane == 0) c.w_verts += 1;
+    }
+    return c.sync();
 }
 
 // ---------------------------------------------------------------------------
@@ -1635,9 +1777,14 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
         unsigned S = ++c.clock;
         M = ++c.clock;
         const DGraph &g = *c.gr;
-        bool cached = p.mode != KM_KEPTSET && o.prune_mode == 1 && o.use_cache && g.kc_in &&
-                      ldro_u8(&g.kc_in[s]) && ldro_u8(&g.kc_in[t]);
-        if (cached) {
+        // kc_case 1: s and t in the cached component; 2: s in B, t in F
+        const bool use_kc = p.mode != KM_KEPTSET && o.prune_mode == 1 && o.use_cache && g.kc_in;
+        int kc_case = 0;
+        if (use_kc) {
+            if (ldro_u8(&g.kc_in[s]) && ldro_u8(&g.kc_in[t])) kc_case = 1;
+            else if (g.kc_fb && (ldro_u8(&g.kc_fb[s]) & KC_B) && (ldro_u8(&g.kc_fb[t]) & KC_F)) kc_case = 2;
+        }
+        if (kc_case == 1) {
             // s and t lie in the cached component: it is the kept set
             nv = g.kc_f + g.kc_b;
             c.vf = g.kc_f;
@@ -1653,7 +1800,10 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
             }
             if (c.leader) c.st.acc[ACC_TOT + T_MASKARCS] = g.kc_arcs;
             if (!c.sync()) return;
-        } else if (!prune(c, s, t, o.prune_mode, S, M, nv, t_reach)) {
+        } else if (kc_case == 2) {
+            if (!prune_ext(c, s, t, S, M, nv)) return;
+            t_reach = true;
+        } else if (!prune(c, s, t, o.prune_mode, S, M, nv, t_reach, use_kc ? g.kc_fb : nullptr)) {
             return;
         }
         if (p.mode == KM_KEPTSET) {
@@ -1665,6 +1815,12 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
                 ko->img[pos] = v;
                 ko->in[v] = 1;
             }
+            // closures of the pivot: F = forward-reached (stamp S or M),
+            // B = a backward search on qmark
+            int bb = c.take_bank();
+            if (!reach_all(c, s, 1, c.st.qmark, S, c.st.qb, bb)) return;
+            for (int v = gt; v < c.n; v += gT)
+                ko->fb[v] = (ldcg(&c.st.mark[v]) >= S ? KC_F : 0) | (ldcg(&c.st.qmark[v]) == S ? KC_B : 0);
             if (c.leader) {
                 qo.mask_n = nv;
                 qo.kept_front = c.vf;
@@ -1686,7 +1842,7 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
             return;
         }
         if (t_reach && nv > 0) {
-            if (cached) {
+            if (kc_case) {
                 // initial residuals of the component, copied whole (16-byte
                 // vectors); ex/h were set with the kept list above
                 const longlong2 *src = reinterpret_cast<const longlong2 *>(g.kc_res);
@@ -1698,6 +1854,7 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
                 if (gt == 0 && (A & 1)) c.st.res[A - 1] = ldro(&g.kc_res[A - 1]);
                 if (c.lane == 0 && c.gw == 0) c.w_verts += nv;
                 if (!c.sync()) return;
+                if (kc_case == 2 && !fix_extra_arcs(c, M, nv)) return;
             } else if (!init_state(c, nv, M)) {
                 return;
             }

@@ -24,6 +24,11 @@ struct DGraph {
     const unsigned char *kc_in;  // n: 1 = in the component
     const int *kc_img;           // n: kept list image
     const i64 *kc_res;           // arcs: initial residuals
+    // Closures of the pivot (KC_F / KC_B bits, NULL: none).  s in B implies
+    // fwd(s) covers F, t in F implies bwd(t) covers B, so a query with
+    // s in B and t in F keeps the component plus a few extra vertices, and
+    // for t outside F (s outside B) the search from t (s) stays outside F (B).
+    const unsigned char *kc_fb;
     int kc_f, kc_b;
     i64 kc_arcs;                 // arcs out of the component's vertices
 };
@@ -135,7 +140,13 @@ enum KMode {
 struct KcOut {
     int *img;             // n: kept list image (vlist layout)
     unsigned char *in;    // n: membership (caller zeroes it)
+    unsigned char *fb;    // n: KC_F | KC_B bits
 };
+
+// kc_fb bits: the vertex is reachable from the pivot (F) / reaches it (B).
+// F is closed under forward arcs, B under backward arcs, F & B = component.
+#define KC_F 1
+#define KC_B 2
 
 struct KParams {
     const DGraph *graphs;
