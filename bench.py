@@ -234,10 +234,15 @@ def run_engine(args):
     alg_bytes = 16.0 * (ax + vx)
     hbm, kind = peaks()
     achieved = alg_bytes / (np.mean(dev_ms) / 1e3) / 1e9
+    # DRAM traffic of one batched launch, from the committed ncu capture of
+    # the same workload (null for other workload sizes)
     traffic = None
     tp = os.path.join(ROOT, "profiles", "mf_kernel_rmat20_traffic.json")
+    workload = "rmat%d_%dq" % (args.scale, nq)
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get("bytes_per_launch")
+        tj = json.load(open(tp))
+        if tj.get("workload") == workload:
+            traffic = tj.get("bytes_per_launch")
     edges = sum(x.mask_arcs for x in stats_last)
     finish = [x.finish_ms for x in stats_last]
     res = {
@@ -257,7 +262,9 @@ def run_engine(args):
         "gpu_launches": 2 * args.steps,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4), "traffic": traffic,
-                     "peak_kind": kind, "alg_bytes_per_launch": alg_bytes},
+                     "peak_kind": kind, "alg_bytes_per_launch": alg_bytes,
+                     "traffic_gbs": (round(traffic / (np.mean(dev_ms) / 1e3) / 1e9, 1) if traffic else None),
+                     "traffic_frac": (round(traffic / (np.mean(dev_ms) / 1e3) / 1e9 / hbm, 4) if traffic else None)},
         "batched": {"qps": round(value, 3), "p50_ms": pct(finish, 50), "p99_ms": pct(finish, 99),
                     "edges_per_s": edges / (np.mean(dev_ms) / 1e3)},
         "plain": {"qps": round(total_q / (plain_total / 1e3), 3) if plain_total else None,
