@@ -83,6 +83,7 @@ size_t slot_bytes(int n, i64 arcs, int nhub) {
     add(sizeof(unsigned));                               // clock
     add(sizeof(int) * 8);                                // meta
     add(sizeof(HubWork) * (size_t)std::max(nhub, 1));    // hubw
+    add(sizeof(unsigned) * 5 * (size_t)bitmap_words(n));  // bits
     return b;
 }
 
@@ -131,6 +132,7 @@ struct SlotPool {
             s.meta = (int *)take(sizeof(int) * 8);
             s.hubw = (HubWork *)take(sizeof(HubWork) * (size_t)std::max(nhub, 1));
             s.nhub = std::max(nhub, 1);
+            s.bits = (unsigned *)take(sizeof(unsigned) * 5 * (size_t)bitmap_words(n));
             bases.push_back(base);
             host.push_back(s);
         }

@@ -56,7 +56,8 @@ constexpr size_t OFF_META = OFF_CLOCK + na_align(sizeof(unsigned));
 // a hub has more than HUB_T arcs, so at most NA_MAX_ARCS / (HUB_T + 1) exist
 constexpr int NA_MAX_HUBS = (int)(NA_MAX_ARCS / (HUB_T + 1)) + 1;
 constexpr size_t OFF_HUBW = OFF_META + na_align(sizeof(int) * 8);
-constexpr size_t NA_BYTES = OFF_HUBW + na_align(sizeof(HubWork) * NA_MAX_HUBS);
+constexpr size_t OFF_BITS = OFF_HUBW + na_align(sizeof(HubWork) * NA_MAX_HUBS);
+constexpr size_t NA_BYTES = OFF_BITS + na_align(sizeof(unsigned) * 5 * ((NA_MAX_N + 31) / 32));
 
 }  // namespace
 
@@ -155,6 +156,7 @@ extern "C" int mf_solve_csr_noalloc(int n, long long arcs, const int32_t *d_row,
     sl.meta = (int *)(b + OFF_META);
     sl.hubw = (HubWork *)(b + OFF_HUBW);
     sl.nhub = NA_MAX_HUBS;
+    sl.bits = (unsigned *)(b + OFF_BITS);
     int ctl[4] = {0, 0, s, t};  // err, q_next, s, t
     GroupBar bar0 = {0, 0, 0, 0};
     cudaError_t e = cudaMemcpyAsync(b + OFF_GRAPH, &g, sizeof g, cudaMemcpyHostToDevice, st);

@@ -345,14 +345,20 @@ __device__ void bu_level(QCtx &c, int *Q, int bank, int level, int nuf, UF uf, i
 // at most a 1/14 share of the unvisited universe (nu - visited), bottom-up
 // otherwise.  Both directions append the newly visited vertices to Q, so
 // the next level can run either way.  nuf = nub = 0: top-down only.
-template <class Claim, class UF, class UB, class Par, class Set>
+// on_level(level) runs on every thread at the start of each level.
+struct NoLevelHook {
+    __device__ void operator()(int) const {}
+};
+
+template <class Claim, class UF, class UB, class Par, class Set, class Hook = NoLevelHook>
 __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, int nuf, UF uf, int nub,
-                        UB ub, Par par, Set set) {
+                        UB ub, Par par, Set set, Hook on_level = Hook{}) {
     int flo = 0, blo = 0, level = 0;
     const long long nu = (long long)nuf + nub;
     long long visited = (long long)fhi + bhi;
     while (flo < fhi || blo < bhi) {
         MF_TRACE(10, level);
+        on_level(level);
         long long fsize = (long long)(fhi - flo) + (bhi - blo);
         if (nu > visited && fsize * 14 > nu - visited)
             bu_level(c, Q, bank, level, nuf, uf, nub, ub, par, set);
@@ -580,7 +586,6 @@ __device__ bool prune_ext(QCtx &c, int s, int t, unsigned S, unsigned M, int &nv
     }
     int f0 = 0, b0 = 0;
     if (!c.sync_tails(xb, f0, b0)) return false;
-    int yf0 = ldcg(&c.st.cnt[yb]), yb0 = ldcg(&c.st.cnt[CNT_BACK + yb]);
     auto xs = [&](int v, int e, int w, int) -> bool {
         i64 ce = ldro(&cap[e]);
         unsigned mw = ldcg(&mark[w]);
@@ -588,6 +593,11 @@ __device__ bool prune_ext(QCtx &c, int s, int t, unsigned S, unsigned M, int &nv
         return atomicMax(&mark[w], S) < S;
     };
     if (!bfs_levels(c, c.st.qa, xb, f0, b0, xs)) return false;
+    // The Y seed count must come from a barrier snapshot: once a CTA starts
+    // the Y search it appends to the same counter, and a plain read by a
+    // slower CTA would see a different frontier (and level count).
+    int yf0 = 0, yb0 = 0;
+    if (!c.sync_tails(yb, yf0, yb0)) return false;
     auto ys = [&](int v, int e, int w, int) -> bool {
         i64 cr = ldro(&cap[ldro(&rev[e])]);
         unsigned qw = ldcg(&qm[w]);
@@ -708,47 +718,72 @@ __device__ bool preflow(QCtx &c, int s) {
 }
 
 // ---------------------------------------------------------------------------
-// BFS of the global relabel (direction-optimizing, exact levels).  Every kept
-// vertex enters with height n, the seeds with 0.  Top-down: frontier vertex
-// v claims an unvisited kept vertex w with residual w->v (stamp CAS, then
-// height).  Bottom-up: an unvisited kept vertex w takes level + 1 when one
-// of its residual arcs reaches a vertex whose height is level.  Only the
-// current frontier has that height: a vertex claimed during this level
-// holds n or level + 1, whichever of its stores a reader sees, so the test
-// needs no ordering between the claim's stores.
-__device__ bool relabel_bfs(QCtx &c, int nv, unsigned M, unsigned cur, int blockv, int bank, int fhi,
-                            int bhi) {
-    unsigned *mark = c.st.mark;
+// BFS of the global relabel (direction-optimizing, exact levels) over the
+// slot's bitmaps: `vis` (visited, pre-set for dropped vertices and the
+// blocked vertex) and three frontier maps used in rotation (level L reads
+// map L % 3, fills map (L+1) % 3 and clears map (L+2) % 3).  The bitmaps
+// (n/8 bytes each) stay in L2 while the per-vertex arrays do not, so the
+// visited and frontier tests per examined arc cost no DRAM sector.
+// Top-down: frontier vertex v claims an unvisited w with residual w->v
+// (atomicOr on the visited word).  Bottom-up: an unvisited kept vertex w
+// takes level + 1 when one of its residual arcs reaches the frontier map.
+// Claims write the height and the next frontier bit.
+__device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi) {
+    const int W = bitmap_words(c.n);
+    unsigned *vis = c.st.bits + W, *F = c.st.bits + 2 * W;
     const int *rev = c.rev;
     i64 *res = c.st.res;
     int *h = c.st.h;
     const int *vl = c.st.vlist;
+    auto fmap = [&](int level) -> unsigned * { return F + (size_t)(level % 3) * W; };
     auto relab = [&](int v, int e, int w, int level) -> bool {
-        // stamp and reverse residual are loaded together (one latency)
-        unsigned mw = ldcg(&mark[w]);
+        const unsigned bit = 1u << (w & 31);
+        unsigned vw = ldcg(&vis[w >> 5]);
         i64 rr = ldcg(&res[ldro(&rev[e])]);
-        if (w == blockv || mw < M || mw >= cur || rr <= 0) return false;
-        if (atomicCAS(&mark[w], mw, cur) != mw) return false;
+        if ((vw & bit) || rr <= 0) return false;
+        if (atomicOr(&vis[w >> 5], bit) & bit) return false;
         h[w] = level + 1;
+        atomicOr(&fmap(level + 1)[w >> 5], bit);
         return true;
     };
+    auto unvisited = [&](int w) -> bool { return !((ldcg(&vis[w >> 5]) >> (w & 31)) & 1u); };
     auto uf = [&](int i) -> int {
         int w = ldcg(&vl[i]);
-        return (w != blockv && ldcg(&mark[w]) != cur) ? w : -1;
+        return unvisited(w) ? w : -1;
     };
     auto ub = [&](int k) -> int {
         int w = back_at(c, vl, k);
-        return (w != blockv && ldcg(&mark[w]) != cur) ? w : -1;
+        return unvisited(w) ? w : -1;
     };
     auto par = [&](int w, int e, int x, int level) -> bool {
-        return ldcg(&res[e]) > 0 && ldcg(&h[x]) == level;
+        return ldcg(&res[e]) > 0 && ((ldcg(&fmap(level)[x >> 5]) >> (x & 31)) & 1u);
     };
     auto set = [&](int w, int level) -> bool {
+        const unsigned bit = 1u << (w & 31);
         h[w] = level + 1;
-        mark[w] = cur;
+        atomicOr(&vis[w >> 5], bit);
+        atomicOr(&fmap(level + 1)[w >> 5], bit);
         return true;
     };
-    return bfs_dir(c, c.st.qa, bank, fhi, bhi, relab, c.vf, uf, nv - c.vf, ub, par, set);
+    auto clear_next = [&](int level) {
+        unsigned *z = fmap(level + 2);
+        int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+        for (int wd = gt; wd < W; wd += gT) z[wd] = 0;
+    };
+    return bfs_dir(c, c.st.qa, bank, fhi, bhi, relab, c.vf, uf, nv - c.vf, ub, par, set, clear_next);
+}
+
+// Kept-vertex bitmap of the query (bit v: mark[v] >= M), read by every
+// global relabel to pre-set the visited map.
+__device__ bool build_kept_bits(QCtx &c, unsigned M) {
+    MF_TRACE(60, c.n);
+    const int W = bitmap_words(c.n);
+    for (int wd = c.gw; wd < W; wd += c.gW) {
+        int v = wd * 32 + c.lane;
+        unsigned word = __ballot_sync(MF_FULL, v < c.n && ldcg(&c.st.mark[v]) >= M);
+        if (c.lane == 0) c.st.bits[wd] = word;
+    }
+    return c.sync();
 }
 
 // ---------------------------------------------------------------------------
@@ -763,10 +798,24 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
                                bool deficit_seeds, int *L, int lbk, int &naf, int &nab, int &nd,
                                i64 *&ab) {
     MF_TRACE(40, nv);
-    unsigned cur = ++c.clock;
     int qbk = c.take_bank();
     const int n = c.n;
-    unsigned *mark = c.st.mark;
+    // bitmaps: visited = not kept, plus the blocked vertex; frontier maps empty
+    const int W = bitmap_words(n);
+    unsigned *kept = c.st.bits, *vis = kept + W, *F0 = kept + 2 * W;
+    {
+        int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+        for (int wd = gt; wd < W; wd += gT) {
+            unsigned x = ~ldcg(&kept[wd]);
+            if (blockv >= 0 && wd == (blockv >> 5)) x |= 1u << (blockv & 31);
+            vis[wd] = x;
+            F0[wd] = 0;
+            F0[W + wd] = 0;
+            F0[2 * W + wd] = 0;
+        }
+    }
+    if (!c.sync()) return false;
+    MF_TRACE(42, nv);
     // seeds
     for (int base = c.gw * 32; base < nv; base += c.gW * 32) {
         int i = base + c.lane;
@@ -776,7 +825,10 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
             v = c.vat(i);
             if (v == sinkv) seed = true;
             else if (deficit_seeds && v != blockv && v != srcv && ldcg(&c.st.ex[v]) < 0) seed = true;
-            if (seed) mark[v] = cur;
+            if (seed) {
+                atomicOr(&vis[v >> 5], 1u << (v & 31));
+                atomicOr(&F0[v >> 5], 1u << (v & 31));
+            }
             // every kept vertex starts the search at height n (unreached)
             c.st.h[v] = seed ? 0 : n;
         }
@@ -784,7 +836,8 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
     }
     int f0 = 0, b0 = 0;
     if (!c.sync_tails(qbk, f0, b0)) return false;
-    if (!relabel_bfs(c, nv, M, cur, blockv, qbk, f0, b0)) return false;
+    MF_TRACE(43, f0 + b0);
+    if (!relabel_bfs(c, nv, qbk, f0, b0)) return false;
     int *h = c.st.h;
 
     // sweep: heights of unreached vertices, active list, counts
@@ -1864,6 +1917,7 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
     i64 flow = 0;
     u64 t_pruned = globaltimer_ns();
     if (t_reach && nv > 0) {
+        if (!build_kept_bits(c, M)) return;
         if (p.mode == KM_HEIGHTS) {
             int naf = 0, nab = 0, nd = 0;
             i64 *ab = nullptr;

@@ -68,7 +68,11 @@ struct DSlot {
     int *meta;         // per-slot query meta (mask stamp, nv, s, t, front count) for warm starts
     HubWork *hubw;     // nhub entries
     int nhub;          // capacity of hubw (hub vertices of the largest graph served)
+    unsigned *bits;    // 5 bitmaps of (n + 31) / 32 words: kept, visited, 3 frontier maps
 };
+
+// Words of one per-vertex bitmap.
+__host__ __device__ inline int bitmap_words(int n) { return (n + 31) >> 5; }
 
 // Options as seen by the kernel (resolved on the host).
 struct KOpts {
