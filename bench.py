@@ -39,7 +39,7 @@ METRIC = "exact max-flow queries/sec + p50/p99 latency, batched vs plain, same B
 WORKLOAD = "rmat20_256q"
 SCALE, DRAWS, NHUB, NUNI, R = 20, 1 << 24, 128, 128, 128
 GRAPH_SEED, QUERY_SEED = 1, 2
-QOUT_BYTES = 160  # device per-query record copied back by mf_solve_batch
+QOUT_BYTES = 184  # device per-query record copied back by mf_solve_batch
 
 
 def peaks():
@@ -162,9 +162,18 @@ def cpu_baseline(n, u, v, c, s, t, budget_s=20.0):
         flows += list(O.dinic_batch(g, s[idx], t[idx], threads))
         t_solve += time.time() - t1
         done += len(idx)
+    # the same solver on one core, over the first queries of the sample
+    one, t_one = 0, 0.0
+    while one < done and t_one < budget_s / 4:
+        t1 = time.time()
+        O.dinic_batch(g, s[order[one:one + 1]], t[order[one:one + 1]], 1)
+        t_one += time.time() - t1
+        one += 1
     return {"value": done / t_solve, "unit": "queries/s", "cores": threads, "kind": "port",
+            "value_1core": (one / t_one) if t_one > 0 else None,
             "sample": "%d of the 256 queries (alternating hub/uniform), C Dinic over %d threads, "
-                      "%.1f s solve (+%.1f s CSR build)" % (done, threads, t_solve, build_s)}, \
+                      "%.1f s solve (+%.1f s CSR build); 1 core: first %d of them, %.1f s" % (
+                          done, threads, t_solve, build_s, one, t_one)}, \
         order[:done], flows
 
 
@@ -232,6 +241,10 @@ def run_engine(args):
     ax = sum(x.arcs_examined for x in stats_last)
     vx = sum(x.vertices_examined for x in stats_last)
     alg_bytes = 16.0 * (ax + vx)
+    # implementation-independent reference figure: what a classic top-down
+    # relabel reads (every kept arc once per global relabel performed); the
+    # direction-optimizing search reads less
+    full_scan_bytes = 16.0 * sum(x.mask_arcs * x.global_relabels for x in stats_last)
     hbm, kind = peaks()
     achieved = alg_bytes / (np.mean(dev_ms) / 1e3) / 1e9
     # DRAM traffic of one batched launch, from the committed ncu capture of
@@ -263,6 +276,7 @@ def run_engine(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4), "traffic": traffic,
                      "peak_kind": kind, "alg_bytes_per_launch": alg_bytes,
+                     "relabel_full_scan_bytes_per_launch": full_scan_bytes,
                      "traffic_gbs": (round(traffic / (np.mean(dev_ms) / 1e3) / 1e9, 1) if traffic else None),
                      "traffic_frac": (round(traffic / (np.mean(dev_ms) / 1e3) / 1e9 / hbm, 4) if traffic else None)},
         "batched": {"qps": round(value, 3), "p50_ms": pct(finish, 50), "p99_ms": pct(finish, 99),
@@ -282,7 +296,7 @@ def run_engine(args):
     if args.dump and rank == 0:
         keys = ["flow", "mask_vertices", "mask_arcs", "rounds", "global_relabels", "arcs_examined",
                 "vertices_examined", "pushes", "path_push_rounds", "hot_sweeps", "rm_fixed", "service_ms",
-                "finish_ms", "prune_ms", "relabel_ms", "rounds_ms", "relabel_arcs"]
+                "finish_ms", "prune_ms", "relabel_ms", "rounds_ms", "relabel_arcs", "hub_arcs", "hub_passes", "hub_relabels"]
         with open(args.dump, "w") as f:
             for i, x in enumerate(stats_last):
                 row = {k: getattr(x, k) for k in keys}
@@ -392,7 +406,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--group", type=int, default=4)
+    ap.add_argument("--group", type=int, default=8)
     ap.add_argument("--serve", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)

@@ -47,7 +47,7 @@ typedef struct mf_graph mf_graph;
 typedef struct mf_opts {
     int kernel_cycles;     /* K: discharge cycles per active vertex per round (RA:1467 uses max(4, avg
                               degree) with one push per cycle; each cycle here pushes to every
-                              downhill arc); 0 = 4 */
+                              downhill arc); 0 = 8 */
     int gr_freq;           /* rounds between global relabels at most (default 16; RA:1466 uses 128) */
     double gr_work_alpha;  /* also relabel once scanned arcs exceed alpha x mask arcs (0 = off) */
     int prune_mode;        /* 0: RA:1391-1445 mask (fwd(s) & undirected comp(t)); 1: fwd(s) & bwd(t) (default) */
@@ -63,7 +63,7 @@ typedef struct mf_opts {
     int force_rm;          /* tests: run RM every rm_freq rounds regardless of frac_high */
     int force_path_push;   /* tests: use path push whenever active <= path_push_switch */
     long long iter_max;    /* round cap per solve (RA:1476) */
-    int group_ctas;        /* CTAs per query group in batched solves (0 = 4) */
+    int group_ctas;        /* CTAs per query group in batched solves (0 = 8) */
     int threads;           /* threads per CTA: a multiple of 32 in [64, 512] (0 = 512) */
     int certify;           /* 1 = return excess to the source and check the certificate */
     int verbose;           /* 1 = per-query log lines on stderr */
@@ -98,6 +98,9 @@ typedef struct mf_stats {
     double relabel_ms;        /* device time in global relabels */
     double rounds_ms;         /* device time in discharge rounds */
     long long relabel_arcs;   /* arc examinations inside global relabels */
+    long long hub_arcs;       /* arc examinations by the chunked discharge of hubs */
+    long long hub_passes;     /* hub discharge passes */
+    long long hub_relabels;   /* hub passes that ended in a relabel (excess left) */
 } mf_stats;
 
 void mf_opts_default(mf_opts *o);

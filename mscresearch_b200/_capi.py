@@ -68,6 +68,9 @@ class MfStats(C.Structure):
         ("relabel_ms", C.c_double),
         ("rounds_ms", C.c_double),
         ("relabel_arcs", C.c_longlong),
+        ("hub_arcs", C.c_longlong),
+        ("hub_passes", C.c_longlong),
+        ("hub_relabels", C.c_longlong),
     ]
 
 

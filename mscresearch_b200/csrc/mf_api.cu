@@ -62,6 +62,9 @@ int dev_info(DevInfo &d, int threads) {
     int dev = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
+    // L2 fetch granularity hint for this process's context (bytes fetched
+    // from DRAM per L2 miss: 0..128); it lasts as long as the context
+    if (const char *e = getenv("MF_L2_FETCH_BYTES")) CK(cudaDeviceSetLimit(cudaLimitMaxL2FetchGranularity, (size_t)atoi(e)));
     d.threads = threads;
     d.bps = mf_kernel_max_blocks_per_sm(threads);
     if (d.bps <= 0) return fail(MF_ERR_CUDA, "mf_kernel cannot be resident with %d threads", threads);
@@ -433,7 +436,7 @@ int ensure_launch_buffers(mf_graph *g, int nq, int nslots) {
 
 KOpts resolve_opts(const mf_opts &o, int avg_deg) {
     KOpts k;
-    k.K = o.kernel_cycles > 0 ? o.kernel_cycles : 4;
+    k.K = o.kernel_cycles > 0 ? o.kernel_cycles : 8;
     (void)avg_deg;
     k.gr_freq = std::max(1, o.gr_freq);
     k.gr_alpha = o.gr_work_alpha;
@@ -578,6 +581,9 @@ void fill_stats(mf_stats *st, const QOut &q, double ms, u64 launch_t0) {
     st->relabel_ms = (double)q.t_relabel * 1e-6;
     st->rounds_ms = (double)q.t_rounds * 1e-6;
     st->relabel_arcs = q.arcs_relabel;
+    st->hub_arcs = q.arcs_hubs;
+    st->hub_passes = q.hub_passes;
+    st->hub_relabels = q.hub_relabels;
     st->finish_ms = launch_t0 ? (double)(q.t_done - launch_t0) * 1e-6 : 0.0;
     st->flow = q.flow;
     st->status = status_from_err(q.status);
@@ -916,7 +922,7 @@ static int solve_common(mf_graph *g, int nq, const int32_t *s, const int32_t *t,
     int rc0 = ensure_kept_cache(g, o);
     if (rc0) return rc0;
     std::vector<QOut> outs(nq);
-    int G = single ? 0 : (o.group_ctas > 0 ? o.group_ctas : 4);
+    int G = single ? 0 : (o.group_ctas > 0 ? o.group_ctas : 8);
     // batched: queue order by expected cost (largest first), results unpermuted
     std::vector<int> perm;
     if (!single && o.schedule && nq > 1 && mode == KM_SOLVE) {
@@ -1150,7 +1156,7 @@ static int session_run(mf_session *ss, int mode, const ArcUpdate *d_upd, int nup
                        mf_stats *stats) {
     mf_graph *g = ss->g;
     std::vector<QOut> outs(ss->nq);
-    int G = ss->opts.group_ctas > 0 ? ss->opts.group_ctas : 4;
+    int G = ss->opts.group_ctas > 0 ? ss->opts.group_ctas : 8;
     int rc = launch(g, ss->pool, ss->nq, ss->s.data(), ss->t.data(), true, ss->opts, mode, nullptr,
                     d_upd, nupd, G, outs.data());
     if (rc) return rc;
@@ -1324,7 +1330,7 @@ int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int ma
         delete sv;
         return rc;
     }
-    sv->G = sv->opts.group_ctas > 0 ? sv->opts.group_ctas : 4;
+    sv->G = sv->opts.group_ctas > 0 ? sv->opts.group_ctas : 8;
     int groups = std::max(1, di.sms * di.bps / sv->G);
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);

@@ -77,6 +77,9 @@
 #define T_PUSH 2
 #define T_MASKARCS 3
 #define T_RARCS 4
+#define T_HARCS 5
+#define T_HPASS 6
+#define T_HREL 7
 
 #define SMALL_T 32  // at most this many arcs: one lane per vertex in discharge
 #define MAX_WARPS 32
@@ -136,12 +139,15 @@ struct QCtx {
         ++aseq;
         return st.acc + b * ACC_BANK;
     }
+    // All 32 lanes call it: the counters live on the lanes that did the work
+    // (lane 0, or the first lane of each 8-lane discharge tile).
     __device__ void flush_warp_counts() {
+        i64 a = warp_sum_i64(w_arcs), v = warp_sum_i64(w_verts), p = warp_sum_i64(w_push);
         if (lane == 0) {
             i64 *tot = st.acc + ACC_TOT;
-            if (w_arcs) atomic_add_i64(&tot[T_ARCS], w_arcs);
-            if (w_verts) atomic_add_i64(&tot[T_VERTS], w_verts);
-            if (w_push) atomic_add_i64(&tot[T_PUSH], w_push);
+            if (a) atomic_add_i64(&tot[T_ARCS], a);
+            if (v) atomic_add_i64(&tot[T_VERTS], v);
+            if (p) atomic_add_i64(&tot[T_PUSH], p);
         }
         w_arcs = w_verts = w_push = 0;
     }
@@ -1096,7 +1102,10 @@ __device__ bool hub_setup(QCtx &c, const int *L, int nb, const int *hot) {
 __device__ void discharge_hubs(QCtx &c, const int *L, int nb, int sinkv, int blockv, int *N, int nbk,
                                unsigned rstamp, i64 *ab) {
     const int n = c.n;
-    i64 arcs = 0;  // this warp's arc examinations, added to the round's work once
+    // this warp's arc examinations (statistics) and the arcs of the chunks it
+    // covered, scanned or skipped (the relabel trigger's work measure: a
+    // skipped chunk stands for work the pass did not need to repeat)
+    i64 arcs = 0, work = 0;
     nb = min(nb, c.st.nhub);
     const int T = ldcg(&c.st.cnt[CNT_HUBCH]);
     // this warp's contiguous share of the (hub, chunk) index space
@@ -1124,6 +1133,13 @@ __device__ void discharge_hubs(QCtx &c, const int *L, int nb, int sinkv, int blo
             int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
             int ch = j - cs;
             int e = b + ch * 32 + c.lane;
+            // Once the hub's budget is spent the pass cannot end in a relabel
+            // (budget only falls), so the chunk's scan would serve nothing:
+            // only its completion is recorded.
+            i64 bud = 0;
+            if (c.lane == 0) bud = ldcg(&hw->budget);
+            bud = __shfl_sync(MF_FULL, bud, 0);
+            if (bud <= 0) e = e1;
             i64 r = 0;
             int w = 0, hwt = MF_INF_H;
             if (e < e1) {
@@ -1153,7 +1169,9 @@ __device__ void discharge_hubs(QCtx &c, const int *L, int nb, int sinkv, int blo
             if (c.lane == 0) {
                 if (take) atomic_add_i64(&c.st.ex[v], -take);
                 if (mh != MF_INF_H) atomicMin(&hw->minh, mh);
-                arcs += min(32, e1 - (b + ch * 32));
+                int chunk_arcs = min(32, ldro(&c.row[v + 1]) - (b + ch * 32));
+                work += chunk_arcs;
+                if (bud > 0) arcs += chunk_arcs;
                 c.w_push += take ? 1 : 0;
                 __threadfence();
                 if (atomicAdd(&hw->done, 1) == nch - 1) {
@@ -1161,10 +1179,12 @@ __device__ void discharge_hubs(QCtx &c, const int *L, int nb, int sinkv, int blo
                     __threadfence();
                     i64 left = atomic_add_i64(&hw->budget, 0);
                     int hnew = hv;
+                    atomic_add_i64(&c.st.acc[ACC_TOT + T_HPASS], 1);
                     if (left > 0) {
                         int m = atomicAdd(&hw->minh, 0);
                         hnew = (m >= n - 1) ? n : m + 1;
                         c.st.h[v] = hnew;
+                        atomic_add_i64(&c.st.acc[ACC_TOT + T_HREL], 1);
                     }
                     i64 ev = ldcg(&c.st.ex[v]);
                     if (ev > 0 && hnew < n && enlist(c, v, rstamp)) append1(c, v, N, nbk);
@@ -1173,9 +1193,10 @@ __device__ void discharge_hubs(QCtx &c, const int *L, int nb, int sinkv, int blo
             }
         }
     }
-    if (c.lane == 0 && arcs) {
+    if (c.lane == 0 && work) {
         c.w_arcs += arcs;
-        atomic_add_i64(&ab[A_WORK], arcs);
+        atomic_add_i64(&ab[A_WORK], work);
+        if (arcs) atomic_add_i64(&c.st.acc[ACC_TOT + T_HARCS], arcs);
     }
 }
 
@@ -1529,11 +1550,11 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
                 force_gr = true;
                 stag = 0;
                 gr_freq = min(2 * gr_base, gr_freq * 2);
-                K = min(16, K * 2);
+                K = min(max(16, 2 * o.K), K * 2);
                 calm = 0;
             } else if (++calm >= o.stagnate) {
                 gr_freq = max(gr_base, gr_freq / 2);
-                K = max(4, K / 2);
+                K = max(o.K, K / 2);
                 calm = 0;
             }
             // hot-region extra sweep over the next worklist (RA:1899-1984)
@@ -1970,6 +1991,9 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
         qo.t_relabel = c.tm_relabel;
         qo.t_rounds = c.tm_rounds;
         qo.arcs_relabel = tot[T_RARCS];
+        qo.arcs_hubs = tot[T_HARCS];
+        qo.hub_passes = tot[T_HPASS];
+        qo.hub_relabels = tot[T_HREL];
         p.out[q] = qo;
         c.st.meta[0] = (int)M;
         c.st.meta[1] = nv;

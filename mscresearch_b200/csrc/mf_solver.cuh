@@ -115,6 +115,9 @@ struct QOut {
     u64 t_relabel; // ns in global relabels
     u64 t_rounds;  // ns in discharge rounds (incl. hot sweep, path push, RM)
     i64 arcs_relabel; // arc examinations inside global relabels
+    i64 arcs_hubs;    // arc examinations by the chunked hub discharge
+    i64 hub_passes;   // hub discharge passes (a hub with excess, all its chunks)
+    i64 hub_relabels; // passes that ended with excess left (the hub was relabeled)
     int mask_n;
     int status;
     int kept_front;  // kept vertices in vlist's front part
