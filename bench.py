@@ -39,7 +39,7 @@ METRIC = "exact max-flow queries/sec + p50/p99 latency, batched vs plain, same B
 WORKLOAD = "rmat20_256q"
 SCALE, DRAWS, NHUB, NUNI, R = 20, 1 << 24, 128, 128, 128
 GRAPH_SEED, QUERY_SEED = 1, 2
-QOUT_BYTES = 184  # device per-query record copied back by mf_solve_batch
+QOUT_BYTES = 208  # device per-query record copied back by mf_solve_batch
 
 
 def peaks():
@@ -296,7 +296,7 @@ def run_engine(args):
     if args.dump and rank == 0:
         keys = ["flow", "mask_vertices", "mask_arcs", "rounds", "global_relabels", "arcs_examined",
                 "vertices_examined", "pushes", "path_push_rounds", "hot_sweeps", "rm_fixed", "service_ms",
-                "finish_ms", "prune_ms", "relabel_ms", "rounds_ms", "relabel_arcs", "hub_arcs", "hub_passes", "hub_relabels"]
+                "finish_ms", "prune_ms", "relabel_ms", "rounds_ms", "relabel_arcs", "hub_arcs", "hub_passes", "hub_relabels", "levels", "levels_bottom_up", "levels_solo"]
         with open(args.dump, "w") as f:
             for i, x in enumerate(stats_last):
                 row = {k: getattr(x, k) for k in keys}

@@ -101,6 +101,9 @@ typedef struct mf_stats {
     long long hub_arcs;       /* arc examinations by the chunked discharge of hubs */
     long long hub_passes;     /* hub discharge passes */
     long long hub_relabels;   /* hub passes that ended in a relabel (excess left) */
+    long long levels;         /* search levels (prune, global relabels, certificate) */
+    long long levels_bottom_up; /* of which bottom-up */
+    long long levels_solo;    /* of which run by a single CTA */
 } mf_stats;
 
 void mf_opts_default(mf_opts *o);

@@ -71,6 +71,9 @@ class MfStats(C.Structure):
         ("hub_arcs", C.c_longlong),
         ("hub_passes", C.c_longlong),
         ("hub_relabels", C.c_longlong),
+        ("levels", C.c_longlong),
+        ("levels_bottom_up", C.c_longlong),
+        ("levels_solo", C.c_longlong),
     ]
 
 

@@ -80,7 +80,7 @@ size_t slot_bytes(int n, i64 arcs, int nhub) {
     for (int i = 0; i < 7; ++i) add(sizeof(int) * (size_t)n);  // h mark qmark claim vlist qa qb
     add(sizeof(int) * 1024);                             // hot
     add(sizeof(int) * 1024);                             // ract
-    add(sizeof(int) * 32);                               // cnt
+    add(sizeof(int) * CNT_WORDS);                        // cnt
     add(sizeof(i64) * 128);                              // acc
     add(sizeof(GroupBar));
     add(sizeof(unsigned));                               // clock
@@ -128,7 +128,7 @@ struct SlotPool {
             s.qb = (int *)take(sizeof(int) * (size_t)n);
             s.hot = (int *)take(sizeof(int) * 1024);
             s.ract = (int *)take(sizeof(int) * 1024);
-            s.cnt = (int *)take(sizeof(int) * 32);
+            s.cnt = (int *)take(sizeof(int) * CNT_WORDS);
             s.acc = (i64 *)take(sizeof(i64) * 128);
             s.bar = (GroupBar *)take(sizeof(GroupBar));
             s.clock = (unsigned *)take(sizeof(unsigned));
@@ -584,6 +584,9 @@ void fill_stats(mf_stats *st, const QOut &q, double ms, u64 launch_t0) {
     st->hub_arcs = q.arcs_hubs;
     st->hub_passes = q.hub_passes;
     st->hub_relabels = q.hub_relabels;
+    st->levels = q.levels;
+    st->levels_bottom_up = q.levels_bottom_up;
+    st->levels_solo = q.levels_solo;
     st->finish_ms = launch_t0 ? (double)(q.t_done - launch_t0) * 1e-6 : 0.0;
     st->flow = q.flow;
     st->status = status_from_err(q.status);

@@ -49,7 +49,7 @@ constexpr size_t OFF_QB = OFF_QA + na_align(sizeof(int) * NA_MAX_N);
 constexpr size_t OFF_HOT = OFF_QB + na_align(sizeof(int) * NA_MAX_N);
 constexpr size_t OFF_RACT = OFF_HOT + na_align(sizeof(int) * 1024);
 constexpr size_t OFF_CNT = OFF_RACT + na_align(sizeof(int) * 1024);
-constexpr size_t OFF_ACC = OFF_CNT + na_align(sizeof(int) * 32);
+constexpr size_t OFF_ACC = OFF_CNT + na_align(sizeof(int) * CNT_WORDS);
 constexpr size_t OFF_BAR = OFF_ACC + na_align(sizeof(i64) * 128);
 constexpr size_t OFF_CLOCK = OFF_BAR + na_align(sizeof(GroupBar));
 constexpr size_t OFF_META = OFF_CLOCK + na_align(sizeof(unsigned));

@@ -43,10 +43,15 @@
 #include <climits>
 #include <cstring>
 
-// cnt[0..7]: front tails of the list banks, cnt[16..23]: their back (hub)
-// tails.  Banks are handed out in rotation; taking bank k zeroes bank k+4
-// (mod 8), last read at least one group barrier earlier (no code path takes
-// more than three banks between two barriers).
+// The slot's control words (CNT_WORDS ints):
+//   cnt[0..7]    front tails of the list banks, cnt[16..23] their back (hub)
+//                tails.  Banks are handed out in rotation; taking bank k
+//                zeroes bank k+4 (mod 8), last read at least one group barrier
+//                earlier (no code path takes more than three banks between
+//                two barriers);
+//   cnt[8..12]   query hand-off and serving request words;
+//   cnt[30]      total chunks of the current hub pass;
+//   cnt[32..38]  level state published by a solo search episode.
 #define NBANKS 8
 #define CNT_BACK 16
 #define CNT_HUBCH 30  // total chunks of the current hub pass
@@ -57,6 +62,9 @@
 #define CNT_RG 12
 #define ACC_BANK 16  // i64 fields per accumulator bank
 #define ACC_TOT 64   // start of per-query totals (within acc, 64 i64 reserved for banks)
+#define ACC_GR_DUR 80  // duration of the last global relabel (ns, leader's clock)
+#define ACC_GR_END 81  // leader's clock at its end
+#define DEEP_LEVELS 256  // a relabel search deeper than this is "deep" (see run_phases)
 
 // accumulator fields (per bank)
 #define A_SUMEX 0
@@ -70,6 +78,7 @@
 #define A_VERTS 8
 #define A_CUT 9
 #define A_BAD 10
+#define A_TIME 11   // leader's clock when it finished the round's discharge
 
 // per-query totals
 #define T_ARCS 0
@@ -80,6 +89,9 @@
 #define T_HARCS 5
 #define T_HPASS 6
 #define T_HREL 7
+#define T_LEVELS 8   // search levels (prune, relabels, certificate)
+#define T_BU 9       // of which bottom-up
+#define T_SOLO 10    // of which run solo by one CTA
 
 #define SMALL_T 32  // at most this many arcs: one lane per vertex in discharge
 #define MAX_WARPS 32
@@ -224,15 +236,20 @@ __shared__ int s_lbs_x[MAX_WARPS][32];
 
 // One top-down level.  Functor cl(v, e, w, level) returns true when arc
 // e = v->w claims w (it performs the claim itself).
+// The level's work is spread over warps gw, gw + gW, ... (the whole group,
+// or one CTA in a solo level).
 template <class Claim>
 __device__ void td_level(QCtx &c, int *Q, int bank, int flo, int fhi, int blo, int bhi, int level,
-                         Claim cl) {
+                         Claim cl, int gw, int gW) {
     int *sv = s_lbs_v[c.warp], *sb = s_lbs_b[c.warp], *sx = s_lbs_x[c.warp];
-    // front: 32 vertices per warp, arcs balanced over the lanes
-    for (int base = flo + c.gw * 32; base < fhi; base += c.gW * 32) {
+    // front: vpw vertices per warp (the frontier spread over all gW warps,
+    // 1 to 32 each), their arcs balanced over the lanes
+    const int nf = fhi - flo;
+    const int vpw = max(1, min(32, (nf + gW - 1) / gW));
+    for (int base = flo + gw * vpw; base < fhi; base += gW * vpw) {
         int i = base + c.lane;
         int v = 0, b = 0, d = 0;
-        if (i < fhi) {
+        if (c.lane < vpw && i < fhi) {
             v = ldcg(&Q[i]);
             if (MF_OK_IDX(v, c.n, 11)) {
                 b = ldro(&c.row[v]);
@@ -263,7 +280,7 @@ __device__ void td_level(QCtx &c, int *Q, int bank, int flo, int fhi, int blo, i
         __syncwarp();
         if (c.lane == 0) {
             c.w_arcs += total;
-            c.w_verts += min(32, fhi - base);
+            c.w_verts += min(vpw, fhi - base);
         }
     }
     // back: hub arcs in 32-arc chunks over all warps of the group
@@ -271,7 +288,7 @@ __device__ void td_level(QCtx &c, int *Q, int bank, int flo, int fhi, int blo, i
         int v = back_at(c, Q, k);
         int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
         int nch = (e1 - b + 31) >> 5;
-        for (int ch = c.gw; ch < nch; ch += c.gW) {
+        for (int ch = gw; ch < nch; ch += gW) {
             int e = b + ch * 32 + c.lane;
             bool ok = false;
             int w = 0;
@@ -282,7 +299,7 @@ __device__ void td_level(QCtx &c, int *Q, int bank, int flo, int fhi, int blo, i
             append2(c, ok, w, Q, bank);
             if (c.lane == 0) c.w_arcs += min(32, e1 - (b + ch * 32));
         }
-        if (c.lane == 0 && c.gw == 0) c.w_verts += 1;
+        if (c.lane == 0 && gw == 0) c.w_verts += 1;
     }
 }
 
@@ -347,37 +364,110 @@ __device__ void bu_level(QCtx &c, int *Q, int bank, int level, int nuf, UF uf, i
     if (c.lane == 0) c.w_arcs += arcs;
 }
 
-// Direction-optimizing BFS: a level runs top-down while the frontier holds
-// at most a 1/14 share of the unvisited universe (nu - visited), bottom-up
-// otherwise.  Both directions append the newly visited vertices to Q, so
-// the next level can run either way.  nuf = nub = 0: top-down only.
-// on_level(level) runs on every thread at the start of each level.
 struct NoLevelHook {
-    __device__ void operator()(int) const {}
+    __device__ void operator()(int, int, int, int, int, int, int) const {}
 };
 
+#define SOLO_MAX 96         // a hub-free top-down frontier at most this large runs solo
+#define SOLO_LEVELS 1024    // levels per solo episode at most
+#define CNT_SOLO 32         // cnt[32..38]: state published by a solo episode
+static_assert(CNT_SOLO >= CNT_BACK + NBANKS && CNT_SOLO > CNT_HUBCH && CNT_SOLO + 7 <= CNT_WORDS,
+              "solo state must not overlap the other control words");
+
+// Direction-optimizing BFS: a level runs bottom-up when the frontier holds
+// more than a 1/14 share of the unvisited universe (nu - visited) and at
+// least 1/64 of the universe, top-down otherwise.  Both directions append
+// the newly visited vertices to Q, so the next level can run either way,
+// and visited = the queue's length.
+// Small top-down frontiers run "solo": the group's first CTA expands them
+// level after level with block barriers (up to SOLO_LEVELS, while the
+// frontier stays top-down, hub-free and at most SOLO_MAX), then publishes the level
+// state; the other CTAs wait at one group barrier instead of one per level
+// (deep, narrow searches: grids, chains).  nuf = nub = 0: top-down only.
+// on_level(level, plo, phi, pblo, pbhi, tid, nthreads) runs at the start of
+// each level on the threads doing it; [plo, phi) and back [pblo, pbhi) are
+// the previous level's frontier.
 template <class Claim, class UF, class UB, class Par, class Set, class Hook = NoLevelHook>
 __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, int nuf, UF uf, int nub,
-                        UB ub, Par par, Set set, Hook on_level = Hook{}) {
-    int flo = 0, blo = 0, level = 0;
+                        UB ub, Par par, Set set, Hook on_level = Hook{}, int *levels_out = nullptr) {
+    int flo = 0, blo = 0, pflo = 0, pblo = 0, level = 0, nbu = 0, nsolo = 0;
     const long long nu = (long long)nuf + nub;
-    long long visited = (long long)fhi + bhi;
+    const int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
     while (flo < fhi || blo < bhi) {
+        const long long visited = (long long)fhi + bhi;
+        const long long fsize = (long long)(fhi - flo) + (bhi - blo);
+        // bottom-up sweeps the whole universe, so the frontier must also be a
+        // sizeable share of it (a small frontier near the end of a deep
+        // search is cheaper to expand than nu candidates are to check)
+        const bool bottom_up = nu > visited && fsize * 14 > nu - visited && fsize * 64 > nu;
+        if (!bottom_up && c.G > 1 && fsize <= SOLO_MAX && bhi == blo) {
+            if (c.crank == 0) {
+                const int wpc = blockDim.x >> 5;
+                for (int k = 0; k < SOLO_LEVELS; ++k) {
+                    MF_TRACE(11, level);
+                    on_level(level, pflo, flo, pblo, blo, threadIdx.x, blockDim.x);
+                    td_level(c, Q, bank, flo, fhi, blo, bhi, level, cl, c.warp, wpc);
+                    __syncthreads();
+                    const int ft = ldcg(&c.st.cnt[bank]), bt = ldcg(&c.st.cnt[CNT_BACK + bank]);
+                    __syncthreads();
+                    pflo = flo;
+                    pblo = blo;
+                    flo = fhi;
+                    fhi = ft;
+                    blo = bhi;
+                    bhi = bt;
+                    ++level;
+                    const long long fs = (long long)(fhi - flo) + (bhi - blo);
+                    const long long vis = (long long)fhi + bhi;
+                    if (fs == 0 || fs > SOLO_MAX || bhi != blo || (nu > vis && fs * 14 > nu - vis && fs * 64 > nu))
+                        break;
+                }
+                if (threadIdx.x == 0) {
+                    int *o = c.st.cnt + CNT_SOLO;
+                    o[0] = flo;
+                    o[1] = fhi;
+                    o[2] = blo;
+                    o[3] = bhi;
+                    o[4] = level;
+                    o[5] = pflo;
+                    o[6] = pblo;
+                }
+            }
+            if (!c.sync()) return false;
+            const int *o = c.st.cnt + CNT_SOLO;
+            nsolo += ldcg(&o[4]) - level;
+            flo = ldcg(&o[0]);
+            fhi = ldcg(&o[1]);
+            blo = ldcg(&o[2]);
+            bhi = ldcg(&o[3]);
+            level = ldcg(&o[4]);
+            pflo = ldcg(&o[5]);
+            pblo = ldcg(&o[6]);
+            continue;
+        }
         MF_TRACE(10, level);
-        on_level(level);
-        long long fsize = (long long)(fhi - flo) + (bhi - blo);
-        if (nu > visited && fsize * 14 > nu - visited)
+        on_level(level, pflo, flo, pblo, blo, gt, gT);
+        if (bottom_up) {
             bu_level(c, Q, bank, level, nuf, uf, nub, ub, par, set);
-        else
-            td_level(c, Q, bank, flo, fhi, blo, bhi, level, cl);
+            ++nbu;
+        } else
+            td_level(c, Q, bank, flo, fhi, blo, bhi, level, cl, c.gw, c.gW);
         int ft = 0, bt = 0;
         if (!c.sync_tails(bank, ft, bt)) return false;
-        visited += (long long)(ft - fhi) + (bt - bhi);
+        pflo = flo;
+        pblo = blo;
         flo = fhi;
         fhi = ft;
         blo = bhi;
         bhi = bt;
         ++level;
+    }
+    if (levels_out) *levels_out = level;
+    if (c.leader) {
+        i64 *tot = c.st.acc + ACC_TOT;
+        tot[T_LEVELS] += level;
+        tot[T_BU] += nbu;
+        tot[T_SOLO] += nsolo;
     }
     return true;
 }
@@ -727,14 +817,15 @@ __device__ bool preflow(QCtx &c, int s) {
 // BFS of the global relabel (direction-optimizing, exact levels) over the
 // slot's bitmaps: `vis` (visited, pre-set for dropped vertices and the
 // blocked vertex) and three frontier maps used in rotation (level L reads
-// map L % 3, fills map (L+1) % 3 and clears map (L+2) % 3).  The bitmaps
+// map L % 3, fills map (L+1) % 3 and takes the previous frontier's bits out
+// of map (L-1) % 3, which level L+1 fills next).  The bitmaps
 // (n/8 bytes each) stay in L2 while the per-vertex arrays do not, so the
 // visited and frontier tests per examined arc cost no DRAM sector.
 // Top-down: frontier vertex v claims an unvisited w with residual w->v
 // (atomicOr on the visited word).  Bottom-up: an unvisited kept vertex w
 // takes level + 1 when one of its residual arcs reaches the frontier map.
 // Claims write the height and the next frontier bit.
-__device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi) {
+__device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &depth) {
     const int W = bitmap_words(c.n);
     unsigned *vis = c.st.bits + W, *F = c.st.bits + 2 * W;
     const int *rev = c.rev;
@@ -771,12 +862,22 @@ __device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi) {
         atomicOr(&fmap(level + 1)[w >> 5], bit);
         return true;
     };
-    auto clear_next = [&](int level) {
-        unsigned *z = fmap(level + 2);
-        int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
-        for (int wd = gt; wd < W; wd += gT) z[wd] = 0;
+    // at level L the previous frontier's bits leave map (L - 1) % 3, which
+    // level L + 1 fills again (cost: the frontier's size, not n)
+    const int *Q = c.st.qa;
+    auto clear_prev = [&](int level, int plo, int phi, int pblo, int pbhi, int tid, int nth) {
+        if (level == 0) return;
+        unsigned *z = fmap(level - 1);
+        for (int i = plo + tid; i < phi; i += nth) {
+            int v = ldcg(&Q[i]);
+            atomicAnd(&z[v >> 5], ~(1u << (v & 31)));
+        }
+        for (int k = pblo + tid; k < pbhi; k += nth) {
+            int v = back_at(c, Q, k);
+            atomicAnd(&z[v >> 5], ~(1u << (v & 31)));
+        }
     };
-    return bfs_dir(c, c.st.qa, bank, fhi, bhi, relab, c.vf, uf, nv - c.vf, ub, par, set, clear_next);
+    return bfs_dir(c, c.st.qa, bank, fhi, bhi, relab, c.vf, uf, nv - c.vf, ub, par, set, clear_prev, &depth);
 }
 
 // Kept-vertex bitmap of the query (bit v: mark[v] >= M), read by every
@@ -802,7 +903,7 @@ __device__ bool build_kept_bits(QCtx &c, unsigned M) {
 // Returns counts in naf / nab (active front / back) and nd (deficits).
 __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int blockv, int srcv,
                                bool deficit_seeds, int *L, int lbk, int &naf, int &nab, int &nd,
-                               i64 *&ab) {
+                               i64 *&ab, int &depth) {
     MF_TRACE(40, nv);
     int qbk = c.take_bank();
     const int n = c.n;
@@ -843,7 +944,7 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
     int f0 = 0, b0 = 0;
     if (!c.sync_tails(qbk, f0, b0)) return false;
     MF_TRACE(43, f0 + b0);
-    if (!relabel_bfs(c, nv, qbk, f0, b0)) return false;
+    if (!relabel_bfs(c, nv, qbk, f0, b0, depth)) return false;
     int *h = c.st.h;
 
     // sweep: heights of unreached vertices, active list, counts
@@ -1417,6 +1518,7 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
     int pp_stable = 0, p_count = 64, pp_iter = 0;
     i64 round = 0;
     i64 mask_arcs = ldcg(&c.st.acc[ACC_TOT + T_MASKARCS]);
+    int gr_depth = 0;  // levels of the last global relabel's search
     for (;;) {
         int sinkv = (phase == PH_A) ? t : (phase == PH_B ? -1 : s);
         int blockv = (phase == PH_C) ? t : s;
@@ -1427,8 +1529,13 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
         int lbk = c.take_bank();
         u64 t0 = globaltimer_ns();
         i64 a0 = c.w_arcs;
-        if (!global_relabel(c, nv, M, sinkv, blockv, s, defseeds, L, lbk, naf, nab, nd, ab)) return false;
+        if (!global_relabel(c, nv, M, sinkv, blockv, s, defseeds, L, lbk, naf, nab, nd, ab, gr_depth)) return false;
         c.tm_relabel += globaltimer_ns() - t0;
+        if (c.leader) {
+            u64 t1 = globaltimer_ns();
+            c.st.acc[ACC_GR_DUR] = (i64)(t1 - t0);
+            c.st.acc[ACC_GR_END] = (i64)t1;
+        }
         if (c.lane == 0 && c.w_arcs > a0) atomic_add_i64(&c.st.acc[ACC_TOT + T_RARCS], c.w_arcs - a0);
         qo.relabels++;
         if (naf + nab == 0) {
@@ -1525,6 +1632,7 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
                 }
             }
             MF_TRACE(46, (int)round);
+            if (c.leader) rb[A_TIME] = (i64)globaltimer_ns();
             int nNf = 0, nNb = 0;
             if (!c.sync_tails(nbk, nNf, nNb)) return false;
             MF_TRACE(47, (int)round);
@@ -1595,8 +1703,22 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
             N = tmp;
             naf = nNf;
             nab = nNb;
-            bool gr_due = force_gr || rounds_since >= gr_freq ||
-                          (o.gr_alpha > 0.0 && (double)work_since >= o.gr_alpha * (double)mask_arcs);
+            // relabel when forced (stagnation, deficits), after alpha x kept
+            // arcs of scanning, or after gr_freq rounds.  After a deep relabel
+            // (more than DEEP_LEVELS levels: long thin residual paths, where
+            // each level is a barrier and the rounds that move excess along
+            // the path are quick) none of these fires before the rounds have
+            // taken as long as that relabel, or the solve would spend far
+            // more time searching than pushing; the relabel that ends a phase
+            // (no active vertex left) is never held.  gr_freq = 1 asks for a
+            // relabel after every round.  The times are the leader's,
+            // published before barriers, so every thread decides alike.
+            const i64 since_gr = ldcg(&rb[A_TIME]) - ldcg(&c.st.acc[ACC_GR_END]);
+            const bool deep_hold = o.gr_freq > 1 && gr_depth > DEEP_LEVELS &&
+                                   since_gr < ldcg(&c.st.acc[ACC_GR_DUR]);
+            bool gr_due = !deep_hold &&
+                          (force_gr || rounds_since >= gr_freq ||
+                           (o.gr_alpha > 0.0 && (double)work_since >= o.gr_alpha * (double)mask_arcs));
             if (gr_due) break;
         }
         c.tm_rounds += globaltimer_ns() - tr0;
@@ -1835,7 +1957,7 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
             c.st.acc[b * ACC_BANK + A_HMIN] = INT_MAX;
             c.st.acc[b * ACC_BANK + A_HMAX] = -1;
         }
-        for (int i = 0; i < 8; ++i) c.st.acc[ACC_TOT + i] = 0;
+        for (int i = 0; i < 16; ++i) c.st.acc[ACC_TOT + i] = 0;
     }
     c.seq = 0;
     c.aseq = 0;
@@ -1943,7 +2065,8 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
             int naf = 0, nab = 0, nd = 0;
             i64 *ab = nullptr;
             int lbk = c.take_bank();
-            if (!global_relabel(c, nv, M, t, s, s, true, c.st.qb, lbk, naf, nab, nd, ab)) return;
+            int depth = 0;
+            if (!global_relabel(c, nv, M, t, s, s, true, c.st.qb, lbk, naf, nab, nd, ab, depth)) return;
             int *hd = (int *)p.dbg;
             int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
             for (int v = gt; v < c.n; v += gT)
@@ -1994,6 +2117,9 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
         qo.arcs_hubs = tot[T_HARCS];
         qo.hub_passes = tot[T_HPASS];
         qo.hub_relabels = tot[T_HREL];
+        qo.levels = tot[T_LEVELS];
+        qo.levels_bottom_up = tot[T_BU];
+        qo.levels_solo = tot[T_SOLO];
         p.out[q] = qo;
         c.st.meta[0] = (int)M;
         c.st.meta[1] = nv;

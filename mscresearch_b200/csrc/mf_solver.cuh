@@ -49,6 +49,9 @@ struct HubWork {
 
 // Working state of one residual slot.  All arrays are full-size for the
 // graph the slot serves; stamps make resets unnecessary between queries.
+// Control words per slot (list tails, query hand-off, search state).
+#define CNT_WORDS 64
+
 struct DSlot {
     i64 *res;          // arcs: residual capacity
     i64 *ex;           // n: excess
@@ -61,7 +64,7 @@ struct DSlot {
     int *qb;           // n: worklist
     int *hot;          // 1024: region counts / hot flags
     int *ract;         // 1024: active-region flags
-    int *cnt;          // 32 ints: rotating list tails (front, back) + control words
+    int *cnt;          // CNT_WORDS ints: rotating list tails (front, back) + control words
     i64 *acc;          // 64 i64: rotating round accumulators + query totals
     GroupBar *bar;     // group barrier
     unsigned *clock;   // persistent stamp clock
@@ -118,6 +121,9 @@ struct QOut {
     i64 arcs_hubs;    // arc examinations by the chunked hub discharge
     i64 hub_passes;   // hub discharge passes (a hub with excess, all its chunks)
     i64 hub_relabels; // passes that ended with excess left (the hub was relabeled)
+    i64 levels;           // search levels (prune, relabels, certificate)
+    i64 levels_bottom_up; // of which bottom-up
+    i64 levels_solo;      // of which run by one CTA
     int mask_n;
     int status;
     int kept_front;  // kept vertices in vlist's front part
