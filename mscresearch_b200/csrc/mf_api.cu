@@ -180,19 +180,32 @@ __global__ void k_reset_slot(DSlot s, int n) {
     if (blockIdx.x == 0 && threadIdx.x == 0) *s.clock = 0;
 }
 
-// Capacity updates: resolve (u,v) to the first forward arc u->v.
+// Capacity updates: resolve (u,v) to the first forward arc u->v (lowest
+// index in u's list).  The shorter of the two lists is scanned: in v's list
+// every reverse arc v->u (fwd = 0) is paired with a forward arc u->v, found
+// through rev, so a hub tail (a super source, an R-MAT hub) does not cost
+// its whole list per update.
 __global__ void k_find_arcs(int nb, const int *u, const int *v, const int *row, const int *col,
-                            const unsigned char *fwd, const i64 *cap, int *arc, i64 *capv) {
+                            const int *rev, const unsigned char *fwd, const i64 *cap, int *arc,
+                            i64 *capv) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nb) return;
     int a = -1;
     int x = u[i], y = v[i];
     if (x >= 0 && y >= 0) {
-        for (int e = row[x]; e < row[x + 1]; ++e)
-            if (col[e] == y && fwd[e]) {
-                a = e;
-                break;
-            }
+        if (row[y + 1] - row[y] < row[x + 1] - row[x]) {
+            for (int e = row[y]; e < row[y + 1]; ++e)
+                if (col[e] == x && !fwd[e]) {
+                    int f = rev[e];
+                    if (a < 0 || f < a) a = f;
+                }
+        } else {
+            for (int e = row[x]; e < row[x + 1]; ++e)
+                if (col[e] == y && fwd[e]) {
+                    a = e;
+                    break;
+                }
+        }
     }
     arc[i] = a;
     capv[i] = (a >= 0) ? cap[a] : 0;
@@ -1054,7 +1067,7 @@ static int resolve_updates(mf_graph *g, int nb, const int32_t *u, const int32_t 
     CK(cudaMalloc(&dcap, sizeof(i64) * nb));
     CK(cudaMemcpy(du, ui.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(dv, vi.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
-    k_find_arcs<<<(nb + 255) / 256, 256, 0, g->stream>>>(nb, du, dv, g->row, g->col, g->fwd, g->cap, darc, dcap);
+    k_find_arcs<<<(nb + 255) / 256, 256, 0, g->stream>>>(nb, du, dv, g->row, g->col, g->rev, g->fwd, g->cap, darc, dcap);
     std::vector<int> arc(nb);
     std::vector<i64> capv(nb);
     CK(cudaMemcpyAsync(arc.data(), darc, sizeof(int) * nb, cudaMemcpyDeviceToHost, g->stream));

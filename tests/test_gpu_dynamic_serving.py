@@ -59,6 +59,33 @@ def test_session_incremental_equals_fresh(scale):
         ss.close()
 
 
+def test_update_caps_hub_tail_parallel_arcs():
+    """Updates on (hub, leaf) pairs are resolved through the leaf's shorter
+    list; with parallel edges the first forward arc in input order must take
+    the change (same rule as the oracle)."""
+    n = 64
+    u = list(range(1, 60)) + [7, 0, 0, 7, 3]
+    v = [0] * 59 + [0, 7, 7, 3, 0]
+    c = list(range(1, 60)) + [4, 5, 9, 2, 8]
+    # vertex 0 gets 59 in-arcs + parallel out-arcs 0->7 (caps 5, 9); 7 and 3 are short lists
+    u, v, c = np.array(u, np.int32), np.array(v, np.int32), np.array(c, np.int64)
+    u = np.concatenate([u, np.zeros(40, np.int32)])
+    v = np.concatenate([v, np.arange(20, 60, dtype=np.int32)])
+    c = np.concatenate([c, np.full(40, 3, np.int64)])
+    g = O.build_csr(n, u, v, c)
+    fwd = g.cap > 0
+    with mf.Graph.from_edges(n, u, v, c, R=4) as eg:
+        uu = np.array([0, 7, 0, 3, 30], np.int32)
+        vv = np.array([7, 0, 7, 0, 0], np.int32)
+        d = np.array([100, -3, -50, 7, 2], np.int64)
+        eg.update_caps(uu, vv, d)
+        apply_updates_oracle(g, fwd, uu, vv, d)
+        ex = eg.export()
+        assert np.array_equal(np.sort(ex["cap"]), np.sort(g.cap))
+        for a, b in [(0, 7), (7, 0), (30, 7), (3, 7)]:
+            assert eg.solve(a, b)[0] == O.dinic(g, a, b), (a, b)
+
+
 def test_update_caps_then_fresh_solve():
     n = 2000
     u, v, c = mf.gen_uniform(n, 12000, 1, 50, seed=2)
