@@ -237,6 +237,19 @@ def run_engine(args):
     served = None
     if args.serve:
         served = serve_run(mf, g, s, t, flows, o, rate=0.6 * nq / (step_ms / 1e3))
+    # ---- every answer certified on the device, outside the timed region:
+    # excess returned to s (zero-excess flow), residuals non-negative and
+    # pair-conserved, s-t cut capacity equal to the flow
+    certified = None
+    if not args.no_certify:
+        oc = type(o).from_buffer_copy(o)
+        oc.certify = 1
+        try:
+            cfl, cst = g.solve_batch(s, t, oc, with_stats=True)
+            ok = sum(1 for f, st in zip(cfl, cst) if st.status == 0 and st.cut_capacity == f)
+            certified = {"queries": nq, "certified": ok, "flows_equal_timed": bool(list(cfl) == list(flows))}
+        except mf.MaxflowError as e:
+            certified = {"queries": nq, "certified": None, "error": str(e)}
     # roofline: algorithmic bytes = 16 B x (arc + vertex examinations)
     ax = sum(x.arcs_examined for x in stats_last)
     vx = sum(x.vertices_examined for x in stats_last)
@@ -287,10 +300,13 @@ def run_engine(args):
     }
     if served:
         res["served"] = served
+    if certified:
+        res["certified"] = certified
     if rank == 0 and world == 1 and not args.no_cpu:
         cb, idx, cflows = cpu_baseline(n, u, v, c, s, t, budget_s=args.cpu_budget)
         assert [int(flows[i]) for i in idx] == [int(x) for x in cflows], "engine differs from oracle"
         res["cpu_baseline"] = cb
+        res["oracle_agreement"] = "%d of %d sampled answers equal to the oracle's Dinic" % (len(idx), len(idx))
     if rank == 0:
         print(json.dumps(res), flush=True)
     if args.dump and rank == 0:
@@ -413,6 +429,7 @@ def main():
     ap.add_argument("--ref-queries-per-step", type=int, default=2)
     ap.add_argument("--ref-timeout", type=int, default=900)
     ap.add_argument("--check", action="store_true")
+    ap.add_argument("--no-certify", action="store_true", help="skip the untimed certification pass")
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--nhub", type=int, default=NHUB)
     ap.add_argument("--nuni", type=int, default=NUNI)

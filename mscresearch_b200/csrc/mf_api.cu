@@ -933,6 +933,9 @@ static int solve_common(mf_graph *g, int nq, const int32_t *s, const int32_t *t,
     mf_opts o;
     if (opts) o = *opts;
     else mf_opts_default(&o);
+    // opts.certify: every answer also returns its excess to s and is checked
+    // on the device (zero-excess flow, equal-capacity s-t cut)
+    if (o.certify && mode == KM_SOLVE) mode = KM_CERTIFY;
     std::vector<int> si(nq), ti(nq);
     for (int i = 0; i < nq; ++i) to_internal(g, s[i], t[i], si[i], ti[i]);
     int rc0 = ensure_kept_cache(g, o);
@@ -941,7 +944,7 @@ static int solve_common(mf_graph *g, int nq, const int32_t *s, const int32_t *t,
     int G = single ? 0 : (o.group_ctas > 0 ? o.group_ctas : 8);
     // batched: queue order by expected cost (largest first), results unpermuted
     std::vector<int> perm;
-    if (!single && o.schedule && nq > 1 && mode == KM_SOLVE) {
+    if (!single && o.schedule && nq > 1 && (mode == KM_SOLVE || mode == KM_CERTIFY)) {
         perm = cost_order(g, nq, si.data(), ti.data(), o);
         std::vector<int> s2(nq), t2(nq);
         for (int i = 0; i < nq; ++i) {

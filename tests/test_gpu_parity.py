@@ -151,6 +151,17 @@ def test_device_certificate(rmat14):
         assert st.status == 0 and st.cut_capacity == f == O.dinic(g, a, b)
 
 
+def test_batch_certify_option(rmat14):
+    """opts.certify = 1 on a batched solve: every answer comes back certified
+    on the device (zero-excess flow, s-t cut of equal capacity)."""
+    n, u, v, c, g, s, t, eg = rmat14
+    exp = oracle_flows(g, s, t)
+    flows, sts = eg.solve_batch(s, t, mf.opts(certify=1), with_stats=True)
+    assert list(flows) == exp
+    for f, st in zip(flows, sts):
+        assert st.status == 0 and st.cut_capacity == f
+
+
 @pytest.mark.parametrize("kw", [
     dict(use_rm=1, force_rm=1, rm_freq=1),
     dict(use_path_push=1, force_path_push=1, path_push_switch=1 << 30),
