@@ -159,3 +159,24 @@ def test_autotune_consistent():
         assert R in (32, 64, 128, 256, 512)
         assert eg.info[2] == R
         assert list(eg.solve_batch(s, t, best)) == exp
+
+
+def test_full_size_dynamic_properties():
+    """R-MAT n = 2^22 with 2^26 draws (the dynamic-serving shape): after a
+    batch of 10k seeded +-U[1,100] capacity changes the session's
+    incrementally repaired answers equal fresh solves, and one is certified."""
+    u, v, c = mf.gen_rmat(22, 1 << 26, seed=5)
+    n = 1 << 22
+    s, t = mf.gen_queries_hub(n, u, v, 4, 4, seed=6)
+    rng = np.random.default_rng(7)
+    with mf.Graph.from_edges(n, u, v, c, R=128) as eg:
+        ss = mf.Session(eg, s, t)
+        f0 = ss.solve()
+        assert list(f0) == list(eg.solve_batch(s, t))
+        idx = rng.integers(0, len(u), 10000)
+        d = rng.integers(1, 101, 10000) * rng.choice([-1, 1], 10000)
+        f1 = ss.update(u[idx], v[idx], d)
+        assert list(f1) == list(eg.solve_batch(s, t))
+        fc, stc = eg.certify(s[0], t[0])
+        assert fc == f1[0] and stc.cut_capacity == fc and stc.status == 0
+        ss.close()

@@ -226,3 +226,21 @@ def test_full_size_rmat20_properties():
             assert f == fb[i]
             fc, stc = eg.certify(s[i], t[i])
             assert fc == f and stc.cut_capacity == f and stc.status == 0
+
+
+def test_full_size_grid_properties():
+    """2048 x 2048 grid with super terminals (segmentation shape, 4.2 M
+    vertices): the s->t flow is device-certified, and batched == plain for it
+    and for pixel pairs (deep, ~3000-level searches)."""
+    W = 2048
+    u, v, c = mf.gen_grid(W, W, seed=9)
+    n = W * W + 2
+    S, T = W * W, W * W + 1
+    rng = np.random.default_rng(3)
+    s = [S] + list(rng.integers(0, W * W, 3))
+    t = [T] + list(rng.integers(0, W * W, 3))
+    with mf.Graph.from_edges(n, u, v, c, R=128) as eg:
+        fb = eg.solve_batch(s, t)
+        assert [eg.solve(a, b)[0] for a, b in zip(s, t)] == list(fb)
+        fc, stc = eg.certify(S, T)
+        assert fc == fb[0] and stc.cut_capacity == fc and stc.status == 0
