@@ -10,6 +10,7 @@
 // equal scores are ordered by increasing vertex id (the reference's
 // std::sort leaves their order unspecified).
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 #include "mf_build.cuh"
@@ -142,49 +143,47 @@ __global__ void k_bitonic_shared(int k, int jstart, u64 *key, int *id) {
     }
 }
 
-// Greedy least-loaded packing (RA:1168-1177) with one warp: region loads
-// live in shared memory, lane j owns regions j, j+32, ...; each lane caches
-// the (load, region) minimum of its own regions, a 5-step shuffle reduction
-// picks the global minimum (lowest region on ties), and only the winning
-// lane refreshes its cache.
-__global__ void k_lpt(int n, int R, const u64 *key, const int *id, int *part) {
-    extern __shared__ double load[];
-    int lane = threadIdx.x;
-    for (int r = lane; r < R; r += 32) load[r] = 0.0;
-    __syncwarp();
-    double lmin = 1e308;
-    int lidx = 0x7fffffff;
-    for (int r = lane; r < R; r += 32)
-        if (load[r] < lmin) {
-            lmin = load[r];
-            lidx = r;
-        }
+// Greedy least-loaded packing (RA:1168-1177): vertices in decreasing score
+// order (the device sort's order) each go to the region with the least load,
+// the lowest region on ties.  Every choice depends on all earlier ones, so
+// the step is a single dependency chain; it runs on the host with a binary
+// heap over (load, region), O(n log R), instead of serialising one GPU warp
+// through n shuffle reductions.  Loads add in IEEE double round-to-nearest,
+// exactly as the oracle does, so the packing is bit-identical.
+static cudaError_t host_lpt(int n, int R, const u64 *d_key, const int *d_id, int *d_part, cudaStream_t st) {
+    std::vector<u64> key((size_t)n);
+    std::vector<int> id((size_t)n), part((size_t)n);
+    cudaError_t e = cudaMemcpyAsync(key.data(), d_key, sizeof(u64) * (size_t)n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(id.data(), d_id, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    std::vector<double> load((size_t)R, 0.0);
+    std::vector<int> heap((size_t)R);
+    for (int r = 0; r < R; ++r) heap[r] = r;  // equal loads: index order is a heap
+    auto less = [&](int x, int y) { return load[x] < load[y] || (load[x] == load[y] && x < y); };
     for (int i = 0; i < n; ++i) {
-        double v = lmin;
-        int ix = lidx;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            double v2 = __shfl_xor_sync(MF_FULL, v, o);
-            int i2 = __shfl_xor_sync(MF_FULL, ix, o);
-            if (v2 < v || (v2 == v && i2 < ix)) {
-                v = v2;
-                ix = i2;
-            }
+        const int r = heap[0];
+        u64 bits = ~key[i];
+        double w;
+        memcpy(&w, &bits, sizeof w);
+        part[id[i]] = r;
+        load[r] = load[r] + w;
+        // sift the grown root down
+        int k = 0;
+        for (;;) {
+            int c = 2 * k + 1;
+            if (c >= R) break;
+            if (c + 1 < R && less(heap[c + 1], heap[c])) ++c;
+            if (!less(heap[c], heap[k])) break;
+            int tmp = heap[c];
+            heap[c] = heap[k];
+            heap[k] = tmp;
+            k = c;
         }
-        double s = __longlong_as_double((long long)~key[i]);
-        if (lane == 0) part[id[i]] = ix;
-        if ((ix & 31) == lane) {
-            load[ix] = MF_DADD(load[ix], s);
-            lmin = 1e308;
-            lidx = 0x7fffffff;
-            for (int r = lane; r < R; r += 32)
-                if (load[r] < lmin) {
-                    lmin = load[r];
-                    lidx = r;
-                }
-        }
-        __syncwarp();
     }
+    e = cudaMemcpyAsync(d_part, part.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e;
 }
 
 #define CHUNK 4096
@@ -452,7 +451,10 @@ cudaError_t mf_partition_reorder(const BuildIn &in, const BuildOut &out, void *s
         for (; j >= 1024; j >>= 1) k_bitonic_global<<<grid_for(P, 256), 256, 0, st>>>(P, k, j, key, id);
         k_bitonic_shared<<<P / 2048, 1024, 0, st>>>(k, j, key, id);
     }
-    k_lpt<<<1, 32, sizeof(double) * R, st>>>(n, R, key, id, out.part);
+    {
+        cudaError_t e = host_lpt(n, R, key, id, out.part, st);
+        if (e != cudaSuccess) return e;
+    }
     cudaFuncSetAttribute(k_chunk_place, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(sizeof(int) * CHUNK_WARPS * 1024));
     k_chunk_counts<<<nchunks, 512, sizeof(int) * R, st>>>(n, R, out.part, ccount);
