@@ -466,6 +466,11 @@ KOpts resolve_opts(const mf_opts &o, int avg_deg) {
     k.force_rm = o.force_rm;
     k.force_pp = o.force_path_push;
     k.use_cache = o.use_kept_cache;
+    // bottom-up once the frontier exceeds 1/56 of the unvisited vertices
+    // (measured on the B200: 1/14, the usual edge-count rule, kept hub-heavy
+    // early levels top-down; MF_BU_FACTOR overrides it for tuning)
+    k.bu_factor = 56;
+    if (const char *e = getenv("MF_BU_FACTOR")) k.bu_factor = std::max(1, atoi(e));
     k.iter_max = o.iter_max > 0 ? o.iter_max : 20000000;
     return k;
 }

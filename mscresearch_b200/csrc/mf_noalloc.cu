@@ -169,7 +169,8 @@ extern "C" int mf_solve_csr_noalloc(int n, long long arcs, const int32_t *d_row,
         return MF_ERR_CUDA;
     }
 
-    KOpts k;
+    KOpts k{};
+    k.bu_factor = 56;
     int avg = (int)(arcs / n);
     k.K = o.kernel_cycles > 0 ? o.kernel_cycles : (avg > 4 ? avg : 4);
     k.gr_freq = o.gr_freq > 0 ? o.gr_freq : 1;

@@ -123,6 +123,7 @@ struct QCtx {
     u64 tm_relabel, tm_rounds;  // leader: accumulated phase times
     // per-warp counters (flushed at the end of the query)
     i64 w_arcs, w_verts, w_push;
+    int bu_factor;  // direction switch of the searches (KOpts::bu_factor)
 
     __device__ bool sync() { return gsync(G, bar, err, lim); }
     // barrier that also returns the front and back tails of list bank `bank`
@@ -375,8 +376,8 @@ static_assert(CNT_SOLO >= CNT_BACK + NBANKS && CNT_SOLO > CNT_HUBCH && CNT_SOLO 
               "solo state must not overlap the other control words");
 
 // Direction-optimizing BFS: a level runs bottom-up when the frontier holds
-// more than a 1/14 share of the unvisited universe (nu - visited) and at
-// least 1/64 of the universe, top-down otherwise.  Both directions append
+// more than a 1/bu_factor share of the unvisited universe (nu - visited)
+// and at least 1/64 of the universe, top-down otherwise.  Both directions append
 // the newly visited vertices to Q, so the next level can run either way,
 // and visited = the queue's length.
 // Small top-down frontiers run "solo": the group's first CTA expands them
@@ -399,7 +400,7 @@ __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, i
         // bottom-up sweeps the whole universe, so the frontier must also be a
         // sizeable share of it (a small frontier near the end of a deep
         // search is cheaper to expand than nu candidates are to check)
-        const bool bottom_up = nu > visited && fsize * 14 > nu - visited && fsize * 64 > nu;
+        const bool bottom_up = nu > visited && fsize * c.bu_factor > nu - visited && fsize * 64 > nu;
         if (!bottom_up && c.G > 1 && fsize <= SOLO_MAX && bhi == blo) {
             if (c.crank == 0) {
                 const int wpc = blockDim.x >> 5;
@@ -419,7 +420,7 @@ __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, i
                     ++level;
                     const long long fs = (long long)(fhi - flo) + (bhi - blo);
                     const long long vis = (long long)fhi + bhi;
-                    if (fs == 0 || fs > SOLO_MAX || bhi != blo || (nu > vis && fs * 14 > nu - vis && fs * 64 > nu))
+                    if (fs == 0 || fs > SOLO_MAX || bhi != blo || (nu > vis && fs * c.bu_factor > nu - vis && fs * 64 > nu))
                         break;
                 }
                 if (threadIdx.x == 0) {
@@ -2142,6 +2143,7 @@ __global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
     c.lane = threadIdx.x & 31;
     c.err = p.err;
     c.lim = p.bar_limit_ns;
+    c.bu_factor = p.o.bu_factor;
     c.leader = (c.crank == 0 && threadIdx.x == 0);
     c.w_arcs = c.w_verts = c.w_push = 0;
     c.t_start = globaltimer_ns();

@@ -95,6 +95,7 @@ struct KOpts {
     int force_rm;
     int force_pp;
     int use_cache;
+    int bu_factor;  // bottom-up when frontier x bu_factor > unvisited (and >= 1/64 of all)
     i64 iter_max;
 };
 
