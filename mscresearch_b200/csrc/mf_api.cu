@@ -682,7 +682,7 @@ void mf_opts_default(mf_opts *o) {
     memset(o, 0, sizeof(*o));
     o->kernel_cycles = 0;
     o->gr_freq = 16;         // RA:1466 starts at 128; exact relabels are cheap here
-    o->gr_work_alpha = 0.5;  // also relabel after ~half a pass over the kept arcs
+    o->gr_work_alpha = 0.35; // also relabel after ~a third of a pass over the kept arcs
     o->prune_mode = 1;
     o->path_push_switch = 8;  // PATH_PUSH_SWITCH (RA:1480)
     o->max_path_len = 256;    // MAX_PATH_LENGTH (RA:1481)

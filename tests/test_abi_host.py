@@ -35,7 +35,7 @@ def test_opts_defaults_match_reference_knobs():
     o = mf.opts()
     # RA:1466 starts GR_FREQ at 128; this engine's exact relabels are cheap
     # (direction-optimizing BFS), so it relabels every 16 rounds at most
-    assert (o.gr_freq, o.gr_work_alpha) == (16, 0.5)
+    assert (o.gr_freq, o.gr_work_alpha) == (16, 0.35)
     assert (o.rm_freq, o.h_cut, o.stagnate_rounds) == (64, 100, 128)
     assert (o.path_push_switch, o.max_path_len, o.hot_regions) == (8, 256, 32)
     assert o.iter_max == 20000000
