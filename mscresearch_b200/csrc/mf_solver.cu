@@ -1222,62 +1222,80 @@ __device__ void discharge_hubs(QCtx &c, const int *L, int nb, int sinkv, int blo
         }
         int k = lo;
         int cs = ldcg(&c.st.hubw[k].cstart), nch = ldcg(&c.st.hubw[k].nch);
-        for (int j = j0; j < j1; ++j) {
+        int j = j0;
+        while (j < j1) {
             while (j >= cs + nch && k + 1 < nb) {
                 ++k;
                 cs = ldcg(&c.st.hubw[k].cstart);
                 nch = ldcg(&c.st.hubw[k].nch);
             }
             if (j >= cs + nch) break;
+            // this warp's run of hub k's chunks, [j, jend): the excess taken,
+            // the lowest height left and the chunks done are flushed once
+            // per run rather than once per chunk
+            const int jbeg = j, jend = min(j1, cs + nch);
             HubWork *hw = &c.st.hubw[k];
-            int v = back_at(c, L, k);
-            int hv = ldcg(&hw->hv);
-            int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
-            int ch = j - cs;
-            int e = b + ch * 32 + c.lane;
-            // Once the hub's budget is spent the pass cannot end in a relabel
-            // (budget only falls), so the chunk's scan would serve nothing:
-            // only its completion is recorded.
-            i64 bud = 0;
-            if (c.lane == 0) bud = ldcg(&hw->budget);
-            bud = __shfl_sync(MF_FULL, bud, 0);
-            if (bud <= 0) e = e1;
-            i64 r = 0;
-            int w = 0, hwt = MF_INF_H;
-            if (e < e1) {
-                r = ldcg(&c.st.res[e]);
-                w = ldro(&c.col[e]);
-                if (r > 0) hwt = ldcg(&c.st.h[w]);
-            }
-            bool adm = r > 0 && hwt < hv;
-            i64 x = adm ? r : 0;
-            i64 incl = warp_incl_scan_i64(x);
-            i64 tot = __shfl_sync(MF_FULL, incl, 31);
-            i64 take = 0;
-            if (tot > 0) {
-                if (c.lane == 0) {
-                    i64 old = atomic_add_i64(&hw->budget, -tot);
-                    take = old >= tot ? tot : (old > 0 ? old : 0);
+            const int v = back_at(c, L, k);
+            const int hv = ldcg(&hw->hv);
+            const int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+            i64 take_sum = 0;
+            int run_minh = MF_INF_H;
+            for (; j < jend; ++j) {
+                const int cb = b + (j - cs) * 32;
+                // Once the hub's budget is spent the pass cannot end in a
+                // relabel (budget only falls), so the rest of the run serves
+                // nothing: its chunks are only counted as done.
+                i64 bud = 0;
+                if (c.lane == 0) bud = ldcg(&hw->budget);
+                bud = __shfl_sync(MF_FULL, bud, 0);
+                if (bud <= 0) {
+                    if (c.lane == 0) work += min(e1, b + (jend - cs) * 32) - cb;
+                    j = jend;
+                    break;
                 }
-                take = __shfl_sync(MF_FULL, take, 0);
+                const int e = cb + c.lane;
+                i64 r = 0;
+                int w = 0, hwt = MF_INF_H;
+                if (e < e1) {
+                    r = ldcg(&c.st.res[e]);
+                    w = ldro(&c.col[e]);
+                    if (r > 0) hwt = ldcg(&c.st.h[w]);
+                }
+                bool adm = r > 0 && hwt < hv;
+                i64 x = adm ? r : 0;
+                i64 incl = warp_incl_scan_i64(x);
+                i64 tot = __shfl_sync(MF_FULL, incl, 31);
+                i64 take = 0;
+                if (tot > 0) {
+                    if (c.lane == 0) {
+                        i64 old = atomic_add_i64(&hw->budget, -tot);
+                        take = old >= tot ? tot : (old > 0 ? old : 0);
+                    }
+                    take = __shfl_sync(MF_FULL, take, 0);
+                }
+                i64 dd = 0;
+                bool act = false;
+                if (adm && take > incl - x) dd = min(r, take - (incl - x));
+                if (dd > 0) act = push_arc(c, e, w, dd, sinkv, blockv);
+                if (act) act = enlist(c, w, rstamp);
+                append2(c, act, w, N, nbk);
+                if (r - dd > 0) run_minh = min(run_minh, hwt);
+                if (c.lane == 0) {
+                    const int chunk_arcs = min(32, e1 - cb);
+                    take_sum += take;
+                    arcs += chunk_arcs;
+                    work += chunk_arcs;
+                    c.w_push += take ? 1 : 0;
+                }
             }
-            i64 dd = 0;
-            bool act = false;
-            if (adm && take > incl - x) dd = min(r, take - (incl - x));
-            if (dd > 0) act = push_arc(c, e, w, dd, sinkv, blockv);
-            if (act) act = enlist(c, w, rstamp);
-            append2(c, act, w, N, nbk);
-            int mh = __reduce_min_sync(MF_FULL, (r - dd > 0) ? hwt : MF_INF_H);
+            const int mh = __reduce_min_sync(MF_FULL, run_minh);
             if (c.lane == 0) {
-                if (take) atomic_add_i64(&c.st.ex[v], -take);
+                if (take_sum) atomic_add_i64(&c.st.ex[v], -take_sum);
                 if (mh != MF_INF_H) atomicMin(&hw->minh, mh);
-                int chunk_arcs = min(32, ldro(&c.row[v + 1]) - (b + ch * 32));
-                work += chunk_arcs;
-                if (bud > 0) arcs += chunk_arcs;
-                c.w_push += take ? 1 : 0;
+                const int nrun = jend - jbeg;
                 __threadfence();
-                if (atomicAdd(&hw->done, 1) == nch - 1) {
-                    // last chunk of this hub: relabel if excess was left over
+                if (atomicAdd(&hw->done, nrun) + nrun == nch) {
+                    // last run of this hub: relabel if excess was left over
                     __threadfence();
                     i64 left = atomic_add_i64(&hw->budget, 0);
                     int hnew = hv;
