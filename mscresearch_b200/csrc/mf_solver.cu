@@ -1240,26 +1240,42 @@ __device__ void discharge_hubs(QCtx &c, const int *L, int nb, int sinkv, int blo
             const int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
             i64 take_sum = 0;
             int run_minh = MF_INF_H;
+            // the lane's residual and head are loaded one chunk ahead (a
+            // residual read early is never above the current one: only this
+            // warp lowers the residuals of its run's arcs)
+            i64 r_nx = 0;
+            int w_nx = 0;
+            {
+                const int e = b + (j - cs) * 32 + c.lane;
+                if (e < e1) {
+                    r_nx = ldcg(&c.st.res[e]);
+                    w_nx = ldro(&c.col[e]);
+                }
+            }
             for (; j < jend; ++j) {
                 const int cb = b + (j - cs) * 32;
+                const int e = cb + c.lane;
+                const i64 r = r_nx;
+                const int w = w_nx;
+                // budget, head heights and the next chunk's arcs in flight together
+                i64 bud = 0;
+                if (c.lane == 0) bud = ldcg(&hw->budget);
+                int hwt = MF_INF_H;
+                if (r > 0) hwt = ldcg(&c.st.h[w]);
+                if (j + 1 < jend && e + 32 < e1) {
+                    r_nx = ldcg(&c.st.res[e + 32]);
+                    w_nx = ldro(&c.col[e + 32]);
+                } else {
+                    r_nx = 0;  // no arc for this lane in the next chunk
+                }
                 // Once the hub's budget is spent the pass cannot end in a
                 // relabel (budget only falls), so the rest of the run serves
                 // nothing: its chunks are only counted as done.
-                i64 bud = 0;
-                if (c.lane == 0) bud = ldcg(&hw->budget);
                 bud = __shfl_sync(MF_FULL, bud, 0);
                 if (bud <= 0) {
                     if (c.lane == 0) work += min(e1, b + (jend - cs) * 32) - cb;
                     j = jend;
                     break;
-                }
-                const int e = cb + c.lane;
-                i64 r = 0;
-                int w = 0, hwt = MF_INF_H;
-                if (e < e1) {
-                    r = ldcg(&c.st.res[e]);
-                    w = ldro(&c.col[e]);
-                    if (r > 0) hwt = ldcg(&c.st.h[w]);
                 }
                 bool adm = r > 0 && hwt < hv;
                 i64 x = adm ? r : 0;
