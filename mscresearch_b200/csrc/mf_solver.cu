@@ -308,9 +308,12 @@ __device__ void td_level(QCtx &c, int *Q, int bank, int flo, int fhi, int blo, i
 // vertex of at most HUB_T arcs and ub(k), k < nub, a hub, or -1 when the
 // candidate is already visited.  par(w, e, x, level) tests whether arc
 // e = w->x links w to the search; set(w, level) claims w and returns true
-// (one lane calls it per candidate, so it may store without atomics).  Small
-// candidates are scanned by 8-lane tiles (four per warp step), hubs by whole
-// warps (one hub per warp); both stop at the first parent.
+// (one lane calls it per candidate, so it may store without atomics).  Each
+// lane first tests its own candidate's first BU_PRE arcs; the rest of a
+// small candidate's arcs are scanned by 8-lane tiles (four per warp step),
+// hubs by whole warps (one hub per warp); all stop at the first parent.
+#define BU_PRE 4  // arcs a bottom-up candidate tests on its own lane before the tiles
+
 template <class UF, class UB, class Par, class Set>
 __device__ void bu_level(QCtx &c, int *Q, int bank, int level, int nuf, UF uf, int nub, UB ub, Par par,
                          Set set) {
@@ -320,8 +323,25 @@ __device__ void bu_level(QCtx &c, int *Q, int bank, int level, int nuf, UF uf, i
     for (int base = c.gw * 32; base < nuf; base += c.gW * 32) {
         int i = base + c.lane;
         int w = i < nuf ? uf(i) : -1;
-        unsigned todo = __ballot_sync(MF_FULL, w >= 0);
         if (c.lane == 0) c.w_verts += min(32, nuf - base);
+        // lane pass: every lane tests its own candidate's first BU_PRE arcs
+        // (independent loads, 32 candidates at once); only candidates with
+        // more arcs and no parent among those go on to the 8-lane tiles
+        bool claimed1 = false, more = false;
+        if (w >= 0) {
+            const int b = ldro(&c.row[w]), e1 = ldro(&c.row[w + 1]);
+            bool hit = false;
+#pragma unroll
+            for (int k = 0; k < BU_PRE; ++k) {
+                const int e = b + k;
+                if (e < e1) hit |= par(w, e, ldro(&c.col[e]), level);
+            }
+            arcs += min(BU_PRE, e1 - b);
+            if (hit) claimed1 = set(w, level);
+            else more = e1 - b > BU_PRE;
+        }
+        append2(c, claimed1, w, Q, bank);
+        unsigned todo = __ballot_sync(MF_FULL, more);
         while (todo) {
             unsigned rest = todo;
             for (int k = 0; k < tile && rest; ++k) rest &= rest - 1;
@@ -330,7 +350,7 @@ __device__ void bu_level(QCtx &c, int *Q, int bank, int level, int nuf, UF uf, i
             for (int k = 0; k < 4 && todo; ++k) todo &= todo - 1;
             bool claimed = false;
             if (src >= 0) {
-                int b = ldro(&c.row[wt]), e1 = ldro(&c.row[wt + 1]);
+                int b = ldro(&c.row[wt]) + BU_PRE, e1 = ldro(&c.row[wt + 1]);
                 bool found = false;
                 for (int eb = b; eb < e1 && !found; eb += 8) {
                     int e = eb + tl;
