@@ -144,6 +144,21 @@ int mf_solve(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, int64_t *fl
  * (and stats[i], if stats != NULL) for query i. */
 int mf_solve_batch(mf_graph *g, int nq, const int32_t *s, const int32_t *t, const mf_opts *opts,
                    int64_t *flows, mf_stats *stats);
+/* nq solves in one launch, each on the graph with its own capacities for a
+ * fixed set of narcs forward arcs u[j] -> v[j] (caller ids): query i runs
+ * with capacity caps[i * narcs + j] on arc j, every other arc keeps the
+ * graph's capacity.  Every (u[j], v[j]) must name an arc of the graph and
+ * 0 <= caps[i * narcs + j] <= its capacity (MF_ERR_ARG otherwise): the graph
+ * is built with the largest capacity each overridden arc takes, so each
+ * query's prune stays a superset of its own.  A query batch of terminal
+ * sets on one segmentation grid (terminal arcs to both super terminals at
+ * the largest weight, each query zeroing or lowering them) replaces one run
+ * of the reference per input directory (RA:2561-2570) when only those
+ * capacities differ.  opts->certify is rejected (the cut check reads the
+ * graph's capacities).  narcs == 0 is mf_solve_batch. */
+int mf_solve_batch_override(mf_graph *g, int nq, const int32_t *s, const int32_t *t, long long narcs,
+                            const int32_t *u, const int32_t *v, const int64_t *caps,
+                            const mf_opts *opts, int64_t *flows, mf_stats *stats);
 /* Device time (ms) of the last mf_solve_batch / mf_solve call on g. */
 double mf_last_device_ms(const mf_graph *g);
 

@@ -147,6 +147,18 @@ class Graph:
                                   _p(flows, C.c_int64), sts))
         return (flows, list(sts)[:nq]) if with_stats else flows
 
+    def solve_batch_override(self, s, t, u, v, caps, o=None, with_stats=False):
+        """Batch where query i gives arcs u[j]->v[j] the capacities caps[i, j]."""
+        s, t, u, v = _i32(s), _i32(t), _i32(u), _i32(v)
+        nq, nb = len(s), len(u)
+        caps = np.ascontiguousarray(np.asarray(caps, np.int64).reshape(nq, nb))
+        flows = np.zeros(nq, np.int64)
+        sts = (MfStats * max(nq, 1))() if with_stats else None
+        _check(lib.mf_solve_batch_override(self._h, nq, _p(s, C.c_int32), _p(t, C.c_int32), nb,
+                                           _p(u, C.c_int32), _p(v, C.c_int32), _p(caps, C.c_int64),
+                                           C.byref(o or opts()), _p(flows, C.c_int64), sts))
+        return (flows, list(sts)[:nq]) if with_stats else flows
+
     @property
     def last_device_ms(self):
         return lib.mf_last_device_ms(self._h)
@@ -308,6 +320,31 @@ def gen_grid(W, H, seed):
                            _p(c, C.c_int64), C.byref(m)))
     k = m.value
     return u[:k].copy(), v[:k].copy(), c[:k].copy()
+
+
+def gen_grid_terminal_sets(W, H, nq, seed, wmax=255):
+    """Segmentation grid whose queries vary the terminal set: the graph holds
+    the neighbour arcs of gen_grid plus S->p and p->T for every pixel p at
+    capacity wmax; query i keeps one of the two per pixel (seeded mask) at a
+    weight uniform in [0, wmax] and zeroes the other.  Returns the graph
+    (n, u, v, cap), the overridden arcs (tu, tv) and caps[nq, 2*W*H]."""
+    u, v, c = gen_grid(W, H, seed)
+    S, T = W * H, W * H + 1
+    nb = (u < S) & (v < S)
+    px = np.arange(W * H, dtype=np.int32)
+    tu = np.concatenate([np.full(W * H, S, np.int32), px])
+    tv = np.concatenate([px, np.full(W * H, T, np.int32)])
+    gu = np.concatenate([u[nb], tu])
+    gv = np.concatenate([v[nb], tv])
+    gc = np.concatenate([c[nb], np.full(2 * W * H, wmax, np.int64)])
+    rng = np.random.default_rng(seed)
+    caps = np.zeros((nq, 2 * W * H), np.int64)
+    for i in range(nq):
+        to_src = rng.integers(0, 2, W * H, dtype=np.int8).astype(bool)
+        w = rng.integers(0, wmax + 1, W * H, dtype=np.int64)
+        caps[i, :W * H] = np.where(to_src, w, 0)
+        caps[i, W * H:] = np.where(to_src, 0, w)
+    return W * H + 2, gu, gv, gc, tu, tv, caps
 
 
 def gen_queries_hub(n, u, v, nhub, nuni, seed):

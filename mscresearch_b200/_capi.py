@@ -90,6 +90,7 @@ SIGNATURES = {
     "mf_graph_repartition": (C.c_int, [C.c_void_p, C.c_int]),
     "mf_solve": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(MfOpts), i64p, C.POINTER(MfStats)]),
     "mf_solve_batch": (C.c_int, [C.c_void_p, C.c_int, i32p, i32p, C.POINTER(MfOpts), i64p, C.POINTER(MfStats)]),
+    "mf_solve_batch_override": (C.c_int, [C.c_void_p, C.c_int, i32p, i32p, C.c_longlong, i32p, i32p, i64p, C.POINTER(MfOpts), i64p, C.POINTER(MfStats)]),
     "mf_last_device_ms": (C.c_double, [C.c_void_p]),
     "mf_debug_prune_mask": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(MfOpts), u8p, C.POINTER(C.c_int)]),
     "mf_debug_initial_heights": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(MfOpts), i32p]),

@@ -211,6 +211,17 @@ __global__ void k_find_arcs(int nb, const int *u, const int *v, const int *row, 
     capv[i] = (a >= 0) ? cap[a] : 0;
 }
 
+// Override checks: every arc resolved, every query's capacity in
+// [0, the graph's capacity of the arc]; counts the violations.
+__global__ void k_check_overrides(long long nov, int nq, const int *arc, const i64 *gcap, const i64 *ov,
+                                  int *bad) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nov * (long long)nq) return;
+    long long j = i % nov;
+    i64 c = ov[i];
+    if (arc[j] < 0 || c < 0 || c > gcap[j]) atomicAdd(bad, 1);
+}
+
 __global__ void k_apply_caps(int nu, const ArcUpdate *upd, i64 *cap) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < nu) cap[upd[i].arc] = upd[i].new_cap;
@@ -498,7 +509,8 @@ int status_from_err(int e) {
 // per_query_slot: query i uses slot i (sessions); else a slot per group.
 int launch(mf_graph *g, SlotPool &pool, int nq, const int *s_int, const int *t_int,
            bool per_query_slot, const mf_opts &o, int mode, void *dbg, const ArcUpdate *d_upd,
-           int nupd, int G_req, QOut *outs) {
+           int nupd, int G_req, QOut *outs, const int *ov_arc = nullptr, const i64 *ov_cap = nullptr,
+           long long ov_n = 0) {
     const int want_threads = o.threads > 0 ? o.threads : 512;
     if (!g->dev.ok || g->dev.threads != want_threads) {
         int rc = dev_info(g->dev, want_threads);
@@ -562,6 +574,9 @@ int launch(mf_graph *g, SlotPool &pool, int nq, const int *s_int, const int *t_i
     p.dbg = dbg;
     p.upd = d_upd;
     p.nupd = nupd;
+    p.ov_arc = ov_arc;
+    p.ov_cap = ov_cap;
+    p.ov_n = ov_n;
     int grid = ngroups * G;
     cudaError_t le = cudaSuccess;
     CK(cudaEventRecord(g->ev0, g->stream));
@@ -993,6 +1008,86 @@ int mf_solve(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, int64_t *fl
 int mf_solve_batch(mf_graph *g, int nq, const int32_t *s, const int32_t *t, const mf_opts *opts,
                    int64_t *flows, mf_stats *stats) {
     return solve_common(g, nq, s, t, opts, flows, stats, KM_SOLVE, nullptr, false);
+}
+
+int mf_solve_batch_override(mf_graph *g, int nq, const int32_t *s, const int32_t *t, long long narcs,
+                            const int32_t *u, const int32_t *v, const int64_t *caps, const mf_opts *opts,
+                            int64_t *flows, mf_stats *stats) {
+    if (!g) return fail(MF_ERR_ARG, "graph is NULL");
+    if (nq < 0 || narcs < 0 || narcs > 0x7fffffffLL || (nq > 0 && (!s || !t || !flows)) ||
+        (narcs > 0 && nq > 0 && (!u || !v || !caps)))
+        return fail(MF_ERR_ARG, "bad query or override arrays");
+    if (nq == 0) return MF_OK;
+    if (narcs == 0) return mf_solve_batch(g, nq, s, t, opts, flows, stats);
+    mf_opts o;
+    if (opts) o = *opts;
+    else mf_opts_default(&o);
+    if (o.certify) return fail(MF_ERR_ARG, "certify is not available with capacity overrides");
+    const int nb = (int)narcs;
+    std::vector<int> iu(nb), iv(nb);
+    for (int j = 0; j < nb; ++j) {
+        iu[j] = (u[j] >= 0 && u[j] < g->n) ? g->new_id[u[j]] : -1;
+        iv[j] = (v[j] >= 0 && v[j] < g->n) ? g->new_id[v[j]] : -1;
+    }
+    int *du = nullptr, *dv = nullptr, *darc = nullptr, *dbad = nullptr;
+    i64 *dgcap = nullptr, *dov = nullptr;
+    const size_t ovn = (size_t)nq * (size_t)nb;
+    int rc = MF_OK;
+    do {
+        if (cudaMalloc(&du, sizeof(int) * nb) != cudaSuccess || cudaMalloc(&dv, sizeof(int) * nb) != cudaSuccess ||
+            cudaMalloc(&darc, sizeof(int) * nb) != cudaSuccess || cudaMalloc(&dgcap, sizeof(i64) * nb) != cudaSuccess ||
+            cudaMalloc(&dov, sizeof(i64) * ovn) != cudaSuccess || cudaMalloc(&dbad, sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            rc = fail(MF_ERR_NOMEM, "override buffers (%zu capacities) do not fit", ovn);
+            break;
+        }
+        if (cudaMemcpy(du, iu.data(), sizeof(int) * nb, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(dv, iv.data(), sizeof(int) * nb, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(dov, caps, sizeof(i64) * ovn, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemset(dbad, 0, sizeof(int)) != cudaSuccess) {
+            rc = fail(MF_ERR_CUDA, "override upload failed");
+            break;
+        }
+        k_find_arcs<<<(nb + 255) / 256, 256, 0, g->stream>>>(nb, du, dv, g->row, g->col, g->rev, g->fwd, g->cap,
+                                                              darc, dgcap);
+        k_check_overrides<<<(unsigned)((ovn + 255) / 256), 256, 0, g->stream>>>(nb, nq, darc, dgcap, dov, dbad);
+        int hbad = 0;
+        if (cudaMemcpyAsync(&hbad, dbad, sizeof(int), cudaMemcpyDeviceToHost, g->stream) != cudaSuccess ||
+            cudaStreamSynchronize(g->stream) != cudaSuccess) {
+            rc = fail(MF_ERR_CUDA, "override check failed: %s", cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        if (hbad) {
+            rc = fail(MF_ERR_ARG, "%d override entries name no forward arc or lie outside [0, the arc's capacity]",
+                      hbad);
+            break;
+        }
+        std::vector<int> si(nq), ti(nq);
+        for (int i = 0; i < nq; ++i) to_internal(g, s[i], t[i], si[i], ti[i]);
+        if ((rc = ensure_kept_cache(g, o))) break;
+        std::vector<QOut> outs(nq);
+        const int G = o.group_ctas > 0 ? o.group_ctas : 8;
+        if ((rc = launch(g, g->pool, nq, si.data(), ti.data(), false, o, KM_SOLVE, nullptr, nullptr, 0, G,
+                         outs.data(), darc, dov, narcs)))
+            break;
+        int worst = MF_OK;
+        u64 t0min = ~0ull;
+        for (int i = 0; i < nq; ++i) t0min = std::min(t0min, outs[i].t_begin);
+        for (int i = 0; i < nq; ++i) {
+            flows[i] = outs[i].flow;
+            if (stats) fill_stats(&stats[i], outs[i], 0.0, t0min);
+            int st = status_from_err(outs[i].status);
+            if (st != MF_OK && worst == MF_OK) worst = st;
+        }
+        if (worst != MF_OK) rc = fail(worst, "a query ended with status %d", worst);
+    } while (0);
+    cudaFree(du);
+    cudaFree(dv);
+    cudaFree(darc);
+    cudaFree(dgcap);
+    cudaFree(dov);
+    cudaFree(dbad);
+    return rc;
 }
 
 double mf_last_device_ms(const mf_graph *g) { return g ? g->last_ms : 0.0; }

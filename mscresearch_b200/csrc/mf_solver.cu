@@ -791,6 +791,22 @@ __device__ bool fix_extra_arcs(QCtx &c, unsigned M, int nv) {
     return c.sync();
 }
 
+// Per-query capacity overrides: the query's own capacity on each override
+// arc whose ends are both kept (the residual was just initialised from the
+// graph's capacity, which bounds the override from above, so the kept set
+// computed with the graph's capacities covers the query's).
+__device__ bool apply_overrides(QCtx &c, const KParams &p, int q, unsigned M) {
+    const long long nov = p.ov_n;
+    const i64 *caps = p.ov_cap + (long long)q * nov;
+    int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+    for (long long j = gt; j < nov; j += gT) {
+        const int e = ldro(&p.ov_arc[j]);
+        const int w = ldro(&c.col[e]), a = ldro(&c.col[ldro(&c.rev[e])]);
+        if (ldcg(&c.st.mark[w]) >= M && ldcg(&c.st.mark[a]) >= M) c.st.res[e] = ldro(&caps[j]);
+    }
+    return c.sync();
+}
+
 // ---------------------------------------------------------------------------
 // Fresh residual state over the kept vertices: excess 0; res[e] = cap[e]
 // when the head is kept, else 0 (the arc is outside the induced subgraph).
@@ -2109,6 +2125,7 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
             } else if (!init_state(c, nv, M)) {
                 return;
             }
+            if (p.ov_arc && !apply_overrides(c, p, q, M)) return;
             if (!preflow(c, s)) return;
         }
     }

@@ -181,6 +181,11 @@ struct KParams {
     void *dbg;
     const ArcUpdate *upd;
     int nupd;
+    // per-query capacity overrides (NULL: none): query q sees capacity
+    // ov_cap[q * ov_n + j] on forward arc ov_arc[j] (never above its cap)
+    const int *ov_arc;
+    const i64 *ov_cap;
+    long long ov_n;
     // serving ring (mode KM_SOLVE with ring != NULL): requests are read from
     // ring_req[i] once ring_tail (host-written) exceeds i; completion flags.
     volatile int *ring_tail;

@@ -244,3 +244,39 @@ def test_full_size_grid_properties():
         assert [eg.solve(a, b)[0] for a, b in zip(s, t)] == list(fb)
         fc, stc = eg.certify(S, T)
         assert fc == fb[0] and stc.cut_capacity == fc and stc.status == 0
+
+
+def test_batch_override_terminal_sets():
+    """Queries that vary the terminal set of one grid (per-query capacities
+    on the terminal arcs) == the oracle on a graph built for each set."""
+    W, H, nq = 24, 16, 5
+    n, gu, gv, gc, tu, tv, caps = mf.gen_grid_terminal_sets(W, H, nq, seed=4)
+    S, T = W * H, W * H + 1
+    nbr = len(gu) - len(tu)
+    exp = []
+    for i in range(nq):
+        keep = caps[i] > 0
+        u = np.concatenate([gu[:nbr], tu[keep]])
+        v = np.concatenate([gv[:nbr], tv[keep]])
+        c = np.concatenate([gc[:nbr], caps[i][keep]])
+        exp.append(O.dinic(O.build_csr(n, u, v, c), S, T))
+    s, t = [S] * nq, [T] * nq
+    with mf.Graph.from_edges(n, gu, gv, gc, R=16) as eg:
+        assert list(eg.solve_batch_override(s, t, tu, tv, caps)) == exp
+        # all capacities at the graph's own values: the plain batch
+        full = np.tile(gc[nbr:], (2, 1))
+        assert list(eg.solve_batch_override([S, 7], [T, T], tu, tv, full)) == list(eg.solve_batch([S, 7], [T, T]))
+        # a pixel pair inside the grid, and a query whose source arcs are all zero
+        z = caps[:2].copy()
+        z[1, :W * H] = 0
+        f = eg.solve_batch_override([3, S], [100, T], tu, tv, z)
+        g0 = O.build_csr(n, np.concatenate([gu[:nbr], tu[z[0] > 0]]), np.concatenate([gv[:nbr], tv[z[0] > 0]]),
+                         np.concatenate([gc[:nbr], z[0][z[0] > 0]]))
+        assert list(f) == [O.dinic(g0, 3, 100), 0]
+        # rejected: an arc the graph lacks, a capacity above the graph's, certify
+        with pytest.raises(mf.MaxflowError):
+            eg.solve_batch_override([S], [T], [0], [W * H - 1], [[1]])
+        with pytest.raises(mf.MaxflowError):
+            eg.solve_batch_override([S], [T], tu[:1], tv[:1], [[256]])
+        with pytest.raises(mf.MaxflowError):
+            eg.solve_batch_override([S], [T], tu[:1], tv[:1], [[1]], o=mf.opts(certify=1))
