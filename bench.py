@@ -447,7 +447,8 @@ def run_mix(args):
         print(json.dumps(res), flush=True)
 
 
-GRID_TUNE = [(16, 0.35), (4, 0.35), (1, 0.35), (64, 2.0)]
+# (gr_freq, gr_work_alpha, CTAs per query group) tried on a sample of the sets
+GRID_TUNE = [(16, 0.35, 8), (4, 0.35, 8), (1, 0.35, 8), (64, 2.0, 8), (16, 0.35, 4), (16, 0.35, 16)]
 
 
 def run_gridsets(args):
@@ -469,22 +470,32 @@ def run_gridsets(args):
     t = np.full(nq, T, np.int32)
     g = mf.Graph.from_edges(n, gu, gv, gc, R=R)
     _, arcs, _ = g.info
-    # tuning (untimed): relabel frequency on a sample of the sets, then R
-    smp = min(8, nq)
+    # tuning (untimed): relabel frequency and group size on a sample of the
+    # sets, then R.  A sample launch runs ceil(smp / groups) waves of queries
+    # and the batch ceil(nq / groups), so the sample time is scaled by that
+    # ratio (groups = resident CTAs / G) to compare group sizes.
+    smp = min(16, nq)
+    ctas = 2 * torch.cuda.get_device_properties(0).multi_processor_count
     tune = []
     best_o, best_ms, best_R = None, None, R
-    for gf, al in GRID_TUNE:
-        o = mf.opts(group_ctas=args.group, gr_freq=gf, gr_work_alpha=al)
+
+    def est(ms, G):
+        gr = max(1, ctas // G)
+        return ms * (-(-nq // gr)) / (-(-smp // gr))
+
+    for gf, al, G in GRID_TUNE:
+        o = mf.opts(group_ctas=G, gr_freq=gf, gr_work_alpha=al)
         g.solve_batch_override(s[:smp], t[:smp], tu, tv, caps[:smp], o)
-        ms = g.last_device_ms
-        tune.append({"gr_freq": gf, "gr_alpha": al, "R": R, "sample_ms": round(ms, 2)})
+        ms = est(g.last_device_ms, G)
+        tune.append({"gr_freq": gf, "gr_alpha": al, "G": G, "R": R, "batch_ms_est": round(ms, 2)})
         if best_ms is None or ms < best_ms:
             best_o, best_ms = o, ms
     for r in (32, 512):
         g.repartition(r)
         g.solve_batch_override(s[:smp], t[:smp], tu, tv, caps[:smp], best_o)
-        ms = g.last_device_ms
-        tune.append({"gr_freq": best_o.gr_freq, "gr_alpha": best_o.gr_work_alpha, "R": r, "sample_ms": round(ms, 2)})
+        ms = est(g.last_device_ms, best_o.group_ctas)
+        tune.append({"gr_freq": best_o.gr_freq, "gr_alpha": best_o.gr_work_alpha, "G": best_o.group_ctas, "R": r,
+                     "batch_ms_est": round(ms, 2)})
         if ms < best_ms:
             best_ms, best_R = ms, r
     if g.info[2] != best_R:

@@ -120,8 +120,25 @@ const char *mf_version(void);
  * R = 0 means 128 (RA:2583), and R is clamped to [1, n]. */
 int mf_graph_create_from_edges(int n, long long m, const int32_t *u, const int32_t *v,
                                const int64_t *cap, int R, mf_graph **out);
-/* Same, reading <path> in graph.txt format (1-based ids, RA:1051-1075). */
+/* Same from edge arrays already in device memory (d_u, d_v, d_cap: device
+ * pointers of m entries each; read only, the caller keeps them). */
+int mf_graph_create_from_device_edges(int n, long long m, const int32_t *d_u, const int32_t *d_v,
+                                      const int64_t *d_cap, int R, mf_graph **out);
+/* Same, reading <path> in graph.txt format (1-based ids; replaces
+ * build_graph, RA:1044-1126).  The file's bytes are copied to the device and
+ * tokenised there with fscanf's rules (an "n m" header, then up to m
+ * "u v cap" triples, stopping at the first triple that does not scan,
+ * RA:1068-1075); the CSR is built on the device in the host build's arc
+ * order.  MF_ERR_IO if the file cannot be read or has no "n m" header with
+ * n > 0, m >= 0. */
 int mf_graph_load_file(const char *path, int R, mf_graph **out);
+/* Binary CSR cache: mf_graph_save writes the region-ordered graph and its
+ * maps; mf_graph_load_binary restores it without parsing, building or
+ * partitioning (checked for consistency on the device; MF_ERR_IO for a file
+ * that is not a cache of this library, truncated or inconsistent).  The
+ * loaded graph equals the saved one array for array. */
+int mf_graph_save(const mf_graph *g, const char *path);
+int mf_graph_load_binary(const char *path, mf_graph **out);
 int mf_graph_destroy(mf_graph *g);
 /* n, kept arcs (2 x kept edges), R. */
 int mf_graph_info(const mf_graph *g, int *n, long long *arcs, int *R);

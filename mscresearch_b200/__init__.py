@@ -85,10 +85,28 @@ class Graph:
         return cls(h.value)
 
     @classmethod
+    def from_device_edges(cls, n, m, d_u, d_v, d_cap, R=128):
+        """Edges already on the device: d_u, d_v, d_cap are device addresses
+        (e.g. torch int32/int32/int64 CUDA tensors' data_ptr())."""
+        h = C.c_void_p()
+        _check(lib.mf_graph_create_from_device_edges(int(n), int(m), C.c_void_p(d_u), C.c_void_p(d_v),
+                                                     C.c_void_p(d_cap), int(R), C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
     def load(cls, path, R=128):
         h = C.c_void_p()
         _check(lib.mf_graph_load_file(path.encode(), int(R), C.byref(h)))
         return cls(h.value)
+
+    @classmethod
+    def load_binary(cls, path):
+        h = C.c_void_p()
+        _check(lib.mf_graph_load_binary(path.encode(), C.byref(h)))
+        return cls(h.value)
+
+    def save(self, path):
+        _check(lib.mf_graph_save(self._h, path.encode()))
 
     def close(self):
         if self._h:

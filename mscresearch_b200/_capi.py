@@ -83,7 +83,10 @@ SIGNATURES = {
     "mf_last_error_string": (C.c_char_p, []),
     "mf_version": (C.c_char_p, []),
     "mf_graph_create_from_edges": (C.c_int, [C.c_int, C.c_longlong, i32p, i32p, i64p, C.c_int, C.POINTER(C.c_void_p)]),
+    "mf_graph_create_from_device_edges": (C.c_int, [C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "mf_graph_load_file": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "mf_graph_save": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "mf_graph_load_binary": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     "mf_graph_destroy": (C.c_int, [C.c_void_p]),
     "mf_graph_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
     "mf_graph_export": (C.c_int, [C.c_void_p, i32p, i32p, i64p, i32p, i32p, i32p, f64p, i32p]),

@@ -349,6 +349,8 @@ int upload_dgraph(mf_graph *g) {
     return MF_OK;
 }
 
+int finalize_graph(mf_graph *g);
+
 // Partition + reorder the device CSR given in (row,col,cap,rev,fwd), whose
 // vertex i is caller vertex in_ids[i].  Replaces the graph arrays.
 int partition_into(mf_graph *g, int R, int *row, int *col, i64 *cap, int *rev, unsigned char *fwd,
@@ -404,6 +406,13 @@ int partition_into(mf_graph *g, int R, int *row, int *col, i64 *cap, int *rev, u
     g->new_id.swap(new_id);
     g->old_id.swap(old_id);
     g->R = R;
+    return finalize_graph(g);
+}
+
+// Host copies of the degrees, the hub list, the cache pivot and the device
+// graph record, from the region-ordered arrays.
+int finalize_graph(mf_graph *g) {
+    const int n = g->n;
     int best = 0;
     {
         std::vector<int> rw(n + 1), hl;
@@ -648,40 +657,93 @@ int to_internal(const mf_graph *g, int s, int t, int &si, int &ti) {
     return 1;
 }
 
-// Host CSR build with the reference reader's rules (RA:1068-1122).
-void host_csr(int n, i64 m, const int32_t *u, const int32_t *v, const int64_t *c,
-              std::vector<int> &row, std::vector<int> &col, std::vector<i64> &cap,
-              std::vector<int> &rev, std::vector<unsigned char> &fwd) {
-    std::vector<int> deg(n + 1, 0);
-    i64 kept = 0;
-    for (i64 i = 0; i < m; ++i) {
-        int a = u[i], b = v[i];
-        if (a < 0 || a >= n || b < 0 || b >= n || a == b || c[i] <= 0) continue;
-        deg[a]++;
-        deg[b]++;
-        ++kept;
+// File -> device copy through two pinned staging buffers: each chunk's copy
+// overlaps the next chunk's read.
+struct FileStream {
+    unsigned char *pin[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    cudaStream_t st = nullptr;
+    size_t chunk = 16u << 20;
+    int k = 0;
+    bool init(cudaStream_t s) {
+        st = s;
+        return cudaMallocHost(&pin[0], chunk) == cudaSuccess && cudaMallocHost(&pin[1], chunk) == cudaSuccess &&
+               cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming) == cudaSuccess;
     }
-    row.assign(n + 1, 0);
-    for (int x = 0; x < n; ++x) row[x + 1] = row[x] + deg[x];
-    i64 arcs = row[n];
-    col.resize(arcs);
-    cap.resize(arcs);
-    rev.resize(arcs);
-    fwd.resize(arcs);
-    for (int x = 0; x < n; ++x) deg[x] = row[x];
-    for (i64 i = 0; i < m; ++i) {
-        int a = u[i], b = v[i];
-        if (a < 0 || a >= n || b < 0 || b >= n || a == b || c[i] <= 0) continue;
-        int ea = deg[a]++, eb = deg[b]++;
-        col[ea] = b;
-        cap[ea] = c[i];
-        rev[ea] = eb;
-        fwd[ea] = 1;
-        col[eb] = a;
-        cap[eb] = 0;
-        rev[eb] = ea;
-        fwd[eb] = 0;
+    // reads up to `bytes` from f into dst; returns the bytes copied
+    size_t copy(FILE *f, void *dst, size_t bytes) {
+        size_t got = 0;
+        while (got < bytes) {
+            const int b = k & 1;
+            if (k >= 2) cudaEventSynchronize(done[b]);
+            size_t want = std::min(chunk, bytes - got);
+            size_t r = fread(pin[b], 1, want, f);
+            if (r == 0) break;
+            if (cudaMemcpyAsync((unsigned char *)dst + got, pin[b], r, cudaMemcpyHostToDevice, st) != cudaSuccess)
+                break;
+            cudaEventRecord(done[b], st);
+            ++k;
+            got += r;
+        }
+        return got;
     }
+    ~FileStream() {
+        if (st) cudaStreamSynchronize(st);
+        cudaFreeHost(pin[0]);
+        cudaFreeHost(pin[1]);
+        if (done[0]) cudaEventDestroy(done[0]);
+        if (done[1]) cudaEventDestroy(done[1]);
+    }
+};
+
+// A graph object with its stream and events, no arrays yet.
+int new_graph(int n, mf_graph **out) {
+    mf_graph *g = new mf_graph();
+    g->n = n;
+    cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete g;
+        return fail(MF_ERR_CUDA, "no CUDA device usable: %s", cudaGetErrorString(e));
+    }
+    cudaEventCreate(&g->ev0);
+    cudaEventCreate(&g->ev1);
+    *out = g;
+    return MF_OK;
+}
+
+// Graph from device edge arrays (caller ids, the reference reader's skip
+// rules): device CSR in input order, then partition + reorder.
+int graph_from_device_edges(int n, i64 m, const int *du, const int *dv, const i64 *dc, int R,
+                            mf_graph **out) {
+    *out = nullptr;
+    if (R <= 0) R = 128;
+    R = std::min(std::min(R, n), 1024);
+    mf_graph *g = nullptr;
+    int rc = new_graph(n, &g);
+    if (rc) return rc;
+    DevCsr csr;
+    cudaError_t e = mf_device_csr(n, m, du, dv, dc, g->stream, csr);
+    if (e != cudaSuccess) {
+        mf_graph_destroy(g);
+        return fail(e == cudaErrorMemoryAllocation ? MF_ERR_NOMEM : MF_ERR_CUDA, "device CSR build failed: %s",
+                    cudaGetErrorString(e));
+    }
+    g->arcs = csr.arcs;
+    g->avg_deg = (int)(g->arcs / n);
+    std::vector<int> ident(n);
+    for (int i = 0; i < n; ++i) ident[i] = i;
+    rc = partition_into(g, R, csr.row, csr.col, csr.cap, csr.rev, csr.fwd, ident);
+    mf_free_dev_csr(csr);
+    if (rc != MF_OK) {
+        mf_graph_destroy(g);
+        return rc;
+    }
+    g->pool.n = n;
+    g->pool.arcs = g->arcs;
+    g->pool.nhub = g->nhub;
+    *out = g;
+    return MF_OK;
 }
 
 }  // namespace
@@ -727,60 +789,94 @@ int mf_graph_create_from_edges(int n, long long m, const int32_t *u, const int32
     if (n <= 0) return fail(MF_ERR_ARG, "n must be positive (got %d)", n);
     if (m < 0 || (m > 0 && (!u || !v || !cap))) return fail(MF_ERR_ARG, "bad edge arrays");
     if (2 * m > 0x7fffffffLL) return fail(MF_ERR_ARG, "too many edges for int32 arc ids");
-    if (R <= 0) R = 128;
-    R = std::min(std::min(R, n), 1024);
-    std::vector<int> row, col, rev;
-    std::vector<i64> cp;
-    std::vector<unsigned char> fwd;
-    host_csr(n, m, u, v, cap, row, col, cp, rev, fwd);
-    mf_graph *g = new mf_graph();
-    g->n = n;
-    g->arcs = row[n];
-    g->avg_deg = (int)(g->arcs / n);
-    cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) {
-        delete g;
-        return fail(MF_ERR_CUDA, "no CUDA device usable: %s", cudaGetErrorString(e));
-    }
-    cudaEventCreate(&g->ev0);
-    cudaEventCreate(&g->ev1);
-    int *drow = nullptr, *dcol = nullptr, *drev = nullptr;
-    i64 *dcap = nullptr;
-    unsigned char *dfwd = nullptr;
-    size_t A = (size_t)std::max<i64>(g->arcs, 1);
+    int *du = nullptr, *dv = nullptr;
+    i64 *dc = nullptr;
+    const size_t M = (size_t)std::max<long long>(m, 1);
     int rc = MF_OK;
+    if (cudaMalloc(&du, sizeof(int) * M) != cudaSuccess || cudaMalloc(&dv, sizeof(int) * M) != cudaSuccess ||
+        cudaMalloc(&dc, sizeof(i64) * M) != cudaSuccess) {
+        cudaGetLastError();
+        rc = fail(MF_ERR_NOMEM, "edge upload allocation failed (%lld edges)", m);
+    } else if (m > 0 && (cudaMemcpy(du, u, sizeof(int) * m, cudaMemcpyHostToDevice) != cudaSuccess ||
+                         cudaMemcpy(dv, v, sizeof(int) * m, cudaMemcpyHostToDevice) != cudaSuccess ||
+                         cudaMemcpy(dc, cap, sizeof(i64) * m, cudaMemcpyHostToDevice) != cudaSuccess)) {
+        rc = fail(MF_ERR_CUDA, "edge upload failed");
+    } else {
+        rc = graph_from_device_edges(n, m, du, dv, dc, R, out);
+    }
+    cudaFree(du);
+    cudaFree(dv);
+    cudaFree(dc);
+    return rc;
+}
+
+int mf_graph_create_from_device_edges(int n, long long m, const int32_t *d_u, const int32_t *d_v,
+                                      const int64_t *d_cap, int R, mf_graph **out) {
+    if (!out) return fail(MF_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (n <= 0) return fail(MF_ERR_ARG, "n must be positive (got %d)", n);
+    if (m < 0 || (m > 0 && (!d_u || !d_v || !d_cap))) return fail(MF_ERR_ARG, "bad edge arrays");
+    if (2 * m > 0x7fffffffLL) return fail(MF_ERR_ARG, "too many edges for int32 arc ids");
+    return graph_from_device_edges(n, m, d_u, d_v, reinterpret_cast<const i64 *>(d_cap), R, out);
+}
+
+int mf_graph_load_file(const char *path, int R, mf_graph **out) {
+    if (!out || !path) return fail(MF_ERR_ARG, "path or out is NULL");
+    *out = nullptr;
+    FILE *f = fopen(path, "rb");
+    if (!f) return fail(MF_ERR_IO, "cannot open %s", path);
+    fseek(f, 0, SEEK_END);
+    long long S = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    if (S < 0) S = 0;
+    unsigned char *dtxt = nullptr;
+    cudaStream_t st = nullptr;
+    int rc = MF_OK;
+    long long got = 0;
+    TextEdges te;
     do {
-        if (cudaMalloc(&drow, sizeof(int) * ((size_t)n + 1)) || cudaMalloc(&dcol, sizeof(int) * A) ||
-            cudaMalloc(&drev, sizeof(int) * A) || cudaMalloc(&dcap, sizeof(i64) * A) ||
-            cudaMalloc(&dfwd, A)) {
-            rc = fail(MF_ERR_NOMEM, "graph upload allocation failed");
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaMalloc(&dtxt, (size_t)std::max<long long>(S, 1)) != cudaSuccess) {
+            cudaGetLastError();
+            rc = fail(MF_ERR_NOMEM, "text staging for %lld bytes failed", S);
             break;
         }
-        cudaMemcpy(drow, row.data(), sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice);
-        if (g->arcs) {
-            cudaMemcpy(dcol, col.data(), sizeof(int) * g->arcs, cudaMemcpyHostToDevice);
-            cudaMemcpy(drev, rev.data(), sizeof(int) * g->arcs, cudaMemcpyHostToDevice);
-            cudaMemcpy(dcap, cp.data(), sizeof(i64) * g->arcs, cudaMemcpyHostToDevice);
-            cudaMemcpy(dfwd, fwd.data(), g->arcs, cudaMemcpyHostToDevice);
+        {
+            FileStream fs;
+            if (!fs.init(st)) {
+                cudaGetLastError();
+                rc = fail(MF_ERR_NOMEM, "pinned staging failed");
+                break;
+            }
+            got = (long long)fs.copy(f, dtxt, (size_t)S);
         }
-        std::vector<int> ident(n);
-        for (int i = 0; i < n; ++i) ident[i] = i;
-        rc = partition_into(g, R, drow, dcol, dcap, drev, dfwd, ident);
+        if (got != S) {
+            rc = fail(MF_ERR_IO, "read of %s stopped at byte %lld of %lld", path, got, S);
+            break;
+        }
+        cudaError_t e = mf_parse_graph_text(dtxt, got, st, te);
+        if (e != cudaSuccess) {
+            rc = fail(e == cudaErrorMemoryAllocation ? MF_ERR_NOMEM : MF_ERR_CUDA, "graph text parse failed: %s",
+                      cudaGetErrorString(e));
+            break;
+        }
+        if (!te.header_ok || te.n <= 0 || te.m_header < 0) {
+            rc = fail(MF_ERR_IO, "%s: no valid \"n m\" header", path);
+            break;
+        }
+        cudaFree(dtxt);
+        dtxt = nullptr;
+        if (2 * te.m > 0x7fffffffLL) {
+            rc = fail(MF_ERR_ARG, "too many edges for int32 arc ids");
+            break;
+        }
+        rc = graph_from_device_edges(te.n, te.m, te.u, te.v, te.c, R, out);
     } while (0);
-    cudaFree(drow);
-    cudaFree(dcol);
-    cudaFree(drev);
-    cudaFree(dcap);
-    cudaFree(dfwd);
-    if (rc != MF_OK) {
-        mf_graph_destroy(g);
-        return rc;
-    }
-    g->pool.n = n;
-    g->pool.arcs = g->arcs;
-    g->pool.nhub = g->nhub;
-    *out = g;
-    return MF_OK;
+    fclose(f);
+    mf_free_text_edges(te);
+    cudaFree(dtxt);
+    if (st) cudaStreamDestroy(st);
+    return rc;
 }
 
 int mf_graph_repartition(mf_graph *g, int R) {
@@ -850,6 +946,62 @@ int mf_graph_export(const mf_graph *g, int32_t *row, int32_t *col, int64_t *cap,
     if (score) memcpy(score, g->score_caller.data(), sizeof(double) * g->n);
     if (part) memcpy(part, g->part_caller.data(), sizeof(int) * g->n);
     return MF_OK;
+}
+
+// ---- binary CSR cache ------------------------------------------------------
+// File: CacheHead, then row[n+1] i32, col[A] i32, cap[A] i64, rev[A] i32,
+// fwd[A] u8, region_start[R+1] i32, region_of[n] i32 (region-ordered CSR),
+// new_id[n] i32, score[n] f64, part[n] i32 (caller ids); native byte order.
+struct CacheHead {
+    char magic[8];
+    int32_t version;
+    int32_t n;
+    int64_t arcs;
+    int32_t R;
+    int32_t pad;
+    int64_t bytes;  // whole file
+};
+static const char kCacheMagic[8] = {'M', 'F', 'B', '2', '0', '0', 'C', 'S'};
+
+static int64_t cache_bytes(int n, i64 A, int R) {
+    return (int64_t)sizeof(CacheHead) + 4 * ((int64_t)n + 1) + 4 * A + 8 * A + 4 * A + A + 4 * ((int64_t)R + 1) +
+           4 * (int64_t)n + 4 * (int64_t)n + 8 * (int64_t)n + 4 * (int64_t)n;
+}
+
+// Consistency of a loaded region-ordered CSR (row and region starts already
+// checked monotone on the host): a warp per vertex over its arcs -- heads in
+// range, rev an involution pairing opposite arcs, one forward arc per pair,
+// capacities >= 0 and 0 on reverse arcs, region ranges covering each vertex.
+// Counts violations.
+__global__ void k_check_csr(int n, i64 A, int R, const int *row, const int *col, const i64 *cap, const int *rev,
+                            const unsigned char *fwd, const int *region_start, const int *region_of, int *bad) {
+    const int lane = threadIdx.x & 31;
+    const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    int nb = 0;
+    if (w0 == 0 && lane == 0) {
+        if (row[0] != 0 || (i64)row[n] != A) ++nb;
+        if (region_start[0] != 0 || region_start[R] != n) ++nb;
+    }
+    for (int x = w0; x < n; x += nw) {
+        const int b = row[x], e1 = row[x + 1];
+        if (lane == 0) {
+            int r = region_of[x];
+            if (r < 0 || r >= R || region_start[r] > x || region_start[r + 1] <= x) ++nb;
+        }
+        if (b < 0 || (i64)e1 > A) {
+            if (lane == 0) ++nb;
+            continue;
+        }
+        for (int e = b + lane; e < e1; e += 32) {
+            int w = col[e], re = rev[e];
+            if (w < 0 || w >= n || w == x || re < 0 || (i64)re >= A) {
+                ++nb;
+                continue;
+            }
+            if (rev[re] != e || col[re] != x || fwd[e] == fwd[re] || cap[e] < 0 || (!fwd[e] && cap[e] != 0)) ++nb;
+        }
+    }
+    if (nb) atomicAdd(bad, nb);
 }
 
 // kc_res[e] = cap[e] if both ends of e are in the component, else 0;
@@ -1091,6 +1243,158 @@ int mf_solve_batch_override(mf_graph *g, int nq, const int32_t *s, const int32_t
 }
 
 double mf_last_device_ms(const mf_graph *g) { return g ? g->last_ms : 0.0; }
+
+int mf_graph_save(const mf_graph *g, const char *path) {
+    if (!g || !path) return fail(MF_ERR_ARG, "graph or path is NULL");
+    const int n = g->n, R = g->R;
+    const i64 A = g->arcs;
+    std::vector<int> row(n + 1), col(A), rev(A), rs(R + 1), ro(n);
+    std::vector<i64> cap(A);
+    std::vector<unsigned char> fwd(A);
+    CK(cudaMemcpy(row.data(), g->row, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+    if (A) {
+        CK(cudaMemcpy(col.data(), g->col, sizeof(int) * A, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(cap.data(), g->cap, sizeof(i64) * A, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(rev.data(), g->rev, sizeof(int) * A, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(fwd.data(), g->fwd, A, cudaMemcpyDeviceToHost));
+    }
+    CK(cudaMemcpy(rs.data(), g->region_start, sizeof(int) * (R + 1), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ro.data(), g->region_of, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CacheHead h{};
+    memcpy(h.magic, kCacheMagic, 8);
+    h.version = 1;
+    h.n = n;
+    h.arcs = A;
+    h.R = R;
+    h.bytes = cache_bytes(n, A, R);
+    FILE *f = fopen(path, "wb");
+    if (!f) return fail(MF_ERR_IO, "cannot create %s", path);
+    bool ok = fwrite(&h, sizeof(h), 1, f) == 1;
+    auto put = [&](const void *p, size_t bytes) {
+        if (ok && bytes) ok = fwrite(p, 1, bytes, f) == bytes;
+    };
+    put(row.data(), 4 * row.size());
+    put(col.data(), 4 * (size_t)A);
+    put(cap.data(), 8 * (size_t)A);
+    put(rev.data(), 4 * (size_t)A);
+    put(fwd.data(), (size_t)A);
+    put(rs.data(), 4 * rs.size());
+    put(ro.data(), 4 * ro.size());
+    put(g->new_id.data(), 4 * (size_t)n);
+    put(g->score_caller.data(), 8 * (size_t)n);
+    put(g->part_caller.data(), 4 * (size_t)n);
+    if (fclose(f) != 0) ok = false;
+    return ok ? MF_OK : fail(MF_ERR_IO, "write to %s failed", path);
+}
+
+int mf_graph_load_binary(const char *path, mf_graph **out) {
+    if (!path || !out) return fail(MF_ERR_ARG, "path or out is NULL");
+    *out = nullptr;
+    FILE *f = fopen(path, "rb");
+    if (!f) return fail(MF_ERR_IO, "cannot open %s", path);
+    fseek(f, 0, SEEK_END);
+    long long S = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    CacheHead h{};
+    if (fread(&h, sizeof(h), 1, f) != 1 || memcmp(h.magic, kCacheMagic, 8) != 0 || h.version != 1 || h.n <= 0 ||
+        h.arcs < 0 || h.arcs > 0x7fffffffLL || h.R <= 0 || h.R > std::min(h.n, 1024) ||
+        h.bytes != cache_bytes(h.n, h.arcs, h.R) || S != h.bytes) {
+        fclose(f);
+        return fail(MF_ERR_IO, "%s is not a CSR cache of this library (or is truncated)", path);
+    }
+    const int n = h.n, R = h.R;
+    const i64 A = h.arcs;
+    mf_graph *g = nullptr;
+    int rc = new_graph(n, &g);
+    if (rc) {
+        fclose(f);
+        return rc;
+    }
+    std::vector<int> row(n + 1), rs(R + 1), nid(n), part(n), old(n, -1);
+    std::vector<double> score(n);
+    int *dbad = nullptr;
+    do {
+        const size_t AA = (size_t)std::max<i64>(A, 1);
+        if (cudaMalloc(&g->row, sizeof(int) * (n + 1)) || cudaMalloc(&g->col, sizeof(int) * AA) ||
+            cudaMalloc(&g->cap, sizeof(i64) * AA) || cudaMalloc(&g->rev, sizeof(int) * AA) ||
+            cudaMalloc(&g->fwd, AA) || cudaMalloc(&g->region_start, sizeof(int) * (R + 1)) ||
+            cudaMalloc(&g->region_of, sizeof(int) * n) || cudaMalloc(&dbad, sizeof(int))) {
+            cudaGetLastError();
+            rc = fail(MF_ERR_NOMEM, "graph allocation failed");
+            break;
+        }
+        // arc arrays and region ids stream to the device; the rest via the host
+        bool ok = fread(row.data(), 4, (size_t)n + 1, f) == (size_t)n + 1;
+        {
+            FileStream fs;
+            if (!fs.init(g->stream)) {
+                cudaGetLastError();
+                rc = fail(MF_ERR_NOMEM, "pinned staging failed");
+                break;
+            }
+            ok = ok && fs.copy(f, g->col, 4 * (size_t)A) == 4 * (size_t)A &&
+                 fs.copy(f, g->cap, 8 * (size_t)A) == 8 * (size_t)A &&
+                 fs.copy(f, g->rev, 4 * (size_t)A) == 4 * (size_t)A && fs.copy(f, g->fwd, (size_t)A) == (size_t)A;
+            ok = ok && fread(rs.data(), 4, (size_t)R + 1, f) == (size_t)R + 1;
+            ok = ok && fs.copy(f, g->region_of, 4 * (size_t)n) == 4 * (size_t)n;
+        }
+        ok = ok && fread(nid.data(), 4, n, f) == (size_t)n && fread(score.data(), 8, n, f) == (size_t)n &&
+             fread(part.data(), 4, n, f) == (size_t)n;
+        if (!ok) {
+            rc = fail(MF_ERR_IO, "read of %s failed", path);
+            break;
+        }
+        for (int x = 0; x < n && rc == MF_OK; ++x) {
+            int y = nid[x];
+            if (y < 0 || y >= n || old[y] != -1) rc = fail(MF_ERR_IO, "%s: new_id is not a permutation", path);
+            else old[y] = x;
+        }
+        // row and region monotonicity on the host (the device check indexes by them)
+        for (int x = 0; x < n && rc == MF_OK; ++x)
+            if (row[x] > row[x + 1]) rc = fail(MF_ERR_IO, "%s: row offsets decrease at %d", path, x);
+        for (int r = 0; r < R && rc == MF_OK; ++r)
+            if (rs[r] > rs[r + 1]) rc = fail(MF_ERR_IO, "%s: region starts decrease at %d", path, r);
+        if (rc) break;
+        if (cudaMemcpy(g->row, row.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(g->region_start, rs.data(), sizeof(int) * (R + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemset(dbad, 0, sizeof(int)) != cudaSuccess) {
+            rc = fail(MF_ERR_CUDA, "graph upload failed");
+            break;
+        }
+        k_check_csr<<<std::max(1, std::min(g->dev.ok ? g->dev.sms * 8 : 148 * 8, (n + 7) / 8)), 256, 0,
+                      g->stream>>>(n, A, R, g->row, g->col, g->cap, g->rev, g->fwd, g->region_start, g->region_of,
+                                   dbad);
+        int hbad = 0;
+        if (cudaMemcpyAsync(&hbad, dbad, sizeof(int), cudaMemcpyDeviceToHost, g->stream) != cudaSuccess ||
+            cudaStreamSynchronize(g->stream) != cudaSuccess) {
+            rc = fail(MF_ERR_CUDA, "cache check failed: %s", cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        if (hbad) {
+            rc = fail(MF_ERR_IO, "%s: %d inconsistencies in the stored CSR", path, hbad);
+            break;
+        }
+        g->arcs = A;
+        g->avg_deg = (int)(A / n);
+        g->R = R;
+        g->new_id.swap(nid);
+        g->old_id.swap(old);
+        g->score_caller.swap(score);
+        g->part_caller.swap(part);
+        rc = finalize_graph(g);
+    } while (0);
+    fclose(f);
+    cudaFree(dbad);
+    if (rc != MF_OK) {
+        mf_graph_destroy(g);
+        return rc;
+    }
+    g->pool.n = n;
+    g->pool.arcs = g->arcs;
+    g->pool.nhub = g->nhub;
+    *out = g;
+    return MF_OK;
+}
 
 int mf_debug_prune_mask(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, uint8_t *mask, int *kept) {
     if (!g || !mask) return fail(MF_ERR_ARG, "bad arguments");

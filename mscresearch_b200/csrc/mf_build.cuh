@@ -31,3 +31,27 @@ size_t mf_partition_scratch_bytes(int n, i64 arcs, int R);
 cudaError_t mf_partition_reorder(const BuildIn &in, const BuildOut &out, void *scratch,
                                  cudaStream_t st);
 void mf_exclusive_scan(int n, const int *in, int *out, int *tmp, cudaStream_t st);
+
+// Paired-arc CSR in input vertex order (mf_ingest.cu); device arrays.
+struct DevCsr {
+    int *row = nullptr;  // n+1
+    int *col = nullptr;
+    i64 *cap = nullptr;
+    int *rev = nullptr;
+    unsigned char *fwd = nullptr;
+    i64 arcs = 0;
+};
+// Edge triples read from graph.txt bytes on the device (mf_ingest.cu).
+struct TextEdges {
+    bool header_ok = false;  // the "n m" header scanned
+    int n = 0;
+    int m_header = 0;
+    i64 m = 0;  // triples read: min(m_header, complete triples before the stream ends)
+    int *u = nullptr, *v = nullptr;  // 0-based (file ids - 1)
+    i64 *c = nullptr;
+};
+cudaError_t mf_device_csr(int n, i64 m, const int *u, const int *v, const i64 *c, cudaStream_t st,
+                          DevCsr &out);
+void mf_free_dev_csr(DevCsr &c);
+cudaError_t mf_parse_graph_text(const unsigned char *txt, i64 S, cudaStream_t st, TextEdges &out);
+void mf_free_text_edges(TextEdges &t);

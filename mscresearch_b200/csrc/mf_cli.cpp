@@ -2,6 +2,7 @@
 // (Region_Aware_PR_with_Pruning_BoundaryCore.cu main, RA:2561-2933):
 //
 //   maxflow_b200 <input_dir> <output_dir> [static|dynamic] [--batch] [--R N]
+//                [--csr-cache FILE]
 //
 // Reads <input_dir>/graph.txt and test.txt (1-based ids), writes
 // <output_dir>/res_mt.txt (static) or res_dynamic.txt (dynamic), one
@@ -13,8 +14,12 @@
 //            divided evenly over the queries.
 //   dynamic  queries in windows of 10 (RA:2852), each window a resident
 //            session whose residual state stays on the GPU.
+//   --csr-cache FILE  load the partitioned graph from FILE (binary CSR
+//            cache) when it holds one with the same R; otherwise build it
+//            from graph.txt and write FILE.
 #include <sys/stat.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -32,16 +37,19 @@ static double now_ms() {
 
 int main(int argc, char **argv) {
     if (argc < 3) {
-        fprintf(stderr, "Usage: %s <input_dir> <output_dir> [mode] [--batch] [--R N]\n", argv[0]);
+        fprintf(stderr, "Usage: %s <input_dir> <output_dir> [mode] [--batch] [--R N] [--csr-cache FILE]\n",
+                argv[0]);
         fprintf(stderr, "  mode = static (default) | dynamic\n");
         return 1;
     }
     std::string in = argv[1], outd = argv[2], mode = "static";
     bool batch = false;
     int R = 128;  // RA:2583
+    std::string cache;
     for (int i = 3; i < argc; ++i) {
         if (!strcmp(argv[i], "--batch")) batch = true;
         else if (!strcmp(argv[i], "--R") && i + 1 < argc) R = atoi(argv[++i]);
+        else if (!strcmp(argv[i], "--csr-cache") && i + 1 < argc) cache = argv[++i];
         else mode = argv[i];
     }
     if (mode != "static" && mode != "dynamic") {
@@ -51,10 +59,31 @@ int main(int argc, char **argv) {
     mkdir(outd.c_str(), 0755);
     mf_graph *g = nullptr;
     double t0 = now_ms();
-    int rc = mf_graph_load_file((in + "/graph.txt").c_str(), R, &g);
-    if (rc != MF_OK) {
-        fprintf(stderr, "Cannot load %s/graph.txt: %s\n", in.c_str(), mf_last_error_string());
-        return 1;
+    int rc = MF_ERR_IO;
+    bool from_cache = false;
+    if (!cache.empty() && mf_graph_load_binary(cache.c_str(), &g) == MF_OK) {
+        int cn = 0, cR = 0;
+        long long ca = 0;
+        mf_graph_info(g, &cn, &ca, &cR);
+        // the R a build from graph.txt would use (0 -> 128, clamped to [1, min(n, 1024)])
+        int want = R <= 0 ? 128 : R;
+        want = std::min(std::min(want, cn), 1024);
+        if (cR == want) {
+            from_cache = true;
+            rc = MF_OK;
+        } else {
+            mf_graph_destroy(g);
+            g = nullptr;
+        }
+    }
+    if (!from_cache) {
+        rc = mf_graph_load_file((in + "/graph.txt").c_str(), R, &g);
+        if (rc != MF_OK) {
+            fprintf(stderr, "Cannot load %s/graph.txt: %s\n", in.c_str(), mf_last_error_string());
+            return 1;
+        }
+        if (!cache.empty() && mf_graph_save(g, cache.c_str()) != MF_OK)
+            fprintf(stderr, "Cannot write the CSR cache %s: %s\n", cache.c_str(), mf_last_error_string());
     }
     int n = 0, Rg = 0;
     long long arcs = 0;

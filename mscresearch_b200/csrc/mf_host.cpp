@@ -289,13 +289,19 @@ struct Scanner {
             ++q;
         }
         if (q >= e || !isdigit((unsigned char)*q)) return false;
+        // magnitude saturates at the limit of its sign, as strtoll does
+        const unsigned long long lim = neg ? (1ull << 63) : (1ull << 63) - 1ull;
         unsigned long long x = 0;
+        bool over = false;
         while (q < e && isdigit((unsigned char)*q)) {
-            x = x * 10 + (unsigned)(*q - '0');
+            const unsigned long long d = (unsigned)(*q - '0');
+            if (x > (lim - d) / 10ull) over = true;
+            else x = x * 10ull + d;
             ++q;
         }
+        if (over) x = lim;
         p = q;
-        out = neg ? -(long long)x : (long long)x;
+        out = (long long)(neg ? (~x + 1ull) : x);
         return true;
     }
 };
@@ -338,8 +344,8 @@ int mf_read_graph_txt(const char *path, int *n, long long *m_read, int32_t *u, i
     for (long long i = 0; i < m && k < cap_len; ++i) {
         long long x, y, c;
         if (!sc.next(x) || !sc.next(y) || !sc.next(c)) break;
-        u[k] = (int32_t)(x - 1);
-        v[k] = (int32_t)(y - 1);
+        u[k] = (int32_t)((uint32_t)x - 1u);
+        v[k] = (int32_t)((uint32_t)y - 1u);
         cap[k] = c;
         ++k;
     }
@@ -347,17 +353,5 @@ int mf_read_graph_txt(const char *path, int *n, long long *m_read, int32_t *u, i
     return MF_OK;
 }
 
-int mf_graph_load_file(const char *path, int R, mf_graph **out) {
-    int n = 0;
-    long long m = 0;
-    if (mf_graph_txt_header(path, &n, &m) != MF_OK) return MF_ERR_IO;
-    if (n <= 0 || m < 0) return MF_ERR_IO;
-    std::vector<int32_t> u(m > 0 ? m : 1), v(m > 0 ? m : 1);
-    std::vector<int64_t> c(m > 0 ? m : 1);
-    long long got = 0;
-    int rc = mf_read_graph_txt(path, &n, &got, u.data(), v.data(), c.data(), m);
-    if (rc != MF_OK) return rc;
-    return mf_graph_create_from_edges(n, got, u.data(), v.data(), c.data(), R, out);
-}
 
 }  // extern "C"
