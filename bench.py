@@ -536,7 +536,11 @@ def run_gridsets(args):
                         "traffic": None, "peak_kind": kind, "alg_bytes_per_launch": alg_bytes},
            "batched": {"p50_ms": pct(finish, 50), "p99_ms": pct(finish, 99),
                        "global_relabels": int(sum(x.global_relabels for x in sts)),
-                       "rounds": int(sum(x.rounds for x in sts))},
+                       "rounds": int(sum(x.rounds for x in sts)),
+                       "per_query_mean": {k: round(float(np.mean([getattr(x, k) for x in sts])), 2) for k in (
+                           "service_ms", "prune_ms", "relabel_ms", "rounds_ms", "rounds", "global_relabels",
+                           "levels", "levels_bottom_up", "levels_solo", "arcs_examined", "relabel_arcs",
+                           "vertices_examined", "pushes", "mask_vertices", "mask_arcs")}},
            "clocks": clk.summary()}
     if not args.no_cpu and rank == 0:
         # oracle Dinic on a graph built for each sampled terminal set

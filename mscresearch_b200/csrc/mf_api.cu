@@ -237,6 +237,8 @@ struct mf_graph {
     int nhub = 0;  // vertices with more than HUB_T arcs
     int pivot = 0;  // internal id of the highest-degree vertex (kept-set cache pivot)
     int *hubs = nullptr;  // device: internal ids of the hubs
+    int ngiant = 0;       // vertices with more than GIANT_T arcs
+    int *giants = nullptr;  // device: their internal ids
     std::vector<int> deg_host;                // internal id -> arcs
     std::vector<unsigned char> kc_in_host;    // internal id -> in the cached component
     // kept-set cache (see DGraph)
@@ -313,6 +315,9 @@ void free_graph_arrays(mf_graph *g) {
     cudaFree(g->d_graph);
     cudaFree(g->hubs);
     g->hubs = nullptr;
+    cudaFree(g->giants);
+    g->giants = nullptr;
+    g->ngiant = 0;
     g->row = g->col = g->rev = g->region_of = g->region_start = nullptr;
     g->cap = nullptr;
     g->fwd = nullptr;
@@ -331,6 +336,8 @@ DGraph make_dgraph(const mf_graph *g) {
     dg.region_of = g->region_of;
     dg.hubs = g->hubs;
     dg.nhub = g->hubs ? g->nhub : 0;
+    dg.giants = g->giants;
+    dg.ngiant = g->giants ? g->ngiant : 0;
     if (g->kc_valid) {
         dg.kc_in = g->kc_in;
         dg.kc_fb = g->kc_fb;
@@ -415,7 +422,7 @@ int finalize_graph(mf_graph *g) {
     const int n = g->n;
     int best = 0;
     {
-        std::vector<int> rw(n + 1), hl;
+        std::vector<int> rw(n + 1), hl, gl;
         CK(cudaMemcpy(rw.data(), g->row, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
         for (int x = 1; x < n; ++x)
             if (rw[x + 1] - rw[x] > rw[best + 1] - rw[best]) best = x;
@@ -423,11 +430,17 @@ int finalize_graph(mf_graph *g) {
         for (int x = 0; x < n; ++x) {
             g->deg_host[x] = rw[x + 1] - rw[x];
             if (rw[x + 1] - rw[x] > HUB_T) hl.push_back(x);
+            if (rw[x + 1] - rw[x] > GIANT_T) gl.push_back(x);
         }
         g->nhub = (int)hl.size();
         if (!hl.empty()) {
             CK(cudaMalloc(&g->hubs, sizeof(int) * hl.size()));
             CK(cudaMemcpy(g->hubs, hl.data(), sizeof(int) * hl.size(), cudaMemcpyHostToDevice));
+        }
+        g->ngiant = (int)gl.size();
+        if (!gl.empty()) {
+            CK(cudaMalloc(&g->giants, sizeof(int) * gl.size()));
+            CK(cudaMemcpy(g->giants, gl.data(), sizeof(int) * gl.size(), cudaMemcpyHostToDevice));
         }
     }
     g->pivot = best;

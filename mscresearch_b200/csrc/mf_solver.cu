@@ -109,6 +109,8 @@ struct QCtx {
     const int *row, *col, *rev, *rof;
     const i64 *cap;
     const DGraph *gr;
+    const int *giants;  // the graph's giant list (gr->giants), ngiant entries
+    int ngiant;
     // slot
     DSlot st;
     int vf;  // kept vertices in the front part of vlist (the rest are at the back)
@@ -126,6 +128,8 @@ struct QCtx {
     int bu_factor;  // direction switch of the searches (KOpts::bu_factor)
 
     __device__ bool sync() { return gsync(G, bar, err, lim); }
+    // a vertex with arcs [b, e1) that for_giants covers
+    __device__ __forceinline__ bool giant(int b, int e1) const { return giants && e1 - b > GIANT_T; }
     // barrier that also returns the front and back tails of list bank `bank`
     // as of the barrier
     __device__ bool sync_tails(int bank, int &ft, int &bt) {
@@ -493,6 +497,21 @@ __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, i
     return true;
 }
 
+// The giants selected by sel(v) (uniform over the group), each with its
+// arcs spread over all the group's threads: pv(v, b, e1) once per giant by
+// the group's thread 0, pa(v, e) per arc.
+template <class Sel, class PerV, class PerArc>
+__device__ void for_giants(QCtx &c, Sel sel, PerV pv, PerArc pa) {
+    const int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+    for (int k = 0; k < c.ngiant; ++k) {
+        const int v = ldro(&c.giants[k]);
+        if (!sel(v)) continue;
+        const int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+        if (gt == 0) pv(v, b, e1);
+        for (int e = b + gt; e < e1; e += gT) pa(v, e);
+    }
+}
+
 struct NoCand {
     __device__ int operator()(int) const { return -1; }
 };
@@ -777,6 +796,8 @@ __device__ bool fix_extra_arcs(QCtx &c, unsigned M, int nv) {
     for (int i = c.gw; i < xf + nb; i += c.gW) {
         int v = i < xf ? ldcg(&c.st.vlist[g.kc_f + i]) : back_at(c, c.st.vlist, g.kc_b + (i - xf));
         int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+        if (c.lane == 0) c.w_verts += 1;
+        if (c.giant(b, e1)) continue;
         for (int e = b + c.lane; e < e1; e += 32) {
             int w = ldro(&c.col[e]);
             bool kw = ldcg(&c.st.mark[w]) >= M;
@@ -786,8 +807,19 @@ __device__ bool fix_extra_arcs(QCtx &c, unsigned M, int nv) {
                 c.st.res[r] = ldro(&c.cap[r]);
             }
         }
-        if (c.lane == 0) c.w_verts += 1;
     }
+    // giant extras: kept and outside the cached component
+    for_giants(
+        c, [&](int v) { return ldcg(&c.st.mark[v]) >= M && !ldro_u8(&g.kc_in[v]); }, [&](int, int, int) {},
+        [&](int, int e) {
+            int w = ldro(&c.col[e]);
+            bool kw = ldcg(&c.st.mark[w]) >= M;
+            c.st.res[e] = kw ? ldro(&c.cap[e]) : 0;
+            if (kw) {
+                int r = ldro(&c.rev[e]);
+                c.st.res[r] = ldro(&c.cap[r]);
+            }
+        });
     return c.sync();
 }
 
@@ -810,9 +842,56 @@ __device__ bool apply_overrides(QCtx &c, const KParams &p, int q, unsigned M) {
 // ---------------------------------------------------------------------------
 // Fresh residual state over the kept vertices: excess 0; res[e] = cap[e]
 // when the head is kept, else 0 (the arc is outside the induced subgraph).
-__device__ bool init_state(QCtx &c, int nv, unsigned M) {
+// count_mask: add the kept vertices' arcs to the query's mask-arc total.
+__device__ bool init_state(QCtx &c, int nv, unsigned M, bool count_mask = true) {
     MF_TRACE(30, nv);
     i64 mask_arcs = 0;
+    if ((i64)nv * 2 > c.n) {
+        // Most vertices kept: a thread per kept vertex for its resets, then
+        // one coalesced sweep over every arc of the graph (four per thread;
+        // arcs whose tail was dropped are never read, so their value does
+        // not matter).  A warp per vertex would walk ~10-arc lists with
+        // dependent loads.
+        const int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+        for (int i = gt; i < nv; i += gT) {
+            int v = c.vat(i);
+            c.st.ex[v] = 0;
+            c.st.h[v] = 0;
+            mask_arcs += c.deg(v);
+            c.w_verts += 1;
+        }
+        const i64 A = ldro(&c.row[c.n]);
+        // 16-byte vectors only on 16-byte aligned arrays (a caller-held CSR
+        // need not be)
+        const bool vec = ((reinterpret_cast<uintptr_t>(c.col) | reinterpret_cast<uintptr_t>(c.cap) |
+                           reinterpret_cast<uintptr_t>(c.st.res)) & 15) == 0;
+        const i64 nq4 = vec ? (A >> 2) : 0;
+        const int4 *col4 = reinterpret_cast<const int4 *>(c.col);
+        const longlong2 *cap2 = reinterpret_cast<const longlong2 *>(c.cap);
+        longlong2 *res2 = reinterpret_cast<longlong2 *>(c.st.res);
+        const unsigned *mark = c.st.mark;
+        i64 swept = 0;
+        for (i64 k = gt; k < nq4; k += gT) {
+            const int4 w = __ldg(&col4[k]);
+            const longlong2 ca = __ldg(&cap2[2 * k]), cb = __ldg(&cap2[2 * k + 1]);
+            longlong2 ra, rb;
+            ra.x = ldcg(&mark[w.x]) >= M ? ca.x : 0;
+            ra.y = ldcg(&mark[w.y]) >= M ? ca.y : 0;
+            rb.x = ldcg(&mark[w.z]) >= M ? cb.x : 0;
+            rb.y = ldcg(&mark[w.w]) >= M ? cb.y : 0;
+            res2[2 * k] = ra;
+            res2[2 * k + 1] = rb;
+            swept += 4;
+        }
+        for (i64 e = 4 * nq4 + gt; e < A; e += gT) {
+            c.st.res[e] = ldcg(&mark[ldro(&c.col[e])]) >= M ? ldro(&c.cap[e]) : 0;
+            ++swept;
+        }
+        c.w_arcs += swept;
+        mask_arcs = warp_sum_i64(mask_arcs);
+        if (count_mask && c.lane == 0 && mask_arcs) atomic_add_i64(&c.st.acc[ACC_TOT + T_MASKARCS], mask_arcs);
+        return c.sync();
+    }
     for (int i = c.gw; i < nv; i += c.gW) {
         int v = c.vat(i);
         int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
@@ -820,17 +899,21 @@ __device__ bool init_state(QCtx &c, int nv, unsigned M) {
             c.st.ex[v] = 0;
             c.st.h[v] = 0;
         }
-        for (int e = b + c.lane; e < e1; e += 32) {
-            int w = ldro(&c.col[e]);
-            c.st.res[e] = (ldcg(&c.st.mark[w]) >= M) ? ldro(&c.cap[e]) : 0;
-        }
         mask_arcs += e1 - b;
         if (c.lane == 0) {
             c.w_arcs += e1 - b;
             c.w_verts += 1;
         }
+        if (c.giant(b, e1)) continue;
+        for (int e = b + c.lane; e < e1; e += 32) {
+            int w = ldro(&c.col[e]);
+            c.st.res[e] = (ldcg(&c.st.mark[w]) >= M) ? ldro(&c.cap[e]) : 0;
+        }
     }
-    if (c.lane == 0 && mask_arcs) atomic_add_i64(&c.st.acc[ACC_TOT + T_MASKARCS], mask_arcs);
+    if (count_mask && c.lane == 0 && mask_arcs) atomic_add_i64(&c.st.acc[ACC_TOT + T_MASKARCS], mask_arcs);
+    for_giants(
+        c, [&](int v) { return ldcg(&c.st.mark[v]) >= M; }, [&](int, int, int) {},
+        [&](int, int e) { c.st.res[e] = (ldcg(&c.st.mark[ldro(&c.col[e])]) >= M) ? ldro(&c.cap[e]) : 0; });
     return c.sync();
 }
 
@@ -1805,20 +1888,26 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
 __device__ bool certify(QCtx &c, int s, int t, int nv, unsigned M, i64 flow, QOut &qo, int &status) {
     i64 *ab = c.take_abank();
     i64 bad = 0;
+    auto arc_ok = [&](int e) -> int {
+        int w = ldro(&c.col[e]);
+        i64 r = ldcg(&c.st.res[e]);
+        int nb = r < 0;
+        if (ldcg(&c.st.mark[w]) >= M) {
+            int re = ldro(&c.rev[e]);
+            if (r + ldcg(&c.st.res[re]) != ldro(&c.cap[e]) + ldro(&c.cap[re])) ++nb;
+        }
+        return nb;
+    };
     for (int i = c.gw; i < nv; i += c.gW) {
         int v = c.vat(i);
         if (c.lane == 0 && v != s && v != t && ldcg(&c.st.ex[v]) != 0) ++bad;
         int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
-        for (int e = b + c.lane; e < e1; e += 32) {
-            int w = ldro(&c.col[e]);
-            i64 r = ldcg(&c.st.res[e]);
-            if (r < 0) ++bad;
-            if (ldcg(&c.st.mark[w]) >= M) {
-                int re = ldro(&c.rev[e]);
-                if (r + ldcg(&c.st.res[re]) != ldro(&c.cap[e]) + ldro(&c.cap[re])) ++bad;
-            }
-        }
+        if (c.giant(b, e1)) continue;
+        for (int e = b + c.lane; e < e1; e += 32) bad += arc_ok(e);
     }
+    for_giants(
+        c, [&](int v) { return ldcg(&c.st.mark[v]) >= M; }, [&](int, int, int) {},
+        [&](int, int e) { bad += arc_ok(e); });
     bad = warp_sum_i64(bad);
     if (c.lane == 0 && bad) atomic_add_i64(&ab[A_BAD], bad);
     // full-graph backward BFS from t
@@ -1845,14 +1934,18 @@ __device__ bool certify(QCtx &c, int s, int t, int nv, unsigned M, i64 flow, QOu
     if (!bfs_levels(c, c.st.qa, bk, f0, b0, cut_bfs)) return false;
     // cut capacity over all vertices
     i64 cut = 0;
+    auto cut_arc = [&](int e) -> i64 {
+        i64 cp = ldro(&cap[e]);
+        return (cp > 0 && ldcg(&qm[ldro(&c.col[e])]) == Z) ? cp : 0;
+    };
     for (int v = c.gw; v < c.n; v += c.gW) {
         if (ldcg(&qm[v]) == Z) continue;
         int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
-        for (int e = b + c.lane; e < e1; e += 32) {
-            i64 cp = ldro(&cap[e]);
-            if (cp > 0 && ldcg(&qm[ldro(&c.col[e])]) == Z) cut += cp;
-        }
+        if (c.giant(b, e1)) continue;
+        for (int e = b + c.lane; e < e1; e += 32) cut += cut_arc(e);
     }
+    for_giants(
+        c, [&](int v) { return ldcg(&qm[v]) != Z; }, [&](int, int, int) {}, [&](int, int e) { cut += cut_arc(e); });
     cut = warp_sum_i64(cut);
     if (c.lane == 0 && cut) atomic_add_i64(&ab[A_CUT], cut);
     if (!c.sync()) return false;
@@ -1869,12 +1962,19 @@ __device__ bool write_full_residual(QCtx &c, unsigned M, i64 *out) {
     for (int v = c.gw; v < c.n; v += c.gW) {
         bool kv = ldcg(&c.st.mark[v]) >= M;
         int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
+        if (c.giant(b, e1)) continue;
         for (int e = b + c.lane; e < e1; e += 32) {
             int w = ldro(&c.col[e]);
             bool kept = kv && ldcg(&c.st.mark[w]) >= M;
             out[e] = kept ? ldcg(&c.st.res[e]) : ldro(&c.cap[e]);
         }
     }
+    for_giants(
+        c, [&](int) { return true; }, [&](int, int, int) {},
+        [&](int v, int e) {
+            bool kept = ldcg(&c.st.mark[v]) >= M && ldcg(&c.st.mark[ldro(&c.col[e])]) >= M;
+            out[e] = kept ? ldcg(&c.st.res[e]) : ldro(&c.cap[e]);
+        });
     return c.sync();
 }
 
@@ -1958,6 +2058,18 @@ __device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int
     if (!c.sync()) return false;
     // fresh state for new vertices; reopen their arc pairs
     i64 add_arcs = 0;
+    auto open_arc = [&](int e) {
+        int w = ldro(&c.col[e]);
+        if (ldcg(&mark[w]) == Mn) {
+            c.st.res[e] = ldro(&cap[e]);
+            if (ldcg(&claim[w]) == O) {
+                int re = ldro(&rev[e]);
+                c.st.res[re] = ldro(&cap[re]);
+            }
+        } else {
+            c.st.res[e] = 0;
+        }
+    };
     for (int i = vf_old + c.gw; i < vf_new; i += c.gW) {
         int v = ldcg(&c.st.vlist[i]);
         int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
@@ -1965,20 +2077,14 @@ __device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int
             c.st.ex[v] = 0;
             c.st.h[v] = 0;
         }
-        for (int e = b + c.lane; e < e1; e += 32) {
-            int w = ldro(&c.col[e]);
-            if (ldcg(&mark[w]) == Mn) {
-                c.st.res[e] = ldro(&cap[e]);
-                if (ldcg(&claim[w]) == O) {
-                    int re = ldro(&rev[e]);
-                    c.st.res[re] = ldro(&cap[re]);
-                }
-            } else {
-                c.st.res[e] = 0;
-            }
-        }
         add_arcs += e1 - b;
+        if (c.giant(b, e1)) continue;
+        for (int e = b + c.lane; e < e1; e += 32) open_arc(e);
     }
+    // new giants: kept now (Mn) and not among the old kept vertices (O)
+    for_giants(
+        c, [&](int v) { return ldcg(&mark[v]) == Mn && ldcg(&claim[v]) != O; }, [&](int, int, int) {},
+        [&](int, int e) { open_arc(e); });
     if (c.lane == 0 && add_arcs) atomic_add_i64(&c.st.acc[ACC_TOT + T_MASKARCS], add_arcs);
     if (!c.sync()) return false;
     // capacity deltas on kept arcs (forward arcs of changed edges)
@@ -2109,7 +2215,13 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
             return;
         }
         if (t_reach && nv > 0) {
-            if (kc_case) {
+            const int nimg = g.kc_f + g.kc_b;
+            if (kc_case == 2 && nv - nimg > nimg) {
+                // the extras outnumber the cached component: a fresh init
+                // costs less than the image copy plus the extras' fix-up
+                // (their arcs are already in the mask-arc total)
+                if (!init_state(c, nv, M, false)) return;
+            } else if (kc_case) {
                 // initial residuals of the component, copied whole (16-byte
                 // vectors); ex/h were set with the kept list above
                 const longlong2 *src = reinterpret_cast<const longlong2 *>(g.kc_res);
@@ -2282,6 +2394,8 @@ __global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
         c.rof = g.region_of;
         c.cap = g.cap;
         c.gr = &p.graphs[gi];
+        c.giants = g.giants;
+        c.ngiant = g.giants ? g.ngiant : 0;
         c.st = p.slots[si];
         c.clock = ldcg(c.st.clock);
         c.q_begin = globaltimer_ns();

@@ -31,7 +31,17 @@ struct DGraph {
     const unsigned char *kc_fb;
     int kc_f, kc_b;
     i64 kc_arcs;                 // arcs out of the component's vertices
+    // Vertices with more than GIANT_T arcs (NULL: none listed; warp-per-vertex
+    // loops then take every vertex themselves).
+    const int *giants;
+    int ngiant;
 };
+
+// Vertices with more arcs than this are "giants": loops that give each
+// vertex one warp (state init, certificate, residual export) skip them and
+// spread their arcs over every thread of the group instead -- one warp
+// walking a 4-million-arc super terminal took ~150 ms.
+#define GIANT_T 4096
 
 // Vertices with more arcs than this are "hubs": worklists keep them at the
 // back and their arcs are processed in 32-arc chunks by all warps of a group.

@@ -280,3 +280,67 @@ def test_batch_override_terminal_sets():
             eg.solve_batch_override([S], [T], tu[:1], tv[:1], [[256]])
         with pytest.raises(mf.MaxflowError):
             eg.solve_batch_override([S], [T], tu[:1], tv[:1], [[1]], o=mf.opts(certify=1))
+
+
+def _giant_graph(seed):
+    """s -> two giants (> 4096 arcs each) -> 12000 leaves -> t, leaves also
+    back to the giants and to each other (so the giants sit in a strongly
+    connected component); random capacities."""
+    rng = np.random.default_rng(seed)
+    L = 12000
+    s, g1, g2, t = 0, 1, 2, 3
+    leaves = np.arange(4, 4 + L, dtype=np.int32)
+    n = 4 + L
+    u = [np.array([s, s], np.int32), np.full(L, g1, np.int32), np.full(L // 2, g2, np.int32), leaves,
+         leaves[:L // 3], leaves[1:]]
+    v = [np.array([g1, g2], np.int32), leaves, leaves[L // 2:], np.full(L, t, np.int32),
+         np.full(L // 3, g1, np.int32), leaves[:-1]]
+    u, v = np.concatenate(u), np.concatenate(v)
+    c = rng.integers(1, 60, len(u)).astype(np.int64)
+    c[:2] = rng.integers(50000, 200000, 2)
+    return n, u, v, c, s, t, g1, g2
+
+
+def test_giant_vertices_init_certify_residual():
+    n, u, v, c, s, t, g1, g2 = _giant_graph(5)
+    g = O.build_csr(n, u, v, c)
+    qs = [s, g1, 10, g1, s]
+    qt = [t, t, t, 500, 700]
+    exp = oracle_flows(g, qs, qt)
+    with mf.Graph.from_edges(n, u, v, c, R=8) as eg:
+        for kc in (1, 0):
+            o = mf.opts(use_kept_cache=kc)
+            assert list(eg.solve_batch(qs, qt, o)) == exp, kc
+            assert [eg.solve(a, b, o)[0] for a, b in zip(qs, qt)] == exp, kc
+        ex = eg.export()
+        gi = O.CSR(n, ex["row"], ex["col"], ex["cap"], ex["rev"])
+        nid = ex["new_id"]
+        for a, b, e in zip(qs, qt, exp):
+            f, res, st = eg.solve_residual(a, b)
+            rc, cut = O.certify(gi, nid[a], nid[b], res, f, require_flow=False)
+            assert f == e and rc == 0 and cut == f, (a, b)
+            fc, stc = eg.certify(a, b)
+            assert fc == e and stc.cut_capacity == e and stc.status == 0, (a, b)
+
+
+def test_giant_vertices_session_repair():
+    """A giant leaves and re-enters a resident query's kept set through
+    capacity updates; every answer equals a fresh solve of the updated graph."""
+    n, u, v, c, s, t, g1, g2 = _giant_graph(6)
+    g = O.build_csr(n, u, v, c)
+    fwd = g.cap > 0
+    with mf.Graph.from_edges(n, u, v, c, R=8) as eg:
+        ss = mf.Session(eg, [s, g1], [t, t])
+        assert list(ss.solve()) == oracle_flows(g, [s, g1], [t, t])
+        for du in ([-int(c[0]), -int(c[1])], [7, 0], [0, 90000], [-3, 5]):
+            uu = np.array([s, s], np.int32)
+            vv = np.array([g1, g2], np.int32)
+            d = np.array(du, np.int64)
+            fr = ss.update(uu, vv, d)
+            for a, b, dd in zip(uu, vv, d):
+                es = [e for e in range(g.row[a], g.row[a + 1]) if g.col[e] == b and fwd[e]]
+                g.cap[es[0]] = max(0, g.cap[es[0]] + dd)
+            exp = oracle_flows(g, [s, g1], [t, t])
+            assert list(fr) == exp, du
+            assert list(eg.solve_batch([s, g1], [t, t])) == exp, du
+        ss.close()
