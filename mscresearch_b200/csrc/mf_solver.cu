@@ -324,21 +324,43 @@ __device__ void bu_level(QCtx &c, int *Q, int bank, int level, int nuf, UF uf, i
     const int tile = c.lane >> 3, tb = tile << 3, tl = c.lane & 7;
     const unsigned tmask = 0xffu << tb;
     i64 arcs = 0;
-    for (int base = c.gw * 32; base < nuf; base += c.gW * 32) {
-        int i = base + c.lane;
-        int w = i < nuf ? uf(i) : -1;
+    // Software-pipelined over the warp's steps: the next step's candidate
+    // and its row bounds are loaded while this step's arcs are in flight,
+    // so a step waits on about three memory latencies instead of five.
+    const int stride = c.gW * 32;
+    int w_nx = -1, b_nx = 0, e_nx = 0;
+    {
+        const int i = c.gw * 32 + c.lane;
+        if (c.gw * 32 < nuf && i < nuf) w_nx = uf(i);
+        if (w_nx >= 0) {
+            b_nx = ldro(&c.row[w_nx]);
+            e_nx = ldro(&c.row[w_nx + 1]);
+        }
+    }
+    for (int base = c.gw * 32; base < nuf; base += stride) {
+        const int w = w_nx, b = b_nx, e1 = e_nx;
         if (c.lane == 0) c.w_verts += min(32, nuf - base);
         // lane pass: every lane tests its own candidate's first BU_PRE arcs
         // (independent loads, 32 candidates at once); only candidates with
         // more arcs and no parent among those go on to the 8-lane tiles
+        int xs[BU_PRE];
+#pragma unroll
+        for (int k = 0; k < BU_PRE; ++k) xs[k] = (w >= 0 && b + k < e1) ? ldro(&c.col[b + k]) : 0;
+        {
+            const int i = base + stride + c.lane;
+            w_nx = (base + stride < nuf && i < nuf) ? uf(i) : -1;
+            if (w_nx >= 0) {
+                b_nx = ldro(&c.row[w_nx]);
+                e_nx = ldro(&c.row[w_nx + 1]);
+            }
+        }
         bool claimed1 = false, more = false;
         if (w >= 0) {
-            const int b = ldro(&c.row[w]), e1 = ldro(&c.row[w + 1]);
             bool hit = false;
 #pragma unroll
             for (int k = 0; k < BU_PRE; ++k) {
                 const int e = b + k;
-                if (e < e1) hit |= par(w, e, ldro(&c.col[e]), level);
+                if (e < e1) hit |= par(w, e, xs[k], level);
             }
             arcs += min(BU_PRE, e1 - b);
             if (hit) claimed1 = set(w, level);
@@ -973,7 +995,10 @@ __device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &de
         return unvisited(w) ? w : -1;
     };
     auto par = [&](int w, int e, int x, int level) -> bool {
-        return ldcg(&res[e]) > 0 && ((ldcg(&fmap(level)[x >> 5]) >> (x & 31)) & 1u);
+        // both loads issued together (the frontier word is in L2)
+        const i64 r = ldcg(&res[e]);
+        const unsigned fw = ldcg(&fmap(level)[x >> 5]);
+        return r > 0 && ((fw >> (x & 31)) & 1u);
     };
     auto set = [&](int w, int level) -> bool {
         const unsigned bit = 1u << (w & 31);
