@@ -251,22 +251,37 @@ __device__ void td_level(QCtx &c, int *Q, int bank, int flo, int fhi, int blo, i
     // 1 to 32 each), their arcs balanced over the lanes
     const int nf = fhi - flo;
     const int vpw = max(1, min(32, (nf + gW - 1) / gW));
-    for (int base = flo + gw * vpw; base < fhi; base += gW * vpw) {
-        int i = base + c.lane;
-        int v = 0, b = 0, d = 0;
-        if (c.lane < vpw && i < fhi) {
-            v = ldcg(&Q[i]);
-            if (MF_OK_IDX(v, c.n, 11)) {
-                b = ldro(&c.row[v]);
-                d = ldro(&c.row[v + 1]) - b;
-            }
-        }
+    const int stride = gW * vpw;
+    // software-pipelined: the next step's frontier vertex is loaded before
+    // this step's scan and its row bounds before this step's arcs
+    int v_nx = 0;
+    {
+        const int i = flo + gw * vpw + c.lane;
+        if (c.lane < vpw && i < fhi) v_nx = ldcg(&Q[i]);
+    }
+    bool have_nx = c.lane < vpw && flo + gw * vpw + c.lane < fhi;
+    int b_nx = 0, d_nx = 0;
+    if (have_nx && MF_OK_IDX(v_nx, c.n, 11)) {
+        b_nx = ldro(&c.row[v_nx]);
+        d_nx = ldro(&c.row[v_nx + 1]) - b_nx;
+    }
+    for (int base = flo + gw * vpw; base < fhi; base += stride) {
+        const int v = v_nx, b = b_nx, d = d_nx;
+        const int i2 = base + stride + c.lane;
+        have_nx = c.lane < vpw && i2 < fhi;
+        if (have_nx) v_nx = ldcg(&Q[i2]);
         int incl = warp_incl_scan_int(d);
         int total = __shfl_sync(MF_FULL, incl, 31);
         sv[c.lane] = v;
         sb[c.lane] = b;
         sx[c.lane] = incl - d;
         __syncwarp();
+        b_nx = 0;
+        d_nx = 0;
+        if (have_nx && MF_OK_IDX(v_nx, c.n, 11)) {
+            b_nx = ldro(&c.row[v_nx]);
+            d_nx = ldro(&c.row[v_nx + 1]) - b_nx;
+        }
         for (int k = 0; k < total; k += 32) {
             int j = k + c.lane;
             bool ok = false;
