@@ -1162,26 +1162,20 @@ __device__ __forceinline__ bool enlist(QCtx &c, int w, unsigned rstamp) {
 // all arcs, v is relabeled to 1 + the lowest height over arcs that still
 // have residual (n when none).  Newly active heads and v itself (if still
 // active) are appended to N.
+//
+// The caller passes v's arc range [b, e1), height hv and excess ev, the
+// same values on every lane of the tile (read by one lane and broadcast):
+// they steer tile-wide branches, and under independent thread scheduling
+// per-lane loads could disagree (another warp may raise ex[v] meanwhile)
+// and split the tile across its shuffles.  An excess read early is a lower
+// bound (only this tile lowers ex[v]); the height is exact (only the owner
+// relabels v during rounds).
 template <int TW>
-__device__ void discharge_tile(QCtx &c, int v, int K, int sinkv, int blockv, int *N, int nbk,
-                               unsigned rstamp, i64 *ab, unsigned mask, int tb) {
+__device__ void discharge_tile(QCtx &c, int v, int b, int e1, int hv, i64 ev, int K, int sinkv, int blockv,
+                               int *N, int nbk, unsigned rstamp, i64 *ab, unsigned mask, int tb) {
     const int n = c.n;
     const int tl = c.lane - tb;  // lane within the tile
     MF_TRACE(50, v);
-    // Height and excess steer tile-wide branches below: read them once on
-    // the tile's first lane and broadcast.  Under independent thread
-    // scheduling the lanes need not load at the same moment, and another warp
-    // may change h[v] / ex[v] in between; per-lane copies could then disagree
-    // and split the tile across its shuffles.
-    int hv = 0;
-    i64 ev = 0;
-    if (tl == 0) {
-        hv = ldcg(&c.st.h[v]);
-        ev = ldcg(&c.st.ex[v]);
-    }
-    hv = __shfl_sync(mask, hv, 0, TW);
-    ev = __shfl_sync(mask, ev, 0, TW);
-    int b = ldro(&c.row[v]), e1 = ldro(&c.row[v + 1]);
     i64 pushes = 0, arcs = 0;
     for (int cyc = 0; cyc < K; ++cyc) {
         if (ev <= 0 || hv >= n) break;
@@ -1256,7 +1250,16 @@ __device__ void discharge_tile(QCtx &c, int v, int K, int sinkv, int blockv, int
 
 __device__ __forceinline__ void discharge_vertex(QCtx &c, int v, int K, int sinkv, int blockv, int *N,
                                                  int nbk, unsigned rstamp, i64 *ab) {
-    discharge_tile<32>(c, v, K, sinkv, blockv, N, nbk, rstamp, ab, MF_FULL, 0);
+    int hv = 0;
+    i64 ev = 0;
+    if (c.lane == 0) {
+        hv = ldcg(&c.st.h[v]);
+        ev = ldcg(&c.st.ex[v]);
+    }
+    hv = __shfl_sync(MF_FULL, hv, 0);
+    ev = __shfl_sync(MF_FULL, ev, 0);
+    discharge_tile<32>(c, v, ldro(&c.row[v]), ldro(&c.row[v + 1]), hv, ev, K, sinkv, blockv, N, nbk, rstamp, ab,
+                       MF_FULL, 0);
 }
 
 // Discharge of the front part L[0, nf): each warp takes 32 entries.
@@ -1266,18 +1269,42 @@ __device__ __forceinline__ void discharge_vertex(QCtx &c, int v, int K, int sink
 // round.  hot != NULL restricts the pass to vertices of hot regions.
 __device__ void discharge_front(QCtx &c, const int *L, int nf, int K, int sinkv, int blockv,
                                 int *N, int nbk, unsigned rstamp, i64 *ab, const int *hot) {
-    for (int base = c.gw * 32; base < nf; base += c.gW * 32) {
-        int i = base + c.lane;
-        int v = -1, d = 0;
-        if (i < nf) {
+    // Software-pipelined: each lane loads the next step's entry, and then
+    // its arc range, height and excess, while this step's tiles work.
+    const int stride = c.gW * 32;
+    auto entry = [&](int base) -> int {
+        const int i = base + c.lane;
+        int v = -1;
+        if (base < nf && i < nf) {
             v = ldcg(&L[i]);
             if (!MF_OK_IDX(v, c.n, 12)) v = -1;
             else if (hot && !ldcg(&hot[ldro(&c.rof[v])])) v = -1;
         }
-        if (v >= 0) d = c.deg(v);
+        return v;
+    };
+    int v_nx = entry(c.gw * 32);
+    int b_nx = 0, e_nx = 0, h_nx = 0;
+    i64 x_nx = 0;
+    if (v_nx >= 0) {
+        b_nx = ldro(&c.row[v_nx]);
+        e_nx = ldro(&c.row[v_nx + 1]);
+        h_nx = ldcg(&c.st.h[v_nx]);
+        x_nx = ldcg(&c.st.ex[v_nx]);
+    }
+    for (int base = c.gw * 32; base < nf; base += stride) {
+        const int v = v_nx, vb = b_nx, ve = e_nx, vh = h_nx;
+        const i64 vx = x_nx;
+        const int d = v >= 0 ? ve - vb : 0;
+        v_nx = entry(base + stride);
         bool small = v >= 0 && d <= SMALL_T;
         unsigned sm = __ballot_sync(MF_FULL, small);
         unsigned med = __ballot_sync(MF_FULL, v >= 0 && !small);
+        if (v_nx >= 0) {
+            b_nx = ldro(&c.row[v_nx]);
+            e_nx = ldro(&c.row[v_nx + 1]);
+            h_nx = ldcg(&c.st.h[v_nx]);
+            x_nx = ldcg(&c.st.ex[v_nx]);
+        }
         // small vertices: 8-lane tiles, four per step
         const int tile = c.lane >> 3, tb = tile << 3;
         const unsigned tmask = 0xffu << tb;
@@ -1285,20 +1312,24 @@ __device__ void discharge_front(QCtx &c, const int *L, int nf, int K, int sinkv,
             // the k-th set bit of sm for k = tile
             unsigned rest = sm;
             for (int k = 0; k < tile && rest; ++k) rest &= rest - 1;
-            int src = rest ? __ffs(rest) - 1 : -1;
-            int vt = __shfl_sync(MF_FULL, v, src < 0 ? 0 : src);
+            const int src = rest ? __ffs(rest) - 1 : -1, sl = src < 0 ? 0 : src;
+            const int vt = __shfl_sync(MF_FULL, v, sl), bt = __shfl_sync(MF_FULL, vb, sl);
+            const int et = __shfl_sync(MF_FULL, ve, sl), ht = __shfl_sync(MF_FULL, vh, sl);
+            const i64 xt = __shfl_sync(MF_FULL, vx, sl);
             for (int k = 0; k < 4 && sm; ++k) sm &= sm - 1;
-            if (src >= 0) discharge_tile<8>(c, vt, K, sinkv, blockv, N, nbk, rstamp, ab, tmask, tb);
+            if (src >= 0) discharge_tile<8>(c, vt, bt, et, ht, xt, K, sinkv, blockv, N, nbk, rstamp, ab, tmask, tb);
             __syncwarp();
         }
         // medium vertices: one warp each
         while (med) {
             int o = __ffs(med) - 1;
             med &= med - 1;
-            int vo = __shfl_sync(MF_FULL, v, o);
-            int dv = __shfl_sync(MF_FULL, d, o);
+            const int vo = __shfl_sync(MF_FULL, v, o), bo = __shfl_sync(MF_FULL, vb, o);
+            const int eo = __shfl_sync(MF_FULL, ve, o), ho = __shfl_sync(MF_FULL, vh, o);
+            const i64 xo = __shfl_sync(MF_FULL, vx, o);
+            int dv = eo - bo;
             int Kv = max(1, min(K, (K * 32) / max(dv, 1)));
-            discharge_tile<32>(c, vo, Kv, sinkv, blockv, N, nbk, rstamp, ab, MF_FULL, 0);
+            discharge_tile<32>(c, vo, bo, eo, ho, xo, Kv, sinkv, blockv, N, nbk, rstamp, ab, MF_FULL, 0);
         }
     }
 }
