@@ -1248,19 +1248,6 @@ __device__ void discharge_tile(QCtx &c, int v, int b, int e1, int hv, i64 ev, in
     }
 }
 
-__device__ __forceinline__ void discharge_vertex(QCtx &c, int v, int K, int sinkv, int blockv, int *N,
-                                                 int nbk, unsigned rstamp, i64 *ab) {
-    int hv = 0;
-    i64 ev = 0;
-    if (c.lane == 0) {
-        hv = ldcg(&c.st.h[v]);
-        ev = ldcg(&c.st.ex[v]);
-    }
-    hv = __shfl_sync(MF_FULL, hv, 0);
-    ev = __shfl_sync(MF_FULL, ev, 0);
-    discharge_tile<32>(c, v, ldro(&c.row[v]), ldro(&c.row[v + 1]), hv, ev, K, sinkv, blockv, N, nbk, rstamp, ab,
-                       MF_FULL, 0);
-}
 
 // Discharge of the front part L[0, nf): each warp takes 32 entries.
 // Vertices with at most SMALL_T arcs go to 8-lane tiles, four at a time (a

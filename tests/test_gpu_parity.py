@@ -273,6 +273,11 @@ def test_batch_override_terminal_sets():
         g0 = O.build_csr(n, np.concatenate([gu[:nbr], tu[z[0] > 0]]), np.concatenate([gv[:nbr], tv[z[0] > 0]]),
                          np.concatenate([gc[:nbr], z[0][z[0] > 0]]))
         assert list(f) == [O.dinic(g0, 3, 100), 0]
+        # one shared pair with no path (T cannot reach S): all zero
+        assert list(eg.solve_batch_override([T, T], [S, S], tu, tv, caps[:2])) == [0, 0]
+        # the graph's own cache is back in place after one-pair batches
+        assert list(eg.solve_batch([S, 7, 3], [T, T, 100])) == oracle_flows(O.build_csr(n, gu, gv, gc), [S, 7, 3],
+                                                                           [T, T, 100])
         # rejected: an arc the graph lacks, a capacity above the graph's, certify
         with pytest.raises(mf.MaxflowError):
             eg.solve_batch_override([S], [T], [0], [W * H - 1], [[1]])
