@@ -1107,25 +1107,33 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
     if (!relabel_bfs(c, nv, qbk, f0, b0, depth)) return false;
     int *h = c.st.h;
 
-    // sweep: heights of unreached vertices, active list, counts
+    // counts over the kept vertices
     MF_TRACE(41, 0);
     ab = c.take_abank();
     i64 l_sum = 0, l_def = 0;
-    for (int base = c.gw * 32; base < nv; base += c.gW * 32) {
-        int i = base + c.lane;
-        bool act = false;
-        int v = 0;
-        if (i < nv) {
-            v = c.vat(i);
-            int hv = ldcg(&h[v]);  // n when the search did not reach v
-            i64 ev = ldcg(&c.st.ex[v]);
-            if (ev > 0 && hv < n && v != sinkv && v != blockv) {
-                act = true;
-                l_sum += ev;
+    for (int i = c.gw * 32 + c.lane; i < nv; i += c.gW * 32) {
+        const int v = c.vat(i);
+        const int hv = ldcg(&h[v]);  // n when the search did not reach v
+        const i64 ev = ldcg(&c.st.ex[v]);
+        if (ev > 0 && hv < n && v != sinkv && v != blockv) l_sum += ev;
+        if (ev < 0 && v != srcv && v != blockv) ++l_def;
+    }
+    // Active list in decreasing height: the search queue (every reached
+    // vertex, in level order) read backwards, so each round's warps take
+    // the highest-labelled vertices first.
+    {
+        const int *Q = c.st.qa;
+        const int qf = ldcg(&c.st.cnt[qbk]), qn = qf + ldcg(&c.st.cnt[CNT_BACK + qbk]);
+        for (int base = c.gw * 32; base < qn; base += c.gW * 32) {
+            const int i = base + c.lane;
+            bool act = false;
+            int v = 0;
+            if (i < qn) {
+                v = i < qf ? ldcg(&Q[qf - 1 - i]) : back_at(c, Q, qn - 1 - i);
+                act = ldcg(&c.st.ex[v]) > 0 && ldcg(&h[v]) < n && v != sinkv && v != blockv;
             }
-            if (ev < 0 && v != srcv && v != blockv) ++l_def;
+            append2(c, act, v, L, lbk);
         }
-        append2(c, act, v, L, lbk);
     }
     l_sum = warp_sum_i64(l_sum);
     l_def = warp_sum_i64(l_def);
