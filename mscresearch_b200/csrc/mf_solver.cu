@@ -1107,20 +1107,22 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
     if (!relabel_bfs(c, nv, qbk, f0, b0, depth)) return false;
     int *h = c.st.h;
 
-    // counts over the kept vertices
+    // Active list in decreasing height: the search queue (every reached
+    // vertex, in level order) read backwards, so each round's warps take
+    // the highest-labelled vertices first.  Active vertices are reached
+    // ones; with deficit seeds every deficit is a seed and so in the queue
+    // too, and one pass over the queue also yields the counts.  Without
+    // them (a deficit may be unreached) the counts take a pass over the
+    // kept vertices.
     MF_TRACE(41, 0);
     ab = c.take_abank();
     i64 l_sum = 0, l_def = 0;
-    for (int i = c.gw * 32 + c.lane; i < nv; i += c.gW * 32) {
-        const int v = c.vat(i);
-        const int hv = ldcg(&h[v]);  // n when the search did not reach v
-        const i64 ev = ldcg(&c.st.ex[v]);
-        if (ev > 0 && hv < n && v != sinkv && v != blockv) l_sum += ev;
-        if (ev < 0 && v != srcv && v != blockv) ++l_def;
+    if (!deficit_seeds) {
+        for (int i = c.gw * 32 + c.lane; i < nv; i += c.gW * 32) {
+            const int v = c.vat(i);
+            if (ldcg(&c.st.ex[v]) < 0 && v != srcv && v != blockv) ++l_def;
+        }
     }
-    // Active list in decreasing height: the search queue (every reached
-    // vertex, in level order) read backwards, so each round's warps take
-    // the highest-labelled vertices first.
     {
         const int *Q = c.st.qa;
         const int qf = ldcg(&c.st.cnt[qbk]), qn = qf + ldcg(&c.st.cnt[CNT_BACK + qbk]);
@@ -1130,7 +1132,10 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
             int v = 0;
             if (i < qn) {
                 v = i < qf ? ldcg(&Q[qf - 1 - i]) : back_at(c, Q, qn - 1 - i);
-                act = ldcg(&c.st.ex[v]) > 0 && ldcg(&h[v]) < n && v != sinkv && v != blockv;
+                const i64 ev = ldcg(&c.st.ex[v]);
+                act = ev > 0 && ldcg(&h[v]) < n && v != sinkv && v != blockv;
+                if (act) l_sum += ev;
+                if (deficit_seeds && ev < 0 && v != srcv && v != blockv) ++l_def;
             }
             append2(c, act, v, L, lbk);
         }

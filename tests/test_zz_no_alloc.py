@@ -56,6 +56,40 @@ def test_noalloc_matches_allocating_entry_point_twice():
     assert any(x > 0 for x in expected)
 
 
+def test_noalloc_unaligned_caller_arrays():
+    """A caller CSR whose arc arrays start off a 16-byte boundary (views one
+    element into larger buffers): the residual init then reads scalars
+    instead of 16-byte vectors, with the same flows."""
+    import torch
+    import mscresearch_b200 as mf
+    from mscresearch_b200 import lib
+    torch.cuda.set_device(0)
+    n = 2000
+    u, v, c = mf.gen_uniform(n, 16000, 1, 40, seed=23)
+    with mf.Graph.from_edges(n, u, v, c, R=8) as g:
+        ex = g.export()
+        arcs = len(ex["col"])
+        bufs = {}
+        for k, dt in (("col", torch.int32), ("rev", torch.int32), ("cap", torch.int64)):
+            b = torch.zeros(arcs + 1, dtype=dt, device="cuda")
+            b[1:] = torch.from_numpy(np.ascontiguousarray(ex[k])).cuda()
+            bufs[k] = b
+        row = torch.from_numpy(np.ascontiguousarray(ex["row"])).cuda()
+        assert (bufs["col"][1:].data_ptr() % 16) != 0 and (bufs["cap"][1:].data_ptr() % 16) != 0
+        dev = {"row": row, "col": bufs["col"][1:], "rev": bufs["rev"][1:], "cap": bufs["cap"][1:]}
+        nid = ex["new_id"]
+        rng = np.random.default_rng(9)
+        queries = [(int(a), int(b)) for a, b in zip(rng.integers(0, n, 6), rng.integers(0, n, 6))]
+        expected = [g.solve(a, b)[0] for a, b in queries]
+        got = []
+        for a, b in queries:
+            rc, f = _noalloc(lib, mf, dev, n, arcs, nid[a], nid[b])
+            assert rc == 0, lib.mf_last_error_string()
+            got.append(f)
+        assert got == expected
+    assert any(x > 0 for x in expected)
+
+
 def test_noalloc_rejects_graphs_over_the_limit():
     import torch
     import mscresearch_b200 as mf
