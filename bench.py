@@ -19,6 +19,13 @@ and a bounded sample of the same queries, and reports its own per-query
 times (res_mt.txt, integer ms, prune included, RA:2808).
 Multi-GPU (torchrun): queries shard across ranks (one graph replica per
 GPU, no data-path collective); timing is the max over ranks.
+
+Other workloads (not the headline line):
+  --workload mix       8 device-resident R-MAT graphs (2^14..2^20) served to
+                       Poisson-arriving requests, against the plain loop;
+  --workload gridsets  a 2048 x 2048 segmentation grid, 64 queries that vary
+                       the terminal set (mf_solve_batch_override), relabel
+                       frequency, group size and R tuned on 16 of the sets.
 """
 import argparse
 import json
