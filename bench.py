@@ -25,7 +25,10 @@ Other workloads (not the headline line):
                        Poisson-arriving requests, against the plain loop;
   --workload gridsets  a 2048 x 2048 segmentation grid, 64 queries that vary
                        the terminal set (mf_solve_batch_override), relabel
-                       frequency, group size and R tuned on 16 of the sets.
+                       frequency, group size and R tuned on 16 of the sets;
+  --workload dynamic   R-MAT 2^22 with 32 resident queries: 1k/10k/100k
+                       capacity-update batches, incremental repair against a
+                       fresh batched solve.
 """
 import argparse
 import json
@@ -569,6 +572,64 @@ def run_gridsets(args):
         print(json.dumps(res), flush=True)
 
 
+def run_dynamic(args):
+    """Dynamic updates: R-MAT n = 2^22, 2^26 draws, caps U[1,1000]; 32
+    resident queries (16 hub, 16 uniform) in one session; batches of 1k, 10k
+    and 100k seeded capacity changes (+-U[1,100], clamped at 0), each applied
+    to the graph and followed by the incremental repair of every resident
+    query (mf_session_update), every answer checked against a fresh batched
+    solve of the same queries on the updated graph."""
+    rank = int(os.environ.get("RANK", "0"))
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    import mscresearch_b200 as mf
+    scale = 22
+    u, v, c = mf.gen_rmat(scale, 1 << (scale + 4), 0.57, 0.19, 0.19, 1, 1000, 5)
+    n = 1 << scale
+    s, t = mf.gen_queries_hub(n, u, v, 16, 16, 6 + 1000 * rank)
+    rng = np.random.default_rng(7)
+    g = mf.Graph.from_edges(n, u, v, c, R=R)
+    _, arcs, _ = g.info
+    o = mf.opts(group_ctas=args.group)
+    g.solve_batch(s, t, o)  # kept-set cache and slots
+    ss = mf.Session(g, s, t, o)
+    t0 = time.perf_counter()
+    f0 = ss.solve()
+    solve_wall = (time.perf_counter() - t0) * 1e3
+    exact0 = list(f0) == list(g.solve_batch(s, t, o))
+    runs = []
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        for k in (1000, 10000, 100000):
+            idx = rng.integers(0, len(u), k)
+            d = rng.integers(1, 101, k) * rng.choice([-1, 1], k)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fr = ss.update(u[idx], v[idx], d)
+            upd_wall = (time.perf_counter() - t0) * 1e3
+            rep_ms = g.last_device_ms
+            fresh = g.solve_batch(s, t, o)
+            fresh_ms = g.last_device_ms
+            runs.append({"updates": k, "update_and_repair_wall_ms": round(upd_wall, 2),
+                         "repair_device_ms": round(rep_ms, 2), "fresh_batch_device_ms": round(fresh_ms, 2),
+                         "repair_speedup_vs_fresh": round(fresh_ms / rep_ms, 2) if rep_ms > 0 else None,
+                         "exact": bool(list(fr) == list(fresh))})
+    ss.close()
+    g.close()
+    mid = runs[1]
+    res = {"metric": "exact max-flow queries/sec after a capacity-update batch (incremental repair)",
+           "value": round(len(s) / (mid["update_and_repair_wall_ms"] / 1e3), 3), "unit": "queries/s",
+           "n_gpus": 1, "higher_is_better": True, "dtype": "int64",
+           "data": "synthetic (seeded R-MAT 2^22, 2^26 draws, caps U[1,1000]; 16 hub + 16 uniform queries; "
+                   "updates +-U[1,100] on random edges, clamped at 0)",
+           "config": {"workload": "rmat22_32q_updates", "n": n, "arcs": arcs, "queries": len(s), "R": R,
+                      "group_ctas": o.group_ctas, "value_from": "10k-update batch, host wall time of "
+                      "mf_session_update (capacity updates + repair of all 32 queries)"},
+           "initial_session_solve_wall_ms": round(solve_wall, 2), "initial_exact": exact0,
+           "batches": runs, "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -649,9 +710,10 @@ def main():
                     help="set any mf_opts field (repeatable), e.g. --opt use_hot_sweep=0")
     ap.add_argument("--gr-freq", type=int, default=0, help="max rounds between global relabels")
     ap.add_argument("--gr-alpha", type=float, default=None, help="relabel after alpha x kept arcs of work")
-    ap.add_argument("--workload", default="rmat", choices=["rmat", "mix", "gridsets"],
+    ap.add_argument("--workload", default="rmat", choices=["rmat", "mix", "gridsets", "dynamic"],
                     help="rmat: the headline R-MAT 2^20 batch; mix: the serving mix of 8 graphs; "
-                         "gridsets: one segmentation grid, queries that vary the terminal set")
+                         "gridsets: one segmentation grid, queries that vary the terminal set; "
+                         "dynamic: capacity-update batches on R-MAT 2^22 with resident queries")
     ap.add_argument("--grid-w", type=int, default=2048)
     ap.add_argument("--grid-sets", type=int, default=64)
     ap.add_argument("--mix-requests", type=int, default=512)
@@ -666,6 +728,8 @@ def main():
         run_mix(args)
     elif args.workload == "gridsets":
         run_gridsets(args)
+    elif args.workload == "dynamic":
+        run_dynamic(args)
     else:
         run_engine(args)
 

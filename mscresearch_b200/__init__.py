@@ -246,12 +246,13 @@ class Session:
         _check(lib.mf_session_solve(self._h, _p(f, C.c_int64), None))
         return f
 
-    def update(self, u, v, delta):
+    def update(self, u, v, delta, with_stats=False):
         u, v, d = _i32(u), _i32(v), _i64(delta)
         f = np.zeros(self.nq, np.int64)
+        sts = (MfStats * max(self.nq, 1))() if with_stats else None
         _check(lib.mf_session_update(self._h, len(u), _p(u, C.c_int32), _p(v, C.c_int32), _p(d, C.c_int64),
-                                     _p(f, C.c_int64), None))
-        return f
+                                     _p(f, C.c_int64), sts))
+        return (f, list(sts)[:self.nq]) if with_stats else f
 
     def close(self):
         if self._h:
