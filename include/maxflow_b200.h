@@ -234,7 +234,10 @@ int mf_update_caps(mf_graph *g, int nb, const int32_t *u, const int32_t *v, cons
  * them from scratch; mf_session_update applies a capacity batch to the graph
  * and repairs every resident query incrementally from its kept residual
  * state (flow cancelled on arcs whose capacity fell below their flow, new
- * capacity saturated from the source, then push-relabel resumes). */
+ * capacity saturated from the source, then push-relabel resumes).  A batch
+ * that changes more than 1/2000 of the graph's arcs re-solves the resident
+ * queries from scratch instead (faster at that size; environment variable
+ * MF_REPAIR_MAX_UPDATES sets another limit). */
 typedef struct mf_session mf_session;
 int mf_session_create(mf_graph *g, int nq, const int32_t *s, const int32_t *t, const mf_opts *opts,
                       mf_session **out);

@@ -36,8 +36,16 @@ def make_updates(rng, u, v, k, n):
     return uu, vv, d
 
 
+@pytest.mark.parametrize("policy", ["repair", "default"])
 @pytest.mark.parametrize("scale", [10, 14])
-def test_session_incremental_equals_fresh(scale):
+def test_session_incremental_equals_fresh(scale, policy, monkeypatch):
+    """Resident answers after each update batch equal the oracle's; "repair"
+    forces the incremental path for every batch size, "default" lets large
+    batches re-solve from scratch."""
+    if policy == "repair":
+        monkeypatch.setenv("MF_REPAIR_MAX_UPDATES", "1000000000")
+    else:
+        monkeypatch.delenv("MF_REPAIR_MAX_UPDATES", raising=False)
     n = 1 << scale
     u, v, c = mf.gen_rmat(scale, 16 * n, seed=31 + scale)
     s, t = mf.gen_queries_hub(n, u, v, 6, 6, seed=8)
