@@ -107,6 +107,48 @@ def test_tokenizer_rule_fuzz(tmp_path):
         _check_model(tmp_path, "7 %d\n%s" % (int(rng.integers(0, 12)), body))
 
 
+def model_csr(n, u, v, c):
+    """The device CSR build, restated: half-arcs h = 2i + side keyed by their
+    tail (n for dropped edges), stably sorted; positions give the arcs."""
+    u, v, c = np.asarray(u, np.int64), np.asarray(v, np.int64), np.asarray(c, np.int64)
+    m = len(u)
+    kept = (u >= 0) & (u < n) & (v >= 0) & (v < n) & (u != v) & (c > 0)
+    key = np.empty(2 * m, np.int64)
+    key[0::2] = np.where(kept, u, n)
+    key[1::2] = np.where(kept, v, n)
+    order = np.argsort(key, kind="stable")
+    arcs = int(2 * kept.sum())
+    h = order[:arcs]
+    pos = np.empty(2 * m, np.int64)
+    pos[h] = np.arange(arcs)
+    i, back = h >> 1, (h & 1) == 1
+    col = np.where(back, u[i], v[i])
+    cap = np.where(back, 0, c[i])
+    rev = pos[h ^ 1]
+    row = np.searchsorted(key[order], np.arange(n + 1), side="left")
+    return row, col, cap, rev
+
+
+def test_half_arc_sort_reproduces_reader_order():
+    """A stable sort of half-arcs by tail gives exactly the arc order of the
+    reference reader's build loop (the oracle's build_csr), dropped edges,
+    parallel arcs and hubs included."""
+    import mscresearch_b200 as mf
+    for scale, m, seed in ((8, 3000, 1), (11, 40000, 2)):
+        n = 1 << scale
+        u, v, c = mf.gen_rmat(scale, m, seed=seed)
+        u, v, c = u.copy(), v.copy(), c.copy()
+        rng = np.random.default_rng(seed)
+        k = rng.integers(0, len(u), 60)
+        c[k[:20]] = 0
+        u[k[20:40]] = v[k[20:40]]
+        v[k[40:]] = n + 5
+        g = O.build_csr(n, u, v, c)
+        row, col, cap, rev = model_csr(n, u, v, c)
+        assert np.array_equal(row, g.row) and np.array_equal(col, g.col)
+        assert np.array_equal(cap, g.cap) and np.array_equal(rev, g.rev)
+
+
 # ---- GPU --------------------------------------------------------------------
 
 def _same_graph(a, b):
