@@ -848,6 +848,13 @@ int mf_graph_load_file(const char *path, int R, mf_graph **out) {
     long long S = ftell(f);
     fseek(f, 0, SEEK_SET);
     if (S < 0) S = 0;
+    // token indices are 32-bit: a file below 4 GiB holds fewer than 2^31
+    // integers (each takes a digit and a separator)
+    if (S >= (4LL << 30)) {
+        fclose(f);
+        return fail(MF_ERR_ARG, "%s is %lld bytes; text graphs of 4 GiB or more are not read (pass edge arrays "
+                                "or a binary CSR cache)", path, S);
+    }
     unsigned char *dtxt = nullptr;
     cudaStream_t st = nullptr;
     int rc = MF_OK;
