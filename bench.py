@@ -630,6 +630,42 @@ def run_dynamic(args):
         print(json.dumps(res), flush=True)
 
 
+def reference_workload(scale=SCALE, nhub=NHUB, nuni=NUNI):
+    """The headline workload from the oracle's restatement of the engine's
+    generators (identical arrays, tests/test_oracle.py), so that the process
+    timing the reference never loads the engine's library."""
+    from oracle import oracle as O
+    u, v, c = O.gen_rmat(scale, 16 << scale, 0.57, 0.19, 0.19, 1, 1000, GRAPH_SEED)
+    n = 1 << scale
+    s, t = O.gen_queries_hub(n, u, v, nhub, nuni, QUERY_SEED)
+    return n, u, v, c, s, t
+
+
+def classify_reference_mismatches(stderr_text, n_full, arcs_full, mismatched):
+    """Classify each query whose reference flow differs from the oracle's.
+    The reference keeps one graph on the device and, when a query's run graph
+    has the same (V, E, R) as the one there, re-uploads only the capacities
+    (init_global_graph_on_device, RA:1303-1331) onto the previous topology.
+    A mismatch on such a query is 'stale-topology'; any other is
+    'unexplained'.  Uses the reference's own per-query log lines
+    ('[QueryPrune+RegionBoundary] ... run_n=.., run_m=..', RA:2815-2819)."""
+    import re
+    dims = []
+    for line in stderr_text.splitlines():
+        if line.startswith("[QueryPrune+RegionBoundary]"):
+            mn = re.search(r"run_n=(\d+)", line)
+            mm = re.search(r"run_m=(\d+)", line)
+            dims.append((int(mn.group(1)), int(mm.group(1))) if mn and mm else None)
+    out = {}
+    for i in mismatched:
+        if i >= len(dims) or dims[i] is None:
+            out[i] = "unexplained (no log line)"
+            continue
+        prev = dims[i - 1] if i > 0 else (n_full, arcs_full)
+        out[i] = "stale-topology" if dims[i] == prev else "unexplained"
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -639,16 +675,15 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ra_ref not built "
                           "(needs the reference sources; oracle/build_ref.sh)"}))
         return
-    import mscresearch_b200 as mf
-    n, u, v, c, s, t = make_workload(0)
+    n, u, v, c, s, t = reference_workload()
     per_step = args.ref_queries_per_step
     nsteps = args.warmup + args.steps
     order = [i for pair in zip(range(NHUB), range(NHUB, NHUB + NUNI)) for i in pair]
     idx = order[: per_step * nsteps]
     d = tempfile.mkdtemp()
     out = os.path.join(d, "out")
-    mf.write_graph_txt(os.path.join(d, "graph.txt"), n, u, v, c)
-    mf.write_test_txt(os.path.join(d, "test.txt"), s[idx], t[idx])
+    O.write_graph_txt(os.path.join(d, "graph.txt"), n, u, v, c)
+    O.write_test_txt(os.path.join(d, "test.txt"), s[idx], t[idx])
     t0 = time.time()
     with ClockSampler(0) as clk:
         r = subprocess.run(["timeout", str(args.ref_timeout), O.REF_BIN, d, out, "static"],
@@ -670,18 +705,27 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic (seeded R-MAT 2^20, 2^24 draws, caps U[1,1000])",
-            "config": {"workload": WORKLOAD, "n": n, "edges": len(u), "queries_sampled": len(idx), "R": 128},
+            "config": {"workload": WORKLOAD, "n": n, "edges": len(u), "queries_sampled": len(idx), "R": 128,
+                       "sample": "queries 0,128,1,129,... of the 256 (hub and uniform alternating)"},
             "p50_ms": pct(timed, 50), "p99_ms": pct(timed, 99),
             "cpu_baseline": {"value": value, "unit": "queries/s", "cores": 1, "kind": "reference",
                              "sample": sample + "; the reference is a CUDA program: host prune on 1 core "
                                                 "+ kernels on the B200"},
             "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "inputs": "graph.txt / test.txt written by the oracle's generators (oracle/gen.c); "
+                      "this process loads no engine library",
             "clocks": clk.summary()}
-    if args.check:
-        from oracle import oracle as O2
-        g = O2.build_csr(n, u, v, c)
-        exp = O2.dinic_batch(g, s[idx], t[idx], os.cpu_count() or 1)
-        line["flows_match_oracle"] = int((res[:, 0] == exp).sum())
+    if not args.no_check:
+        g = O.build_csr(n, u, v, c)
+        exp = O.dinic_batch(g, s[idx], t[idx], os.cpu_count() or 1)
+        got = res[:, 0]
+        bad = [i for i in range(len(idx)) if int(got[i]) != int(exp[i])]
+        line["flows_match_oracle"] = len(idx) - len(bad)
+        line["flows_checked"] = len(idx)
+        if bad:
+            cls = classify_reference_mismatches(r.stderr, n, g.arcs, bad)
+            line["mismatches"] = [{"query": int(idx[i]), "reference": int(got[i]), "oracle": int(exp[i]),
+                                   "class": cls[i]} for i in bad]
     print(json.dumps(line), flush=True)
 
 
@@ -697,7 +741,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--ref-queries-per-step", type=int, default=2)
     ap.add_argument("--ref-timeout", type=int, default=900)
-    ap.add_argument("--check", action="store_true")
+    ap.add_argument("--no-check", action="store_true",
+                    help="reference arm: skip checking its flows against the oracle's Dinic")
     ap.add_argument("--no-certify", action="store_true", help="skip the untimed certification pass")
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--nhub", type=int, default=NHUB)

@@ -187,6 +187,16 @@ int mf_debug_prune_mask(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, 
                         int *kept);
 int mf_debug_initial_heights(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts,
                              int32_t *heights);
+/* Allocation accounting and failure injection, for tests of the failure
+ * paths (no counterpart in the reference, whose allocations are unchecked,
+ * RA:1336-1372).  Every device and pinned-host allocation the engine makes
+ * goes through one wrapper.  mf_debug_alloc_fail_after(k): the k-th next
+ * allocation (0 = the next one) reports out-of-memory without allocating;
+ * k < 0 disarms it.  mf_debug_alloc_live: allocations and bytes the engine
+ * holds now, and the armed countdown (-1 = none); any pointer may be NULL. */
+int mf_debug_alloc_fail_after(long long k);
+int mf_debug_alloc_live(long long *count, long long *bytes, long long *fail_after);
+
 /* Solve and copy the final residual capacities back (arcs in region order,
  * matching mf_graph_export's CSR). */
 int mf_solve_residual(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, int64_t *flow,
@@ -205,16 +215,24 @@ int mf_certify(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, int64_t *
  * device memory pool, a service that reserves everything at start-up and
  * must not let cudaMalloc synchronize the device on the request path, a
  * plugin handed only device pointers.  The caller passes a paired-arc CSR
- * already in device memory (d_row: n+1 offsets; d_col/d_rev/d_cap: arcs
- * entries, any vertex order, rev pairing each arc with its reverse) and gets
- * the exact max flow from s to t in *flow (host).  Scratch is a fixed
- * file-scope device array of about 11 MB sized for n <= 65536 vertices and
- * arcs <= 1048576; larger graphs are rejected with MF_ERR_ARG.  The call
- * makes no cudaMalloc / cudaFree or other allocating call.  Its first call on
- * a device resolves the array's device address and zeroes it; make that first
- * call before any stream capture.  Every call shares the array and it keeps
- * the last call's contents, so calls that overlap on the GPU race: serialize
- * them.  stream: a cudaStream_t (NULL = default stream); stats may be NULL. */
+ * already in device memory (d_row: n+1 offsets from 0 to arcs; d_col/d_rev/
+ * d_cap: arcs entries, any vertex order; every head in [0, n); rev[e] is an
+ * arc of e's head back to e's tail with rev[rev[e]] == e; capacities >= 0)
+ * and gets the exact max flow from s to t in *flow (host).  A check kernel
+ * validates those rules first and a CSR that breaks one is rejected with
+ * MF_ERR_ARG.  Scratch is a fixed file-scope device array of about 11 MB
+ * sized for n <= 65536 vertices and arcs <= 1048576; larger graphs are
+ * rejected with MF_ERR_ARG.  The call makes no cudaMalloc / cudaFree or
+ * other allocating call.  Its first call on a device resolves the array's
+ * device address and zeroes it (once per device, also when several host
+ * threads make their first call together); make that first call before any
+ * stream capture.  The address is kept for the process's life, so a
+ * cudaDeviceReset of that device is not supported afterwards.  Options are
+ * resolved and device statuses reported exactly as mf_solve does.  Every
+ * call waits for its stream to finish its work before returning.  Every call
+ * shares the array and it keeps the last call's contents, so calls that
+ * overlap on the GPU race: serialize them.  stream: a cudaStream_t (NULL =
+ * default stream); stats may be NULL. */
 int mf_solve_csr_noalloc(int n, long long arcs, const int32_t *d_row, const int32_t *d_col,
                          const int32_t *d_rev, const int64_t *d_cap, int32_t s, int32_t t,
                          const mf_opts *opts, void *stream, int64_t *flow, mf_stats *stats);

@@ -259,6 +259,12 @@ class Session:
             lib.mf_session_destroy(self._h)
             self._h = C.c_void_p()
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
     def __del__(self):
         try:
             self.close()

@@ -99,6 +99,8 @@ SIGNATURES = {
     "mf_debug_initial_heights": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(MfOpts), i32p]),
     "mf_solve_residual": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(MfOpts), i64p, i64p, C.POINTER(MfStats)]),
     "mf_certify": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(MfOpts), i64p, C.POINTER(MfStats)]),
+    "mf_debug_alloc_fail_after": (C.c_int, [C.c_longlong]),
+    "mf_debug_alloc_live": (C.c_int, [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "mf_solve_csr_noalloc": (C.c_int, [C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.POINTER(MfOpts), C.c_void_p, i64p, C.POINTER(MfStats)]),
     "mf_update_caps": (C.c_int, [C.c_void_p, C.c_int, i32p, i32p, i64p, C.POINTER(C.c_int)]),
     "mf_session_create": (C.c_int, [C.c_void_p, C.c_int, i32p, i32p, C.POINTER(MfOpts), C.POINTER(C.c_void_p)]),

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "../../include/maxflow_b200.h"
+#include "mf_alloc.h"
 #include "mf_build.cuh"
 #include "mf_solver.cuh"
 
@@ -103,13 +104,17 @@ struct SlotPool {
         while ((int)host.size() < want) {
             size_t bytes = slot_bytes(n, arcs, nhub);
             void *base = nullptr;
-            cudaError_t e = cudaMalloc(&base, bytes);
+            cudaError_t e = mf_dmalloc(&base, bytes);
             if (e != cudaSuccess) {
                 cudaGetLastError();
                 return fail(MF_ERR_NOMEM, "residual slot allocation (%zu bytes) failed: %s", bytes,
                             cudaGetErrorString(e));
             }
-            CK(cudaMemset(base, 0, bytes));
+            e = cudaMemset(base, 0, bytes);
+            if (e != cudaSuccess) {
+                mf_dfree(base);
+                return fail(MF_ERR_CUDA, "residual slot clear failed: %s", cudaGetErrorString(e));
+            }
             char *p = (char *)base;
             auto take = [&](size_t x) {
                 char *r = p;
@@ -140,20 +145,20 @@ struct SlotPool {
             host.push_back(s);
         }
         if (dev_cap < (int)host.size()) {
-            if (dev) cudaFree(dev);
+            if (dev) mf_dfree(dev);
             dev = nullptr;
             dev_cap = 0;
-            CK(cudaMalloc(&dev, sizeof(DSlot) * host.size()));
+            CK(mf_dmalloc(&dev, sizeof(DSlot) * host.size()));
             dev_cap = (int)host.size();
         }
         CK(cudaMemcpy(dev, host.data(), sizeof(DSlot) * host.size(), cudaMemcpyHostToDevice));
         return MF_OK;
     }
     void release() {
-        for (void *b : bases) cudaFree(b);
+        for (void *b : bases) mf_dfree(b);
         bases.clear();
         host.clear();
-        if (dev) cudaFree(dev);
+        if (dev) mf_dfree(dev);
         dev = nullptr;
         dev_cap = 0;
     }
@@ -296,11 +301,11 @@ struct mf_session {
 namespace {
 
 void free_kept_cache(mf_graph *g) {
-    cudaFree(g->kc_in);
-    cudaFree(g->kc_fb);
+    mf_dfree(g->kc_in);
+    mf_dfree(g->kc_fb);
     g->kc_fb = nullptr;
-    cudaFree(g->kc_img);
-    cudaFree(g->kc_res);
+    mf_dfree(g->kc_img);
+    mf_dfree(g->kc_res);
     g->kc_in = nullptr;
     g->kc_img = nullptr;
     g->kc_res = nullptr;
@@ -311,17 +316,17 @@ void free_kept_cache(mf_graph *g) {
 
 void free_graph_arrays(mf_graph *g) {
     free_kept_cache(g);
-    cudaFree(g->row);
-    cudaFree(g->col);
-    cudaFree(g->rev);
-    cudaFree(g->cap);
-    cudaFree(g->fwd);
-    cudaFree(g->region_of);
-    cudaFree(g->region_start);
-    cudaFree(g->d_graph);
-    cudaFree(g->hubs);
+    mf_dfree(g->row);
+    mf_dfree(g->col);
+    mf_dfree(g->rev);
+    mf_dfree(g->cap);
+    mf_dfree(g->fwd);
+    mf_dfree(g->region_of);
+    mf_dfree(g->region_start);
+    mf_dfree(g->d_graph);
+    mf_dfree(g->hubs);
     g->hubs = nullptr;
-    cudaFree(g->giants);
+    mf_dfree(g->giants);
     g->giants = nullptr;
     g->ngiant = 0;
     g->row = g->col = g->rev = g->region_of = g->region_start = nullptr;
@@ -372,31 +377,29 @@ int partition_into(mf_graph *g, int R, int *row, int *col, i64 *cap, int *rev, u
     const i64 arcs = g->arcs;
     BuildIn in{n, R, arcs, row, col, cap, rev, fwd};
     BuildOut out{};
-    CK(cudaMalloc(&out.row, sizeof(int) * ((size_t)n + 1)));
-    CK(cudaMalloc(&out.col, sizeof(int) * (size_t)std::max<i64>(arcs, 1)));
-    CK(cudaMalloc(&out.cap, sizeof(i64) * (size_t)std::max<i64>(arcs, 1)));
-    CK(cudaMalloc(&out.rev, sizeof(int) * (size_t)std::max<i64>(arcs, 1)));
-    CK(cudaMalloc(&out.fwd, (size_t)std::max<i64>(arcs, 1)));
-    CK(cudaMalloc(&out.new_id, sizeof(int) * (size_t)n));
-    CK(cudaMalloc(&out.old_id, sizeof(int) * (size_t)n));
-    CK(cudaMalloc(&out.region_start, sizeof(int) * ((size_t)R + 1)));
-    CK(cudaMalloc(&out.region_of, sizeof(int) * (size_t)n));
-    CK(cudaMalloc(&out.score, sizeof(double) * (size_t)n));
-    CK(cudaMalloc(&out.part, sizeof(int) * (size_t)n));
+    // the new graph arrays (kept on success) and the build's temporaries:
+    // both scopes free what they hold if any step fails
+    DevScope keep, tmp;
+    CK(keep.alloc(&out.row, sizeof(int) * ((size_t)n + 1)));
+    CK(keep.alloc(&out.col, sizeof(int) * (size_t)std::max<i64>(arcs, 1)));
+    CK(keep.alloc(&out.cap, sizeof(i64) * (size_t)std::max<i64>(arcs, 1)));
+    CK(keep.alloc(&out.rev, sizeof(int) * (size_t)std::max<i64>(arcs, 1)));
+    CK(keep.alloc(&out.fwd, (size_t)std::max<i64>(arcs, 1)));
+    CK(keep.alloc(&out.region_start, sizeof(int) * ((size_t)R + 1)));
+    CK(keep.alloc(&out.region_of, sizeof(int) * (size_t)n));
+    CK(tmp.alloc(&out.new_id, sizeof(int) * (size_t)n));
+    CK(tmp.alloc(&out.old_id, sizeof(int) * (size_t)n));
+    CK(tmp.alloc(&out.score, sizeof(double) * (size_t)n));
+    CK(tmp.alloc(&out.part, sizeof(int) * (size_t)n));
     void *scratch = nullptr;
-    CK(cudaMalloc(&scratch, mf_partition_scratch_bytes(n, arcs, R)));
+    CK(tmp.alloc(&scratch, mf_partition_scratch_bytes(n, arcs, R)));
     CK(mf_partition_reorder(in, out, scratch, g->stream));
     CK(cudaStreamSynchronize(g->stream));
-    cudaFree(scratch);
     std::vector<int> nid(n), sc_part(n);
     std::vector<double> sc(n);
     CK(cudaMemcpy(nid.data(), out.new_id, sizeof(int) * n, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(sc.data(), out.score, sizeof(double) * n, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(sc_part.data(), out.part, sizeof(int) * n, cudaMemcpyDeviceToHost));
-    cudaFree(out.new_id);
-    cudaFree(out.old_id);
-    cudaFree(out.score);
-    cudaFree(out.part);
     // compose: caller -> input index -> internal
     std::vector<int> new_id(n), old_id(n);
     g->score_caller.assign(n, 0.0);
@@ -409,6 +412,7 @@ int partition_into(mf_graph *g, int R, int *row, int *col, i64 *cap, int *rev, u
         g->part_caller[x] = sc_part[i];
     }
     free_graph_arrays(g);
+    keep.release();
     g->row = out.row;
     g->col = out.col;
     g->cap = out.cap;
@@ -440,47 +444,50 @@ int finalize_graph(mf_graph *g) {
         }
         g->nhub = (int)hl.size();
         if (!hl.empty()) {
-            CK(cudaMalloc(&g->hubs, sizeof(int) * hl.size()));
+            CK(mf_dmalloc(&g->hubs, sizeof(int) * hl.size()));
             CK(cudaMemcpy(g->hubs, hl.data(), sizeof(int) * hl.size(), cudaMemcpyHostToDevice));
         }
         g->ngiant = (int)gl.size();
         if (!gl.empty()) {
-            CK(cudaMalloc(&g->giants, sizeof(int) * gl.size()));
+            CK(mf_dmalloc(&g->giants, sizeof(int) * gl.size()));
             CK(cudaMemcpy(g->giants, gl.data(), sizeof(int) * gl.size(), cudaMemcpyHostToDevice));
         }
     }
     g->pivot = best;
-    CK(cudaMalloc(&g->d_graph, sizeof(DGraph)));
+    CK(mf_dmalloc(&g->d_graph, sizeof(DGraph)));
     return upload_dgraph(g);
 }
 
 int ensure_launch_buffers(mf_graph *g, int nq, int nslots) {
     if (!g->d_err) {
-        CK(cudaMalloc(&g->d_err, sizeof(int) * 2));
+        CK(mf_dmalloc(&g->d_err, sizeof(int) * 2));
         g->d_qnext = g->d_err + 1;
     }
     if (g->out_cap < nq) {
-        cudaFree(g->d_out);
-        cudaFreeHost(g->h_out);
+        mf_dfree(g->d_out);
+        mf_hfree(g->h_out);
         g->d_out = nullptr;
         g->h_out = nullptr;
-        CK(cudaMalloc(&g->d_out, sizeof(QOut) * nq));
-        CK(cudaMallocHost(&g->h_out, sizeof(QOut) * nq));
+        g->out_cap = 0;  // a failed allocation below leaves no stale capacity
+        CK(mf_dmalloc(&g->d_out, sizeof(QOut) * nq));
+        CK(mf_hmalloc(&g->h_out, sizeof(QOut) * nq));
         g->out_cap = nq;
     }
     if (g->q_cap < nq) {
-        cudaFree(g->d_q);
-        cudaFreeHost(g->h_pin);
+        mf_dfree(g->d_q);
+        mf_hfree(g->h_pin);
         g->d_q = nullptr;
         g->h_pin = nullptr;
-        CK(cudaMalloc(&g->d_q, sizeof(int) * 3 * (size_t)nq));
-        CK(cudaMallocHost(&g->h_pin, sizeof(int) * 3 * (size_t)nq));
+        g->q_cap = 0;
+        CK(mf_dmalloc(&g->d_q, sizeof(int) * 3 * (size_t)nq));
+        CK(mf_hmalloc(&g->h_pin, sizeof(int) * 3 * (size_t)nq));
         g->q_cap = nq;
     }
     if (g->clocks_cap < nslots) {
-        cudaFree(g->d_clocks);
+        mf_dfree(g->d_clocks);
         g->d_clocks = nullptr;
-        CK(cudaMalloc(&g->d_clocks, sizeof(unsigned) * nslots));
+        g->clocks_cap = 0;
+        CK(mf_dmalloc(&g->d_clocks, sizeof(unsigned) * nslots));
         g->clocks_cap = nslots;
     }
     return MF_OK;
@@ -686,7 +693,7 @@ struct FileStream {
     int k = 0;
     bool init(cudaStream_t s) {
         st = s;
-        return cudaMallocHost(&pin[0], chunk) == cudaSuccess && cudaMallocHost(&pin[1], chunk) == cudaSuccess &&
+        return mf_hmalloc(&pin[0], chunk) == cudaSuccess && mf_hmalloc(&pin[1], chunk) == cudaSuccess &&
                cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming) == cudaSuccess;
     }
@@ -709,8 +716,8 @@ struct FileStream {
     }
     ~FileStream() {
         if (st) cudaStreamSynchronize(st);
-        cudaFreeHost(pin[0]);
-        cudaFreeHost(pin[1]);
+        mf_hfree(pin[0]);
+        mf_hfree(pin[1]);
         if (done[0]) cudaEventDestroy(done[0]);
         if (done[1]) cudaEventDestroy(done[1]);
     }
@@ -771,6 +778,91 @@ int graph_from_device_edges(int n, i64 m, const int *du, const int *dv, const i6
 // (used by entry points implemented in other translation units).
 void mf_set_last_error(const char *msg) { g_err = msg ? msg : ""; }
 
+// ---- allocation wrapper (mf_alloc.h) -------------------------------------
+namespace {
+std::mutex g_alloc_mu;
+std::unordered_map<void *, size_t> g_alloc_live;  // live allocation -> bytes
+long long g_alloc_bytes = 0;
+long long g_alloc_fail_after = -1;  // allocations left before an injected failure (-1: none)
+
+// true: this allocation is the injected failure
+bool alloc_inject() {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    if (g_alloc_fail_after < 0) return false;
+    if (g_alloc_fail_after == 0) {
+        g_alloc_fail_after = -1;
+        return true;
+    }
+    --g_alloc_fail_after;
+    return false;
+}
+void alloc_track(void *p, size_t bytes) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    g_alloc_live[p] = bytes;
+    g_alloc_bytes += (long long)bytes;
+}
+void alloc_untrack(void *p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    auto it = g_alloc_live.find(p);
+    if (it == g_alloc_live.end()) return;
+    g_alloc_bytes -= (long long)it->second;
+    g_alloc_live.erase(it);
+}
+}  // namespace
+
+cudaError_t mf_dmalloc_raw(void **p, size_t bytes) {
+    *p = nullptr;
+    if (alloc_inject()) return cudaErrorMemoryAllocation;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) alloc_track(*p, bytes);
+    return e;
+}
+cudaError_t mf_dfree(void *p) {
+    alloc_untrack(p);
+    return cudaFree(p);
+}
+cudaError_t mf_hmalloc_raw(void **p, size_t bytes) {
+    *p = nullptr;
+    if (alloc_inject()) return cudaErrorMemoryAllocation;
+    cudaError_t e = cudaMallocHost(p, bytes);
+    if (e == cudaSuccess) alloc_track(*p, bytes);
+    return e;
+}
+cudaError_t mf_hostalloc_raw(void **p, size_t bytes, unsigned flags) {
+    *p = nullptr;
+    if (alloc_inject()) return cudaErrorMemoryAllocation;
+    cudaError_t e = cudaHostAlloc(p, bytes, flags);
+    if (e == cudaSuccess) alloc_track(*p, bytes);
+    return e;
+}
+cudaError_t mf_hfree(void *p) {
+    alloc_untrack(p);
+    return cudaFreeHost(p);
+}
+
+extern "C" int mf_debug_alloc_fail_after(long long k) {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    g_alloc_fail_after = k < 0 ? -1 : k;
+    return MF_OK;
+}
+
+extern "C" int mf_debug_alloc_live(long long *count, long long *bytes, long long *fail_after) {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    if (count) *count = (long long)g_alloc_live.size();
+    if (bytes) *bytes = g_alloc_bytes;
+    if (fail_after) *fail_after = g_alloc_fail_after;
+    return MF_OK;
+}
+
+// Option resolution, the launch time limit and the device-status mapping,
+// shared with entry points in other translation units so that every entry
+// point resolves options and reports device statuses alike.
+KOpts mf_resolve_opts(const mf_opts &o, int avg_deg) { return resolve_opts(o, avg_deg); }
+u64 mf_launch_time_limit_ns() { return launch_time_limit_ns(); }
+int mf_status_from_err(int e) { return status_from_err(e); }
+
 // ===========================================================================
 extern "C" {
 
@@ -812,8 +904,8 @@ int mf_graph_create_from_edges(int n, long long m, const int32_t *u, const int32
     i64 *dc = nullptr;
     const size_t M = (size_t)std::max<long long>(m, 1);
     int rc = MF_OK;
-    if (cudaMalloc(&du, sizeof(int) * M) != cudaSuccess || cudaMalloc(&dv, sizeof(int) * M) != cudaSuccess ||
-        cudaMalloc(&dc, sizeof(i64) * M) != cudaSuccess) {
+    if (mf_dmalloc(&du, sizeof(int) * M) != cudaSuccess || mf_dmalloc(&dv, sizeof(int) * M) != cudaSuccess ||
+        mf_dmalloc(&dc, sizeof(i64) * M) != cudaSuccess) {
         cudaGetLastError();
         rc = fail(MF_ERR_NOMEM, "edge upload allocation failed (%lld edges)", m);
     } else if (m > 0 && (cudaMemcpy(du, u, sizeof(int) * m, cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -823,9 +915,9 @@ int mf_graph_create_from_edges(int n, long long m, const int32_t *u, const int32
     } else {
         rc = graph_from_device_edges(n, m, du, dv, dc, R, out);
     }
-    cudaFree(du);
-    cudaFree(dv);
-    cudaFree(dc);
+    mf_dfree(du);
+    mf_dfree(dv);
+    mf_dfree(dc);
     return rc;
 }
 
@@ -862,7 +954,7 @@ int mf_graph_load_file(const char *path, int R, mf_graph **out) {
     TextEdges te;
     do {
         if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaMalloc(&dtxt, (size_t)std::max<long long>(S, 1)) != cudaSuccess) {
+            mf_dmalloc(&dtxt, (size_t)std::max<long long>(S, 1)) != cudaSuccess) {
             cudaGetLastError();
             rc = fail(MF_ERR_NOMEM, "text staging for %lld bytes failed", S);
             break;
@@ -890,7 +982,7 @@ int mf_graph_load_file(const char *path, int R, mf_graph **out) {
             rc = fail(MF_ERR_IO, "%s: no valid \"n m\" header", path);
             break;
         }
-        cudaFree(dtxt);
+        mf_dfree(dtxt);
         dtxt = nullptr;
         if (2 * te.m > 0x7fffffffLL) {
             rc = fail(MF_ERR_ARG, "too many edges for int32 arc ids");
@@ -900,7 +992,7 @@ int mf_graph_load_file(const char *path, int R, mf_graph **out) {
     } while (0);
     fclose(f);
     mf_free_text_edges(te);
-    cudaFree(dtxt);
+    mf_dfree(dtxt);
     if (st) cudaStreamDestroy(st);
     return rc;
 }
@@ -923,14 +1015,14 @@ int mf_graph_repartition(mf_graph *g, int R) {
     g->d_graph = nullptr;
     std::vector<int> in_to_caller = g->old_id;
     int rc = partition_into(g, R, row, col, cap, rev, fwd, in_to_caller);
-    cudaFree(row);
-    cudaFree(col);
-    cudaFree(rev);
-    cudaFree(cap);
-    cudaFree(fwd);
-    cudaFree(ro);
-    cudaFree(rs);
-    cudaFree(dg);
+    mf_dfree(row);
+    mf_dfree(col);
+    mf_dfree(rev);
+    mf_dfree(cap);
+    mf_dfree(fwd);
+    mf_dfree(ro);
+    mf_dfree(rs);
+    mf_dfree(dg);
     return rc;
 }
 
@@ -938,12 +1030,12 @@ int mf_graph_destroy(mf_graph *g) {
     if (!g) return MF_OK;
     free_graph_arrays(g);
     g->pool.release();
-    cudaFree(g->d_err);
-    cudaFree(g->d_clocks);
-    cudaFree(g->d_out);
-    cudaFree(g->d_q);
-    cudaFreeHost(g->h_pin);
-    cudaFreeHost(g->h_out);
+    mf_dfree(g->d_err);
+    mf_dfree(g->d_clocks);
+    mf_dfree(g->d_out);
+    mf_dfree(g->d_q);
+    mf_hfree(g->h_pin);
+    mf_hfree(g->h_out);
     if (g->ev0) cudaEventDestroy(g->ev0);
     if (g->ev1) cudaEventDestroy(g->ev1);
     if (g->stream) cudaStreamDestroy(g->stream);
@@ -1050,41 +1142,55 @@ __global__ void k_kept_res(int n, const int *row, const int *col, const i64 *cap
 // strongly connected component of the highest-degree vertex, found by the
 // solver's own prune with s = t = pivot, and the pivot's forward / backward
 // closures (F / B bits per vertex).
+static int build_kept_cache(mf_graph *g, const mf_opts &o);
+
+// Builds the kept-set cache on first use.  Any failure frees what the build
+// allocated and marks the cache as tried: the error is returned once and
+// later solves run without the cache.
 static int ensure_kept_cache(mf_graph *g, const mf_opts &o) {
     if (g->kc_valid || g->kc_tried || o.prune_mode != 1 || !o.use_kept_cache) return MF_OK;
+    int rc = build_kept_cache(g, o);
+    if (rc) {
+        free_kept_cache(g);
+        g->kc_tried = true;
+        upload_dgraph(g);
+    }
+    return rc;
+}
+
+static int build_kept_cache(mf_graph *g, const mf_opts &o) {
     g->kc_tried = true;
     int n = g->n;
     KcOut ko{};
-    CK(cudaMalloc(&g->kc_in, n));
-    CK(cudaMalloc(&g->kc_img, sizeof(int) * (size_t)n));
-    CK(cudaMalloc(&g->kc_res, sizeof(i64) * (size_t)std::max<i64>(g->arcs, 1)));
+    CK(mf_dmalloc(&g->kc_in, n));
+    CK(mf_dmalloc(&g->kc_img, sizeof(int) * (size_t)n));
+    CK(mf_dmalloc(&g->kc_res, sizeof(i64) * (size_t)std::max<i64>(g->arcs, 1)));
     CK(cudaMemset(g->kc_in, 0, n));
-    CK(cudaMalloc(&g->kc_fb, n));
+    CK(mf_dmalloc(&g->kc_fb, n));
     ko.img = g->kc_img;
     ko.in = g->kc_in;
     ko.fb = g->kc_fb;
     KcOut *dko = nullptr;
-    CK(cudaMalloc(&dko, sizeof(KcOut)));
-    CK(cudaMemcpy(dko, &ko, sizeof(KcOut), cudaMemcpyHostToDevice));
+    CK(mf_dmalloc(&dko, sizeof(KcOut)));
+    if (cudaMemcpy(dko, &ko, sizeof(KcOut), cudaMemcpyHostToDevice) != cudaSuccess) {
+        mf_dfree(dko);
+        return fail(MF_ERR_CUDA, "kept-set cache set-up copy failed");
+    }
     int piv = g->pivot;
     QOut out;
     int rc = launch(g, g->pool, 1, &piv, &piv, false, o, KM_KEPTSET, dko, nullptr, 0, 0, &out);
-    cudaFree(dko);
-    if (rc) {
-        free_kept_cache(g);
-        g->kc_tried = true;
-        return rc;
-    }
+    mf_dfree(dko);
+    if (rc) return rc;
     g->kc_f = out.kept_front;
     g->kc_b = out.mask_n - out.kept_front;
     unsigned long long *darcs = nullptr;
-    CK(cudaMalloc(&darcs, sizeof(unsigned long long)));
+    DevScope tmp;
+    CK(tmp.alloc(&darcs, sizeof(unsigned long long)));
     CK(cudaMemset(darcs, 0, sizeof(unsigned long long)));
     k_kept_res<<<g->dev.sms * 8, 256, 0, g->stream>>>(n, g->row, g->col, g->cap, g->kc_in, g->kc_res, darcs);
     unsigned long long ka = 0;
     CK(cudaMemcpyAsync(&ka, darcs, sizeof(ka), cudaMemcpyDeviceToHost, g->stream));
     CK(cudaStreamSynchronize(g->stream));
-    cudaFree(darcs);
     g->kc_arcs = (i64)ka;
     g->kc_valid = out.mask_n >= 2;
     if (g->kc_valid) {
@@ -1212,9 +1318,9 @@ int mf_solve_batch_override(mf_graph *g, int nq, const int32_t *s, const int32_t
     const size_t ovn = (size_t)nq * (size_t)nb;
     int rc = MF_OK;
     do {
-        if (cudaMalloc(&du, sizeof(int) * nb) != cudaSuccess || cudaMalloc(&dv, sizeof(int) * nb) != cudaSuccess ||
-            cudaMalloc(&darc, sizeof(int) * nb) != cudaSuccess || cudaMalloc(&dgcap, sizeof(i64) * nb) != cudaSuccess ||
-            cudaMalloc(&dov, sizeof(i64) * ovn) != cudaSuccess || cudaMalloc(&dbad, sizeof(int)) != cudaSuccess) {
+        if (mf_dmalloc(&du, sizeof(int) * nb) != cudaSuccess || mf_dmalloc(&dv, sizeof(int) * nb) != cudaSuccess ||
+            mf_dmalloc(&darc, sizeof(int) * nb) != cudaSuccess || mf_dmalloc(&dgcap, sizeof(i64) * nb) != cudaSuccess ||
+            mf_dmalloc(&dov, sizeof(i64) * ovn) != cudaSuccess || mf_dmalloc(&dbad, sizeof(int)) != cudaSuccess) {
             cudaGetLastError();
             rc = fail(MF_ERR_NOMEM, "override buffers (%zu capacities) do not fit", ovn);
             break;
@@ -1259,12 +1365,12 @@ int mf_solve_batch_override(mf_graph *g, int nq, const int32_t *s, const int32_t
         }
         if (worst != MF_OK) rc = fail(worst, "a query ended with status %d", worst);
     } while (0);
-    cudaFree(du);
-    cudaFree(dv);
-    cudaFree(darc);
-    cudaFree(dgcap);
-    cudaFree(dov);
-    cudaFree(dbad);
+    mf_dfree(du);
+    mf_dfree(dv);
+    mf_dfree(darc);
+    mf_dfree(dgcap);
+    mf_dfree(dov);
+    mf_dfree(dbad);
     return rc;
 }
 
@@ -1341,10 +1447,10 @@ int mf_graph_load_binary(const char *path, mf_graph **out) {
     int *dbad = nullptr;
     do {
         const size_t AA = (size_t)std::max<i64>(A, 1);
-        if (cudaMalloc(&g->row, sizeof(int) * (n + 1)) || cudaMalloc(&g->col, sizeof(int) * AA) ||
-            cudaMalloc(&g->cap, sizeof(i64) * AA) || cudaMalloc(&g->rev, sizeof(int) * AA) ||
-            cudaMalloc(&g->fwd, AA) || cudaMalloc(&g->region_start, sizeof(int) * (R + 1)) ||
-            cudaMalloc(&g->region_of, sizeof(int) * n) || cudaMalloc(&dbad, sizeof(int))) {
+        if (mf_dmalloc(&g->row, sizeof(int) * (n + 1)) || mf_dmalloc(&g->col, sizeof(int) * AA) ||
+            mf_dmalloc(&g->cap, sizeof(i64) * AA) || mf_dmalloc(&g->rev, sizeof(int) * AA) ||
+            mf_dmalloc(&g->fwd, AA) || mf_dmalloc(&g->region_start, sizeof(int) * (R + 1)) ||
+            mf_dmalloc(&g->region_of, sizeof(int) * n) || mf_dmalloc(&dbad, sizeof(int))) {
             cudaGetLastError();
             rc = fail(MF_ERR_NOMEM, "graph allocation failed");
             break;
@@ -1410,7 +1516,7 @@ int mf_graph_load_binary(const char *path, mf_graph **out) {
         rc = finalize_graph(g);
     } while (0);
     fclose(f);
-    cudaFree(dbad);
+    mf_dfree(dbad);
     if (rc != MF_OK) {
         mf_graph_destroy(g);
         return rc;
@@ -1425,7 +1531,7 @@ int mf_graph_load_binary(const char *path, mf_graph **out) {
 int mf_debug_prune_mask(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, uint8_t *mask, int *kept) {
     if (!g || !mask) return fail(MF_ERR_ARG, "bad arguments");
     unsigned char *d = nullptr;
-    CK(cudaMalloc(&d, g->n));
+    CK(mf_dmalloc(&d, g->n));
     CK(cudaMemset(d, 0, g->n));
     int64_t f = 0;
     mf_stats st;
@@ -1440,14 +1546,14 @@ int mf_debug_prune_mask(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, 
         }
         if (kept) *kept = k;
     }
-    cudaFree(d);
+    mf_dfree(d);
     return rc;
 }
 
 int mf_debug_initial_heights(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, int32_t *heights) {
     if (!g || !heights) return fail(MF_ERR_ARG, "bad arguments");
     int *d = nullptr;
-    CK(cudaMalloc(&d, sizeof(int) * g->n));
+    CK(mf_dmalloc(&d, sizeof(int) * g->n));
     int64_t f = 0;
     mf_stats st;
     int rc = solve_common(g, 1, &s, &t, opts, &f, &st, KM_HEIGHTS, d, true);
@@ -1456,7 +1562,7 @@ int mf_debug_initial_heights(mf_graph *g, int32_t s, int32_t t, const mf_opts *o
         cudaMemcpy(h.data(), d, sizeof(int) * g->n, cudaMemcpyDeviceToHost);
         for (int x = 0; x < g->n; ++x) heights[x] = h[g->new_id[x]];
     }
-    cudaFree(d);
+    mf_dfree(d);
     return rc;
 }
 
@@ -1464,13 +1570,13 @@ int mf_solve_residual(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, in
                       int64_t *res, mf_stats *stats) {
     if (!g || !res) return fail(MF_ERR_ARG, "bad arguments");
     i64 *d = nullptr;
-    CK(cudaMalloc(&d, sizeof(i64) * (size_t)std::max<i64>(g->arcs, 1)));
+    CK(mf_dmalloc(&d, sizeof(i64) * (size_t)std::max<i64>(g->arcs, 1)));
     int64_t f = 0;
     mf_stats st;
     int rc = solve_common(g, 1, &s, &t, opts, &f, stats ? stats : &st, KM_RESIDUAL, d, true);
     if (rc == MF_OK && g->arcs) cudaMemcpy(res, d, sizeof(i64) * g->arcs, cudaMemcpyDeviceToHost);
     if (flow) *flow = f;
-    cudaFree(d);
+    mf_dfree(d);
     return rc;
 }
 
@@ -1494,10 +1600,11 @@ static int resolve_updates(mf_graph *g, int nb, const int32_t *u, const int32_t 
     }
     int *du = nullptr, *dv = nullptr, *darc = nullptr;
     i64 *dcap = nullptr;
-    CK(cudaMalloc(&du, sizeof(int) * nb));
-    CK(cudaMalloc(&dv, sizeof(int) * nb));
-    CK(cudaMalloc(&darc, sizeof(int) * nb));
-    CK(cudaMalloc(&dcap, sizeof(i64) * nb));
+    DevScope tmp;
+    CK(tmp.alloc(&du, sizeof(int) * nb));
+    CK(tmp.alloc(&dv, sizeof(int) * nb));
+    CK(tmp.alloc(&darc, sizeof(int) * nb));
+    CK(tmp.alloc(&dcap, sizeof(i64) * nb));
     CK(cudaMemcpy(du, ui.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(dv, vi.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
     k_find_arcs<<<(unsigned)((nb + 7) / 8), 256, 0, g->stream>>>(nb, du, dv, g->row, g->col, g->rev, g->fwd, g->cap, darc, dcap);
@@ -1506,10 +1613,6 @@ static int resolve_updates(mf_graph *g, int nb, const int32_t *u, const int32_t 
     CK(cudaMemcpyAsync(arc.data(), darc, sizeof(int) * nb, cudaMemcpyDeviceToHost, g->stream));
     CK(cudaMemcpyAsync(capv.data(), dcap, sizeof(i64) * nb, cudaMemcpyDeviceToHost, g->stream));
     CK(cudaStreamSynchronize(g->stream));
-    cudaFree(du);
-    cudaFree(dv);
-    cudaFree(darc);
-    cudaFree(dcap);
     // apply sequentially (clamp at 0 after each change), one entry per arc
     std::unordered_map<int, int> at;
     int skip = 0;
@@ -1546,7 +1649,7 @@ static int apply_updates(mf_graph *g, const std::vector<ArcUpdate> &ups, ArcUpda
         if (rc) return rc;
     }
     ArcUpdate *d = nullptr;
-    CK(cudaMalloc(&d, sizeof(ArcUpdate) * ups.size()));
+    CK(mf_dmalloc(&d, sizeof(ArcUpdate) * ups.size()));
     CK(cudaMemcpy(d, ups.data(), sizeof(ArcUpdate) * ups.size(), cudaMemcpyHostToDevice));
     k_apply_caps<<<((int)ups.size() + 255) / 256, 256, 0, g->stream>>>((int)ups.size(), d, g->cap);
     CK(cudaStreamSynchronize(g->stream));
@@ -1564,7 +1667,7 @@ int mf_update_caps(mf_graph *g, int nb, const int32_t *u, const int32_t *v, cons
     if (rc) return rc;
     ArcUpdate *d = nullptr;
     rc = apply_updates(g, ups, &d);
-    cudaFree(d);
+    mf_dfree(d);
     return rc;
 }
 
@@ -1661,7 +1764,7 @@ int mf_session_update(mf_session *ss, int nb, const int32_t *u, const int32_t *v
     if (const char *e = getenv("MF_REPAIR_MAX_UPDATES")) lim = atoll(e);
     if ((long long)ups.size() > lim) rc = session_run(ss, KM_SOLVE, nullptr, 0, flows, stats);
     else rc = session_run(ss, KM_REPAIR, d, (int)ups.size(), flows, stats);
-    cudaFree(d);
+    mf_dfree(d);
     return rc;
 }
 
@@ -1707,10 +1810,10 @@ static int server_launch(mf_server *sv) {
     CK(cudaMemsetAsync(sv->d_err, 0, sizeof(int), sv->stream));
     int ns = (int)sv->pool.host.size();
     unsigned *clk = nullptr;
-    CK(cudaMalloc(&clk, sizeof(unsigned) * ns));
+    CK(mf_dmalloc(&clk, sizeof(unsigned) * ns));
     k_prepare_slots<<<(ns + 127) / 128, 128, 0, sv->stream>>>(sv->pool.dev, ns, clk);
     CK(cudaStreamSynchronize(sv->stream));
-    cudaFree(clk);
+    mf_dfree(clk);
     *(volatile int *)sv->h_stop = 0;
     KParams p{};
     p.graphs = sv->d_graphs;
@@ -1816,19 +1919,19 @@ int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int ma
         delete sv;
         return rc;
     }
-    if (cudaMalloc(&sv->d_graphs, sizeof(DGraph) * ngraphs) != cudaSuccess ||
+    if (mf_dmalloc(&sv->d_graphs, sizeof(DGraph) * ngraphs) != cudaSuccess ||
         cudaMemcpy(sv->d_graphs, dg.data(), sizeof(DGraph) * ngraphs, cudaMemcpyHostToDevice) != cudaSuccess) {
         sv->pool.release();
         delete sv;
         return fail(MF_ERR_NOMEM, "server graph table");
     }
     sv->cap = 1 << 20;
-    bool ok = cudaHostAlloc(&sv->h_tail, sizeof(int) * 2, cudaHostAllocMapped) == cudaSuccess &&
-              cudaHostAlloc(&sv->h_done, sizeof(int) * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
-              cudaHostAlloc(&sv->h_req, sizeof(int4) * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
-              cudaHostAlloc(&sv->h_t0, sizeof(u64) * 2 * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
-              cudaHostAlloc(&sv->h_out, sizeof(QOut) * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
-              cudaMalloc(&sv->d_qnext, sizeof(int) * 2) == cudaSuccess;
+    bool ok = mf_hostalloc(&sv->h_tail, sizeof(int) * 2, cudaHostAllocMapped) == cudaSuccess &&
+              mf_hostalloc(&sv->h_done, sizeof(int) * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
+              mf_hostalloc(&sv->h_req, sizeof(int4) * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
+              mf_hostalloc(&sv->h_t0, sizeof(u64) * 2 * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
+              mf_hostalloc(&sv->h_out, sizeof(QOut) * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
+              mf_dmalloc(&sv->d_qnext, sizeof(int) * 2) == cudaSuccess;
     if (!ok) {
         mf_server_destroy(sv);
         return fail(MF_ERR_NOMEM, "server ring allocation failed");
@@ -1918,13 +2021,13 @@ int mf_server_destroy(mf_server *sv) {
     std::atomic_thread_fence(std::memory_order_seq_cst);
     if (sv->stream) cudaStreamSynchronize(sv->stream);
     sv->pool.release();
-    cudaFree(sv->d_graphs);
-    cudaFree(sv->d_qnext);
-    cudaFreeHost(sv->h_tail);
-    cudaFreeHost(sv->h_done);
-    cudaFreeHost(sv->h_req);
-    cudaFreeHost(sv->h_t0);
-    cudaFreeHost(sv->h_out);
+    mf_dfree(sv->d_graphs);
+    mf_dfree(sv->d_qnext);
+    mf_hfree(sv->h_tail);
+    mf_hfree(sv->h_done);
+    mf_hfree(sv->h_req);
+    mf_hfree(sv->h_t0);
+    mf_hfree(sv->h_out);
     if (sv->done_ev) cudaEventDestroy(sv->done_ev);
     if (sv->stream) cudaStreamDestroy(sv->stream);
     delete sv;

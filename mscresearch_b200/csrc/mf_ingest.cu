@@ -27,6 +27,7 @@
 #include <cstdio>
 #include <vector>
 
+#include "mf_alloc.h"
 #include "mf_build.cuh"
 
 namespace {
@@ -248,13 +249,13 @@ cudaError_t mf_device_csr(int n, i64 m, const int *u, const int *v, const i64 *c
     for (unsigned x = (unsigned)n; x; x >>= 8) ++passes;
     do {
         const size_t NN = (size_t)std::max<i64>(N, 1);
-        if ((e = cudaMalloc(&key, sizeof(int) * NN)) || (e = cudaMalloc(&val, sizeof(int) * NN)) ||
-            (e = cudaMalloc(&key2, sizeof(int) * NN)) || (e = cudaMalloc(&val2, sizeof(int) * NN)) ||
-            (e = cudaMalloc(&cnt, sizeof(int) * (size_t)nbins)) ||
-            (e = cudaMalloc(&off, sizeof(int) * ((size_t)nbins + 1))) ||
-            (e = cudaMalloc(&tmp, sizeof(int) * ((size_t)std::max(nbins, n + 1) / 1024 + 2))) ||
-            (e = cudaMalloc(&deg, sizeof(int) * ((size_t)n + 1))) ||
-            (e = cudaMalloc(&out.row, sizeof(int) * ((size_t)n + 1))))
+        if ((e = mf_dmalloc(&key, sizeof(int) * NN)) || (e = mf_dmalloc(&val, sizeof(int) * NN)) ||
+            (e = mf_dmalloc(&key2, sizeof(int) * NN)) || (e = mf_dmalloc(&val2, sizeof(int) * NN)) ||
+            (e = mf_dmalloc(&cnt, sizeof(int) * (size_t)nbins)) ||
+            (e = mf_dmalloc(&off, sizeof(int) * ((size_t)nbins + 1))) ||
+            (e = mf_dmalloc(&tmp, sizeof(int) * ((size_t)std::max(nbins, n + 1) / 1024 + 2))) ||
+            (e = mf_dmalloc(&deg, sizeof(int) * ((size_t)n + 1))) ||
+            (e = mf_dmalloc(&out.row, sizeof(int) * ((size_t)n + 1))))
             break;
         if (m > 0) k_halfarcs<<<grid_of(m, 256), 256, 0, st>>>(n, m, u, v, c, key, val);
         for (int ps = 0; ps < passes && N > 0; ++ps) {
@@ -274,9 +275,9 @@ cudaError_t mf_device_csr(int n, i64 m, const int *u, const int *v, const i64 *c
             break;
         out.arcs = arcs;
         const size_t A = (size_t)std::max(arcs, 1);
-        if ((e = cudaMalloc(&out.col, sizeof(int) * A)) || (e = cudaMalloc(&out.cap, sizeof(i64) * A)) ||
-            (e = cudaMalloc(&out.rev, sizeof(int) * A)) || (e = cudaMalloc(&out.fwd, A)) ||
-            (e = cudaMalloc(&pos, sizeof(int) * NN)))
+        if ((e = mf_dmalloc(&out.col, sizeof(int) * A)) || (e = mf_dmalloc(&out.cap, sizeof(i64) * A)) ||
+            (e = mf_dmalloc(&out.rev, sizeof(int) * A)) || (e = mf_dmalloc(&out.fwd, A)) ||
+            (e = mf_dmalloc(&pos, sizeof(int) * NN)))
             break;
         if (arcs > 0) {
             k_pos_of<<<grid_of(arcs, 256), 256, 0, st>>>(arcs, val, pos);
@@ -286,25 +287,25 @@ cudaError_t mf_device_csr(int n, i64 m, const int *u, const int *v, const i64 *c
         e = cudaStreamSynchronize(st);
         if (e == cudaSuccess) e = cudaGetLastError();
     } while (0);
-    cudaFree(key);
-    cudaFree(val);
-    cudaFree(key2);
-    cudaFree(val2);
-    cudaFree(cnt);
-    cudaFree(off);
-    cudaFree(tmp);
-    cudaFree(deg);
-    cudaFree(pos);
+    mf_dfree(key);
+    mf_dfree(val);
+    mf_dfree(key2);
+    mf_dfree(val2);
+    mf_dfree(cnt);
+    mf_dfree(off);
+    mf_dfree(tmp);
+    mf_dfree(deg);
+    mf_dfree(pos);
     if (e != cudaSuccess) mf_free_dev_csr(out);
     return e;
 }
 
 void mf_free_dev_csr(DevCsr &c) {
-    cudaFree(c.row);
-    cudaFree(c.col);
-    cudaFree(c.cap);
-    cudaFree(c.rev);
-    cudaFree(c.fwd);
+    mf_dfree(c.row);
+    mf_dfree(c.col);
+    mf_dfree(c.cap);
+    mf_dfree(c.rev);
+    mf_dfree(c.fwd);
     c = DevCsr{};
 }
 
@@ -318,10 +319,10 @@ cudaError_t mf_parse_graph_text(const unsigned char *txt, i64 S, cudaStream_t st
     if (nb64 > 0x7fffffffLL) return cudaErrorInvalidValue;
     const int nb = (int)nb64;
     do {
-        if ((e = cudaMalloc(&bcount, sizeof(int) * (size_t)nb)) ||
-            (e = cudaMalloc(&boff, sizeof(int) * ((size_t)nb + 1))) ||
-            (e = cudaMalloc(&tmp, sizeof(int) * ((size_t)nb / 1024 + 2))) || (e = cudaMalloc(&ntok, sizeof(int))) ||
-            (e = cudaMalloc(&first_bad, sizeof(u64))))
+        if ((e = mf_dmalloc(&bcount, sizeof(int) * (size_t)nb)) ||
+            (e = mf_dmalloc(&boff, sizeof(int) * ((size_t)nb + 1))) ||
+            (e = mf_dmalloc(&tmp, sizeof(int) * ((size_t)nb / 1024 + 2))) || (e = mf_dmalloc(&ntok, sizeof(int))) ||
+            (e = mf_dmalloc(&first_bad, sizeof(u64))))
             break;
         const u64 none = ~0ull;
         if ((e = cudaMemcpyAsync(first_bad, &none, sizeof(u64), cudaMemcpyHostToDevice, st)) ||
@@ -333,7 +334,7 @@ cudaError_t mf_parse_graph_text(const unsigned char *txt, i64 S, cudaStream_t st
         if ((e = cudaMemcpyAsync(&total, boff + nb, sizeof(int), cudaMemcpyDeviceToHost, st)) ||
             (e = cudaStreamSynchronize(st)))
             break;
-        if ((e = cudaMalloc(&tok, sizeof(i64) * (size_t)std::max(total, 2)))) break;
+        if ((e = mf_dmalloc(&tok, sizeof(i64) * (size_t)std::max(total, 2)))) break;
         k_tok_values<<<nb, TOK_B, 0, st>>>(S, txt, boff, first_bad, tok, ntok);
         int K = 0;
         i64 hdr[2] = {0, 0};
@@ -351,27 +352,27 @@ cudaError_t mf_parse_graph_text(const unsigned char *txt, i64 S, cudaStream_t st
         i64 m = std::min<i64>(std::max<i64>(out.m_header, 0), (K - 2) / 3);
         out.m = m;
         const size_t M = (size_t)std::max<i64>(m, 1);
-        if ((e = cudaMalloc(&out.u, sizeof(int) * M)) || (e = cudaMalloc(&out.v, sizeof(int) * M)) ||
-            (e = cudaMalloc(&out.c, sizeof(i64) * M)))
+        if ((e = mf_dmalloc(&out.u, sizeof(int) * M)) || (e = mf_dmalloc(&out.v, sizeof(int) * M)) ||
+            (e = mf_dmalloc(&out.c, sizeof(i64) * M)))
             break;
         if (m > 0) k_tok_edges<<<grid_of(m, 256), 256, 0, st>>>(m, tok, out.u, out.v, out.c);
         e = cudaStreamSynchronize(st);
         if (e == cudaSuccess) e = cudaGetLastError();
     } while (0);
-    cudaFree(bcount);
-    cudaFree(boff);
-    cudaFree(tmp);
-    cudaFree(ntok);
-    cudaFree(first_bad);
-    cudaFree(tok);
+    mf_dfree(bcount);
+    mf_dfree(boff);
+    mf_dfree(tmp);
+    mf_dfree(ntok);
+    mf_dfree(first_bad);
+    mf_dfree(tok);
     if (e != cudaSuccess) mf_free_text_edges(out);
     return e;
 }
 
 void mf_free_text_edges(TextEdges &t) {
-    cudaFree(t.u);
-    cudaFree(t.v);
-    cudaFree(t.c);
+    mf_dfree(t.u);
+    mf_dfree(t.v);
+    mf_dfree(t.c);
     t.u = t.v = nullptr;
     t.c = nullptr;
 }

@@ -15,14 +15,25 @@
 // call's contents, so calls whose work overlaps on the GPU (concurrent calls
 // from several host threads, or on several streams of one device) race and
 // must be serialized by the caller.
+//
+// Before the solve, a check kernel validates the caller's CSR (offsets,
+// head and reverse-arc ranges, the reverse pairing, non-negative
+// capacities), so a malformed graph is rejected with MF_ERR_ARG instead of
+// steering the solver's indexing outside its scratch regions.
 #include <cstdio>
 #include <cstring>
 
 #include "../../include/maxflow_b200.h"
 #include "mf_solver.cuh"
 
-// mf_api.cu: sets the text returned by mf_last_error_string() on this thread.
+#include <mutex>
+
+// mf_api.cu: the last-error text of this thread, and the option resolution,
+// launch time limit and status mapping every entry point shares.
 void mf_set_last_error(const char *msg);
+KOpts mf_resolve_opts(const mf_opts &o, int avg_deg);
+u64 mf_launch_time_limit_ns();
+int mf_status_from_err(int e);
 
 namespace {
 
@@ -66,10 +77,47 @@ constexpr size_t NA_BYTES = OFF_BITS + na_align(sizeof(unsigned) * 5 * ((NA_MAX_
 // cudaGetSymbolAddress, once per device (na_base below).
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
 
+// CSR defects found by k_na_check (bits of the check word).
+#define NA_BAD_ROW 1   // offsets not 0 .. arcs, or decreasing
+#define NA_BAD_COL 2   // head outside [0, n)
+#define NA_BAD_REV 4   // reverse arc outside [0, arcs), outside its head's range, or not paired back
+#define NA_BAD_CAP 8   // negative capacity
+
+// One warp per vertex: its offsets, then every arc e = v -> w: w in [0, n),
+// r = rev[e] inside w's arc range, col[r] == v, rev[r] == e, cap[e] >= 0.
+// Every load is guarded by the checks before it, so a malformed CSR is
+// reported, never indexed out of bounds.
+__global__ void k_na_check(int n, long long arcs, const int *row, const int *col, const int *rev,
+                           const i64 *cap, int *bad) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
+        const long long b = row[v], e1 = row[v + 1];
+        if (b < 0 || b > e1 || e1 > arcs || (v == 0 && b != 0) || (v == n - 1 && e1 != arcs)) {
+            if (lane == 0) atomicOr(bad, NA_BAD_ROW);
+            continue;
+        }
+        int flags = 0;
+        for (long long e = b + lane; e < e1; e += 32) {
+            const int w = col[e];
+            if (cap[e] < 0) flags |= NA_BAD_CAP;
+            if (w < 0 || w >= n) {
+                flags |= NA_BAD_COL;
+                continue;
+            }
+            const long long r = rev[e];
+            if (r < 0 || r >= arcs || r < row[w] || r >= row[w + 1] || col[r] != v || rev[r] != e)
+                flags |= NA_BAD_REV;
+        }
+        if (flags) atomicOr(bad, flags);
+    }
+}
+
 namespace {
 
 char *na_base[64];  // per device: address of g_noalloc_scratch
 int na_sms[64], na_bps[64];
+std::mutex na_mu;   // guards the first-call set-up of every device
 
 thread_local char na_msg[256];
 int na_fail(int code, const char *msg) {
@@ -77,9 +125,13 @@ int na_fail(int code, const char *msg) {
     return code;
 }
 
-// First call on a device: resolve the scratch address and zero it.
+// First call on a device: resolve the scratch address and zero it.  Under
+// na_mu, so two host threads making their first call at once set it up
+// exactly once.  The address is kept for the life of the process: after a
+// cudaDeviceReset of that device it would be stale (unsupported).
 int na_setup(int dev, cudaStream_t st) {
     if (dev < 0 || dev >= 64) return na_fail(MF_ERR_ARG, "mf_solve_csr_noalloc: device index out of range");
+    std::lock_guard<std::mutex> lk(na_mu);
     if (na_base[dev]) return MF_OK;
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -136,6 +188,35 @@ extern "C" int mf_solve_csr_noalloc(int n, long long arcs, const int32_t *d_row,
     if (opts) o = *opts;
     else mf_opts_default(&o);
 
+    // validate the caller's CSR on the device (the check word is ctl[4])
+    {
+        int *dbad = (int *)(b + OFF_CTL) + 4;
+        int hbad = 0;
+        cudaError_t e = cudaMemsetAsync(dbad, 0, sizeof(int), st);
+        if (e == cudaSuccess) {
+            k_na_check<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(n, arcs, d_row, d_col, d_rev,
+                                                               (const i64 *)d_cap, dbad);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&hbad, dbad, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            snprintf(na_msg, sizeof na_msg, "mf_solve_csr_noalloc: CSR check failed: %s", cudaGetErrorString(e));
+            mf_set_last_error(na_msg);
+            return MF_ERR_CUDA;
+        }
+        if (hbad) {
+            snprintf(na_msg, sizeof na_msg,
+                     "mf_solve_csr_noalloc: malformed CSR:%s%s%s%s",
+                     (hbad & NA_BAD_ROW) ? " row offsets not 0..arcs non-decreasing;" : "",
+                     (hbad & NA_BAD_COL) ? " head outside [0, n);" : "",
+                     (hbad & NA_BAD_REV) ? " reverse arcs not paired;" : "",
+                     (hbad & NA_BAD_CAP) ? " negative capacity;" : "");
+            mf_set_last_error(na_msg);
+            return MF_ERR_ARG;
+        }
+    }
+
     DGraph g{n, 1, arcs, d_row, d_col, d_rev, (const i64 *)d_cap, (const int *)(b + OFF_ROF)};
     DSlot sl;
     sl.res = (i64 *)(b + OFF_RES);
@@ -169,25 +250,7 @@ extern "C" int mf_solve_csr_noalloc(int n, long long arcs, const int32_t *d_row,
         return MF_ERR_CUDA;
     }
 
-    KOpts k{};
-    k.bu_factor = 56;
-    int avg = (int)(arcs / n);
-    k.K = o.kernel_cycles > 0 ? o.kernel_cycles : (avg > 4 ? avg : 4);
-    k.gr_freq = o.gr_freq > 0 ? o.gr_freq : 1;
-    k.gr_alpha = o.gr_work_alpha;
-    k.prune_mode = o.prune_mode;
-    k.pp_switch = o.path_push_switch;
-    k.max_path = o.max_path_len > 0 ? o.max_path_len : 1;
-    k.use_pp = o.use_path_push;
-    k.use_hot = o.use_hot_sweep;
-    k.hot_k = o.hot_regions > 0 ? o.hot_regions : 1;
-    k.use_rm = o.use_rm;
-    k.rm_freq = o.rm_freq > 0 ? o.rm_freq : 1;
-    k.h_cut = o.h_cut;
-    k.stagnate = o.stagnate_rounds > 0 ? o.stagnate_rounds : 1;
-    k.force_rm = o.force_rm;
-    k.force_pp = o.force_path_push;
-    k.iter_max = o.iter_max > 0 ? o.iter_max : 20000000;
+    const KOpts k = mf_resolve_opts(o, (int)(arcs / n));
 
     int *dctl = (int *)(b + OFF_CTL);
     KParams p{};
@@ -201,7 +264,7 @@ extern "C" int mf_solve_csr_noalloc(int n, long long arcs, const int32_t *d_row,
     p.out = (QOut *)(b + OFF_OUT);
     p.err = dctl;
     p.bar_limit_ns = 20ull * 1000 * 1000 * 1000;
-    p.time_limit_ns = 600ull * 1000 * 1000 * 1000;
+    p.time_limit_ns = mf_launch_time_limit_ns();
     p.o = k;
     p.mode = KM_SOLVE;
     cudaError_t le = cudaSuccess;
@@ -226,7 +289,7 @@ extern "C" int mf_solve_csr_noalloc(int n, long long arcs, const int32_t *d_row,
     if (herr) {
         snprintf(na_msg, sizeof na_msg, "mf_solve_csr_noalloc: device solve aborted (status %d)", herr);
         mf_set_last_error(na_msg);
-        return herr == 6 ? MF_ERR_TIMEOUT : MF_ERR_CUDA;
+        return mf_status_from_err(herr);
     }
     // stamps are compared against a monotonic 32-bit clock kept in the
     // scratch; zero them (and the clock) well before it could wrap
@@ -239,7 +302,7 @@ extern "C" int mf_solve_csr_noalloc(int n, long long arcs, const int32_t *d_row,
     if (flow) *flow = q.flow;
     if (stats) {
         stats->flow = q.flow;
-        stats->status = q.status;
+        stats->status = mf_status_from_err(q.status);
         stats->mask_vertices = q.mask_n;
         stats->mask_arcs = q.mask_arcs;
         stats->rounds = q.rounds;
@@ -252,7 +315,7 @@ extern "C" int mf_solve_csr_noalloc(int n, long long arcs, const int32_t *d_row,
     if (q.status != 0) {
         snprintf(na_msg, sizeof na_msg, "mf_solve_csr_noalloc: solve ended with status %d", q.status);
         mf_set_last_error(na_msg);
-        return q.status;
+        return mf_status_from_err(q.status);
     }
     return MF_OK;
 }

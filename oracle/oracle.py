@@ -18,7 +18,8 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-if not os.path.exists(LIB):
+if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(
+        os.path.getmtime(os.path.join(HERE, f)) for f in ("oracle.c", "gen.c")):
     build()
 _lib = C.CDLL(LIB)
 
@@ -43,6 +44,11 @@ _sig = {
     "or_dinic_batch": (None, [C.c_int, i32p, i32p, i64p, i32p, C.c_int, i32p, i32p, i64p, C.c_int]),
     "or_push_relabel": (C.c_longlong, [C.c_int, i32p, i32p, i64p, i32p, C.c_int, C.c_int, i64p]),
     "or_certify": (C.c_int, [C.c_int, i32p, i32p, i64p, i32p, C.c_int, C.c_int, i64p, C.c_longlong, C.c_int, C.POINTER(C.c_longlong)]),
+    "gn_rmat": (C.c_longlong, [C.c_int, C.c_longlong, C.c_double, C.c_double, C.c_double, C.c_longlong, C.c_longlong,
+                               C.c_uint64, i32p, i32p, i64p]),
+    "gn_queries_hub": (C.c_int, [C.c_int, C.c_longlong, i32p, i32p, C.c_int, C.c_int, C.c_uint64, i32p, i32p]),
+    "gn_write_graph_txt": (C.c_int, [C.c_char_p, C.c_int, C.c_longlong, i32p, i32p, i64p]),
+    "gn_write_test_txt": (C.c_int, [C.c_char_p, C.c_int, i32p, i32p]),
 }
 for _n, (_r, _a) in _sig.items():
     _f = getattr(_lib, _n)
@@ -211,3 +217,39 @@ def certify(g, s, t, res, value, require_flow=False):
     rc = _lib.or_certify(*g.args(), int(s), int(t), _p(res, C.c_int64), int(value), int(require_flow),
                          C.byref(cut))
     return rc, cut.value
+
+
+# ---- workload generators (the engine's seeded generators restated, gen.c) --
+
+def gen_rmat(scale, m, a=0.57, b=0.19, c=0.19, lo=1, hi=1000, seed=1):
+    u = np.zeros(max(m, 1), np.int32)
+    v = np.zeros(max(m, 1), np.int32)
+    cp = np.zeros(max(m, 1), np.int64)
+    k = _lib.gn_rmat(int(scale), int(m), a, b, c, int(lo), int(hi), int(seed), _p(u, C.c_int32), _p(v, C.c_int32),
+                     _p(cp, C.c_int64))
+    if k < 0:
+        raise ValueError("gn_rmat: bad arguments")
+    return u[:k].copy(), v[:k].copy(), cp[:k].copy()
+
+
+def gen_queries_hub(n, u, v, nhub, nuni, seed=1):
+    u, v = _c(u, np.int32), _c(v, np.int32)
+    s = np.zeros(max(nhub + nuni, 1), np.int32)
+    t = np.zeros(max(nhub + nuni, 1), np.int32)
+    if _lib.gn_queries_hub(int(n), len(u), _p(u, C.c_int32), _p(v, C.c_int32), int(nhub), int(nuni), int(seed),
+                           _p(s, C.c_int32), _p(t, C.c_int32)) != 0:
+        raise ValueError("gn_queries_hub: bad arguments")
+    return s[:nhub + nuni].copy(), t[:nhub + nuni].copy()
+
+
+def write_graph_txt(path, n, u, v, cap):
+    u, v, cap = _c(u, np.int32), _c(v, np.int32), _c(cap, np.int64)
+    if _lib.gn_write_graph_txt(path.encode(), int(n), len(u), _p(u, C.c_int32), _p(v, C.c_int32),
+                               _p(cap, C.c_int64)) != 0:
+        raise IOError(path)
+
+
+def write_test_txt(path, s, t):
+    s, t = _c(s, np.int32), _c(t, np.int32)
+    if _lib.gn_write_test_txt(path.encode(), len(s), _p(s, C.c_int32), _p(t, C.c_int32)) != 0:
+        raise IOError(path)

@@ -192,3 +192,44 @@ def test_boundary_core_is_not_flow_preserving():
     sub, o2s, _ = O.induced_subgraph(g, mk)
     assert O.dinic(g, 0, 9) == 5
     assert O.dinic(sub, o2s[0], o2s[9]) == 0
+
+
+def test_checker_generators_equal_engine_generators(tmp_path):
+    """The reference arm of bench.py writes the reference program's inputs
+    with the oracle's generators (so its process never loads the engine's
+    library); they must produce exactly the engine's workload: the same
+    R-MAT arrays, the same query mix, byte-identical graph.txt / test.txt."""
+    import mscresearch_b200 as mf
+    for scale, m, seed in ((10, 8192, 3), (14, 16 << 14, 1), (16, 300001, 77)):
+        u1, v1, c1 = mf.gen_rmat(scale, m, 0.57, 0.19, 0.19, 1, 1000, seed)
+        u2, v2, c2 = O.gen_rmat(scale, m, 0.57, 0.19, 0.19, 1, 1000, seed)
+        assert np.array_equal(u1, u2) and np.array_equal(v1, v2) and np.array_equal(c1, c2)
+        n = 1 << scale
+        s1, t1 = mf.gen_queries_hub(n, u1, v1, 16, 16, seed + 5)
+        s2, t2 = O.gen_queries_hub(n, u2, v2, 16, 16, seed + 5)
+        assert np.array_equal(s1, s2) and np.array_equal(t1, t2)
+        mf.write_graph_txt(str(tmp_path / "g1.txt"), n, u1, v1, c1)
+        O.write_graph_txt(str(tmp_path / "g2.txt"), n, u2, v2, c2)
+        assert (tmp_path / "g1.txt").read_bytes() == (tmp_path / "g2.txt").read_bytes()
+        mf.write_test_txt(str(tmp_path / "t1.txt"), s1, t1)
+        O.write_test_txt(str(tmp_path / "t2.txt"), s2, t2)
+        assert (tmp_path / "t1.txt").read_bytes() == (tmp_path / "t2.txt").read_bytes()
+
+
+@pytest.mark.parametrize("d", CASES, ids=[os.path.basename(x) for x in CASES])
+def test_reference_mismatch_classifier_on_golden_logs(d):
+    """bench.py's reference arm classifies each reference/oracle mismatch from
+    the reference's own log.  On the recorded B200 runs every known mismatch
+    (ref_mismatch.txt) must come out as 'stale-topology' (RA:1303-1331)."""
+    import bench
+    p = os.path.join(d, "ref_res_mt.txt")
+    log = os.path.join(d, "ref_log_static.txt")
+    if not (os.path.exists(p) and os.path.exists(log)):
+        pytest.skip("no reference output recorded for this case")
+    g, s, t, exp = load_case(d)
+    ref = np.loadtxt(p, dtype=np.int64, ndmin=2)[:, 0]
+    if not all(0 <= a < g.n and 0 <= b < g.n and a != b for a, b in zip(s, t)):
+        pytest.skip("case has invalid queries (no log line for them)")
+    bad = [i for i in range(len(exp)) if ref[i] != exp[i]]
+    cls = bench.classify_reference_mismatches(open(log).read(), g.n, g.arcs, bad)
+    assert all(c == "stale-topology" for c in cls.values()), cls
