@@ -266,24 +266,49 @@ int mf_session_destroy(mf_session *ss);
 
 /* ---- serving ------------------------------------------------------------ */
 
-/* Continuous-batching server over several device-resident graphs.  A
- * persistent kernel pulls requests from a host-written ring; requests that
- * arrive while others run are admitted as soon as a residual slot frees up.
- * Slots are sized for the largest graph and their number is chosen from free
- * HBM at creation (max_slots caps it; 0 = as many as fit, up to the GPU's
- * query groups). */
+/* Continuous-batching server over several device-resident graphs (the
+ * reference's dynamic mode, RA:2844-2916, grown into a request loop; its
+ * capacity updates replace the unwired incremental_update_max_flow_with_state,
+ * RA:2273-2335).  One persistent kernel takes requests from a host-written
+ * ring in ticket order: (s,t) queries and capacity-update batches.  Requests
+ * that arrive while others run are admitted as soon as a query group with a
+ * residual slot frees up.  Slots are sized for the largest graph and
+ * admitted by free HBM as requests open up: the server starts with up to 4
+ * and, whenever more requests are open than slots exist, allocates another
+ * if cudaMemGetInfo shows room (85 % of free HBM), up to max_slots (0 = one
+ * per query group of the GPU).  The ring holds 65536 requests (environment
+ * variable MF_SERVER_RING sets another size): a ticket's entry is reused
+ * once the ticket `ring size` later is submitted, so poll each result before
+ * that; a submit while that many requests are still unfinished returns
+ * MF_ERR_NOMEM.  The graphs must not be used through other entry points
+ * while the server exists; after mf_server_destroy they are usable again
+ * with the capacities the served updates left. */
 typedef struct mf_server mf_server;
 int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int max_slots,
                      mf_server **out);
+/* Slots admitted so far. */
 int mf_server_slots(const mf_server *sv, int *slots);
-/* Enqueue one request; returns its ticket (0,1,2,...) in *ticket. */
+/* Enqueue one query; returns its ticket (0,1,2,...) in *ticket.  It is
+ * answered on the graph as left by every update batch submitted before it
+ * on that graph, and by none submitted after it. */
 int mf_server_submit(mf_server *sv, int graph, int32_t s, int32_t t, long long *ticket);
+/* Enqueue a capacity-update batch on one graph: arc u[i] -> v[i] (first
+ * matching forward arc, caller ids) gets cap += delta[i], clamped at 0 after
+ * each change, in order (mf_update_caps semantics; pairs with no such arc
+ * are skipped).  It is applied on the device after every query submitted
+ * before it on that graph has finished and before any query submitted after
+ * it starts; queries on other graphs run on meanwhile.  Its ticket polls
+ * done (flow 0) once applied.  The batch's distinct (u, v) pairs must fit
+ * the update arena (1048576 entries; MF_SERVER_UPDATE_ARENA sets another). */
+int mf_server_update(mf_server *sv, int graph, int nb, const int32_t *u, const int32_t *v,
+                     const int64_t *delta, long long *ticket);
 /* Non-blocking: 1 in *done when the ticket finished (flow, device latency in
  * ms from admission to completion, status). */
 int mf_server_poll(mf_server *sv, long long ticket, int *done, int64_t *flow, double *latency_ms,
                    int *status);
 /* Block until every submitted request has finished. */
 int mf_server_drain(mf_server *sv);
+/* Stops the kernel (requests not yet started are dropped: drain first). */
 int mf_server_destroy(mf_server *sv);
 
 /* ---- autotuning ---------------------------------------------------------- */

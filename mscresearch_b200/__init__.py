@@ -293,6 +293,14 @@ class Server:
         _check(lib.mf_server_submit(self._h, int(graph), int(s), int(t), C.byref(tk)))
         return tk.value
 
+    def update(self, graph, u, v, delta):
+        """Enqueue a capacity-update batch on `graph`; returns its ticket."""
+        u, v, d = _i32(u), _i32(v), _i64(delta)
+        tk = C.c_longlong()
+        _check(lib.mf_server_update(self._h, int(graph), len(u), _p(u, C.c_int32), _p(v, C.c_int32),
+                                    _p(d, C.c_int64), C.byref(tk)))
+        return tk.value
+
     def poll(self, ticket):
         done, f, lat, st = C.c_int(), C.c_int64(), C.c_double(), C.c_int()
         _check(lib.mf_server_poll(self._h, int(ticket), C.byref(done), C.byref(f), C.byref(lat), C.byref(st)))
@@ -305,6 +313,12 @@ class Server:
         if self._h:
             lib.mf_server_destroy(self._h)
             self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
     def __del__(self):
         try:

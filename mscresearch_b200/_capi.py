@@ -110,6 +110,7 @@ SIGNATURES = {
     "mf_server_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(MfOpts), C.c_int, C.POINTER(C.c_void_p)]),
     "mf_server_slots": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "mf_server_submit": (C.c_int, [C.c_void_p, C.c_int, C.c_int32, C.c_int32, C.POINTER(C.c_longlong)]),
+    "mf_server_update": (C.c_int, [C.c_void_p, C.c_int, C.c_int, i32p, i32p, i64p, C.POINTER(C.c_longlong)]),
     "mf_server_poll": (C.c_int, [C.c_void_p, C.c_longlong, C.POINTER(C.c_int), i64p, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     "mf_server_drain": (C.c_int, [C.c_void_p]),
     "mf_server_destroy": (C.c_int, [C.c_void_p]),

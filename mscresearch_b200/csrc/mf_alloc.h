@@ -18,6 +18,11 @@ cudaError_t mf_dfree(void *p);                               // cudaFree
 cudaError_t mf_hmalloc_raw(void **p, size_t bytes);          // cudaMallocHost
 cudaError_t mf_hostalloc_raw(void **p, size_t bytes, unsigned flags);  // cudaHostAlloc
 cudaError_t mf_hfree(void *p);                               // cudaFreeHost
+// Stream-ordered device allocation (cudaMallocAsync / cudaFreeAsync): the
+// server admits residual slots with it on a side stream while its
+// persistent kernel runs.
+cudaError_t mf_dmalloc_async_raw(void **p, size_t bytes, cudaStream_t st);
+cudaError_t mf_dfree_async(void *p, cudaStream_t st);
 
 template <class T>
 inline cudaError_t mf_dmalloc(T **p, size_t bytes) {

@@ -16,6 +16,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <map>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -91,6 +93,38 @@ size_t slot_bytes(int n, i64 arcs, int nhub) {
     return b;
 }
 
+// The arrays of one residual slot inside one allocation of slot_bytes(),
+// each 256-byte aligned, in this order (the residuals first: everything
+// after them is what a new slot must have zeroed).
+DSlot carve_slot(char *p, int n, i64 arcs, int nhub) {
+    auto take = [&](size_t x) {
+        char *r = p;
+        p += (x + 255) & ~(size_t)255;
+        return (void *)r;
+    };
+    DSlot s;
+    s.res = (i64 *)take(sizeof(i64) * (size_t)std::max<i64>(arcs, 1));
+    s.ex = (i64 *)take(sizeof(i64) * (size_t)n);
+    s.h = (int *)take(sizeof(int) * (size_t)n);
+    s.mark = (unsigned *)take(sizeof(int) * (size_t)n);
+    s.qmark = (unsigned *)take(sizeof(int) * (size_t)n);
+    s.claim = (unsigned *)take(sizeof(int) * (size_t)n);
+    s.vlist = (int *)take(sizeof(int) * (size_t)n);
+    s.qa = (int *)take(sizeof(int) * (size_t)n);
+    s.qb = (int *)take(sizeof(int) * (size_t)n);
+    s.hot = (int *)take(sizeof(int) * 1024);
+    s.ract = (int *)take(sizeof(int) * 1024);
+    s.cnt = (int *)take(sizeof(int) * CNT_WORDS);
+    s.acc = (i64 *)take(sizeof(i64) * 128);
+    s.bar = (GroupBar *)take(sizeof(GroupBar));
+    s.clock = (unsigned *)take(sizeof(unsigned));
+    s.meta = (int *)take(sizeof(int) * 8);
+    s.hubw = (HubWork *)take(sizeof(HubWork) * (size_t)std::max(nhub, 1));
+    s.nhub = std::max(nhub, 1);
+    s.bits = (unsigned *)take(sizeof(unsigned) * 5 * (size_t)bitmap_words(n));
+    return s;
+}
+
 struct SlotPool {
     int n = 0;
     i64 arcs = 0;
@@ -115,32 +149,7 @@ struct SlotPool {
                 mf_dfree(base);
                 return fail(MF_ERR_CUDA, "residual slot clear failed: %s", cudaGetErrorString(e));
             }
-            char *p = (char *)base;
-            auto take = [&](size_t x) {
-                char *r = p;
-                p += (x + 255) & ~(size_t)255;
-                return (void *)r;
-            };
-            DSlot s;
-            s.res = (i64 *)take(sizeof(i64) * (size_t)std::max<i64>(arcs, 1));
-            s.ex = (i64 *)take(sizeof(i64) * (size_t)n);
-            s.h = (int *)take(sizeof(int) * (size_t)n);
-            s.mark = (unsigned *)take(sizeof(int) * (size_t)n);
-            s.qmark = (unsigned *)take(sizeof(int) * (size_t)n);
-            s.claim = (unsigned *)take(sizeof(int) * (size_t)n);
-            s.vlist = (int *)take(sizeof(int) * (size_t)n);
-            s.qa = (int *)take(sizeof(int) * (size_t)n);
-            s.qb = (int *)take(sizeof(int) * (size_t)n);
-            s.hot = (int *)take(sizeof(int) * 1024);
-            s.ract = (int *)take(sizeof(int) * 1024);
-            s.cnt = (int *)take(sizeof(int) * CNT_WORDS);
-            s.acc = (i64 *)take(sizeof(i64) * 128);
-            s.bar = (GroupBar *)take(sizeof(GroupBar));
-            s.clock = (unsigned *)take(sizeof(unsigned));
-            s.meta = (int *)take(sizeof(int) * 8);
-            s.hubw = (HubWork *)take(sizeof(HubWork) * (size_t)std::max(nhub, 1));
-            s.nhub = std::max(nhub, 1);
-            s.bits = (unsigned *)take(sizeof(unsigned) * 5 * (size_t)bitmap_words(n));
+            DSlot s = carve_slot((char *)base, n, arcs, nhub);
             bases.push_back(base);
             host.push_back(s);
         }
@@ -349,6 +358,7 @@ DGraph make_dgraph(const mf_graph *g) {
     dg.nhub = g->hubs ? g->nhub : 0;
     dg.giants = g->giants;
     dg.ngiant = g->giants ? g->ngiant : 0;
+    dg.fwd = g->fwd;
     if (g->kc_valid) {
         dg.kc_in = g->kc_in;
         dg.kc_fb = g->kc_fb;
@@ -822,6 +832,17 @@ cudaError_t mf_dmalloc_raw(void **p, size_t bytes) {
 cudaError_t mf_dfree(void *p) {
     alloc_untrack(p);
     return cudaFree(p);
+}
+cudaError_t mf_dmalloc_async_raw(void **p, size_t bytes, cudaStream_t st) {
+    *p = nullptr;
+    if (alloc_inject()) return cudaErrorMemoryAllocation;
+    cudaError_t e = cudaMallocAsync(p, bytes, st);
+    if (e == cudaSuccess) alloc_track(*p, bytes);
+    return e;
+}
+cudaError_t mf_dfree_async(void *p, cudaStream_t st) {
+    alloc_untrack(p);
+    return p ? cudaFreeAsync(p, st) : cudaSuccess;
 }
 cudaError_t mf_hmalloc_raw(void **p, size_t bytes) {
     *p = nullptr;
@@ -1778,77 +1799,69 @@ int mf_session_destroy(mf_session *ss) {
 }  // extern "C"
 
 // ---- continuous-batching server ---------------------------------------------
+//
+// One persistent cooperative launch of all the GPU's query groups serves a
+// ring of requests in mapped pinned host memory: (s,t) queries and
+// capacity-update batches on any of the server's graphs (device-resident
+// for the server's life).  Group i serves with slot i once the host has
+// admitted one; groups without a slot are parked.  A request is admitted to
+// the ring if its entry is free (the ticket `cap` earlier has finished), and
+// slots are admitted one request at a time: whenever more requests are open
+// than slots exist, another slot is allocated if free HBM allows
+// (cudaMemGetInfo, 85 % rule), stream-ordered on a side stream so the
+// running launch is not disturbed, and published to a parked group.
+
+namespace {
+constexpr int SRV_RING_DEFAULT = 1 << 16;       // ring entries
+constexpr long long SRV_UPD_DEFAULT = 1 << 20;  // update-arena entries
+constexpr int SRV_INITIAL_SLOTS = 4;
+}  // namespace
 
 struct mf_server {
     std::vector<mf_graph *> graphs;
     DGraph *d_graphs = nullptr;
-    SlotPool pool;
+    GState *d_gstate = nullptr;
+    GroupCtl *d_gctl = nullptr;
+    SrvCtl *d_srv = nullptr;
+    int *d_err = nullptr;
     mf_opts opts;
     KOpts ko;
-    int G = 2;
-    int nslots = 0;
+    int G = 8;
     int threads = 512;
-    int cap = 0;  // ring capacity (requests)
+    int ngroups = 0;    // groups of a launch (co-resident CTAs / G)
+    int max_slots = 0;  // admission cap (<= ngroups)
+    int nslots = 0;     // slots admitted; group i serves with slot i
+    int slot_n = 0, slot_nhub = 0;
+    i64 slot_arcs = 0;
+    size_t slot_size = 0;
+    std::vector<void *> slot_mem;
     // mapped pinned host memory
-    int *h_tail = nullptr, *h_stop = nullptr, *h_done = nullptr;
-    int4 *h_req = nullptr;
+    int cap = 0;
+    unsigned long long *h_tail = nullptr;
+    int *h_stop = nullptr;
+    int *h_done = nullptr;
+    RingReq *h_req = nullptr;
     u64 *h_t0 = nullptr;
     QOut *h_out = nullptr;
-    int *d_qnext = nullptr, *d_err = nullptr;
-    cudaStream_t stream = nullptr;
+    DSlot *h_slot_tab = nullptr;
+    int *h_slot_ready = nullptr;
+    UpdEntry *h_upd = nullptr;
+    long long upd_cap = 0;
+    // host bookkeeping
+    std::vector<long long> tk_of;  // ring entry -> ticket in it (-1: none yet)
+    long long submitted = 0;
+    long long first_open = 0;      // smallest ticket not known to be finished
+    // update arena: batches occupy [lo, hi) of a virtual offset space
+    // (physical offset = virtual % upd_cap, a batch never wraps)
+    long long upd_lo = 0, upd_hi = 0;
+    std::deque<std::pair<long long, long long>> upd_live;  // (ticket, virtual end), oldest first
+    std::vector<long long> nq_sub;   // per graph: queries submitted
+    std::vector<int> nupd_sub;       // per graph: update batches submitted
+    std::vector<char> updated;       // per graph: a batch was submitted
+    cudaStream_t stream = nullptr, side = nullptr;
     cudaEvent_t done_ev = nullptr;
     bool running = false;
-    long long submitted = 0;
 };
-
-static int server_launch(mf_server *sv) {
-    // resume after the last claimed request
-    long long first = 0;
-    while (first < sv->submitted && sv->h_done[first] != 0) ++first;
-    int q0 = (int)first;
-    CK(cudaMemcpyAsync(sv->d_qnext, &q0, sizeof(int), cudaMemcpyHostToDevice, sv->stream));
-    CK(cudaMemsetAsync(sv->d_err, 0, sizeof(int), sv->stream));
-    int ns = (int)sv->pool.host.size();
-    unsigned *clk = nullptr;
-    CK(mf_dmalloc(&clk, sizeof(unsigned) * ns));
-    k_prepare_slots<<<(ns + 127) / 128, 128, 0, sv->stream>>>(sv->pool.dev, ns, clk);
-    CK(cudaStreamSynchronize(sv->stream));
-    mf_dfree(clk);
-    *(volatile int *)sv->h_stop = 0;
-    KParams p{};
-    p.graphs = sv->d_graphs;
-    p.slots = sv->pool.dev;
-    p.G = sv->G;
-    p.nq = sv->cap;
-    p.q_next = sv->d_qnext;
-    int *dtail = nullptr, *dstop = nullptr, *ddone = nullptr;
-    int4 *dreq = nullptr;
-    u64 *dt0 = nullptr;
-    QOut *dout = nullptr;
-    CK(cudaHostGetDevicePointer((void **)&dtail, sv->h_tail, 0));
-    CK(cudaHostGetDevicePointer((void **)&dstop, sv->h_stop, 0));
-    CK(cudaHostGetDevicePointer((void **)&ddone, sv->h_done, 0));
-    CK(cudaHostGetDevicePointer((void **)&dreq, sv->h_req, 0));
-    CK(cudaHostGetDevicePointer((void **)&dt0, sv->h_t0, 0));
-    CK(cudaHostGetDevicePointer((void **)&dout, sv->h_out, 0));
-    p.out = dout;
-    p.err = sv->d_err;
-    p.bar_limit_ns = 20ull * 1000 * 1000 * 1000;
-    p.o = sv->ko;
-    p.mode = KM_SOLVE;
-    p.ring_tail = dtail;
-    p.ring_req = dreq;
-    p.ring_done = ddone;
-    p.ring_t0 = dt0;
-    p.ring_stop = dstop;
-    p.idle_limit_ns = 300ull * 1000 * 1000;  // groups idle this long end the launch
-    cudaError_t le = cudaSuccess;
-    mf_launch_kernel(p, sv->nslots * sv->G, sv->threads, sv->stream, sv->G > 1, &le);
-    if (le != cudaSuccess) return fail(MF_ERR_CUDA, "server launch: %s", cudaGetErrorString(le));
-    CK(cudaEventRecord(sv->done_ev, sv->stream));
-    sv->running = true;
-    return MF_OK;
-}
 
 static bool server_alive(mf_server *sv) {
     if (!sv->running) return false;
@@ -1856,6 +1869,119 @@ static bool server_alive(mf_server *sv) {
     if (q == cudaErrorNotReady) return true;
     sv->running = false;
     return false;
+}
+
+static int server_launch(mf_server *sv) {
+    if (sv->nslots < 1) return fail(MF_ERR_NOMEM, "server: no residual slot admitted");
+    CK(cudaMemsetAsync(sv->d_gctl, 0, sizeof(GroupCtl) * sv->ngroups, sv->stream));
+    CK(cudaMemsetAsync(&sv->d_srv->live, 0, sizeof(int), sv->stream));
+    CK(cudaMemsetAsync(sv->d_err, 0, sizeof(int), sv->stream));
+    *(volatile int *)sv->h_stop = 0;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    KParams p{};
+    p.graphs = sv->d_graphs;
+    p.G = sv->G;
+    p.nq = 0;
+    p.err = sv->d_err;
+    p.bar_limit_ns = 20ull * 1000 * 1000 * 1000;
+    p.o = sv->ko;
+    p.mode = KM_SOLVE;
+    CK(cudaHostGetDevicePointer((void **)&p.ring_tail, sv->h_tail, 0));
+    CK(cudaHostGetDevicePointer((void **)&p.ring_stop, sv->h_stop, 0));
+    CK(cudaHostGetDevicePointer((void **)&p.ring_done, sv->h_done, 0));
+    CK(cudaHostGetDevicePointer((void **)&p.ring_req, sv->h_req, 0));
+    CK(cudaHostGetDevicePointer((void **)&p.ring_t0, sv->h_t0, 0));
+    CK(cudaHostGetDevicePointer((void **)&p.out, sv->h_out, 0));
+    CK(cudaHostGetDevicePointer((void **)&p.slot_tab, sv->h_slot_tab, 0));
+    CK(cudaHostGetDevicePointer((void **)&p.slot_ready, sv->h_slot_ready, 0));
+    CK(cudaHostGetDevicePointer((void **)&p.srv_upd, sv->h_upd, 0));
+    p.ring_cap = sv->cap;
+    p.idle_limit_ns = 300ull * 1000 * 1000;  // groups idle this long end the launch
+    p.srv = sv->d_srv;
+    p.gstate = sv->d_gstate;
+    p.gctl = sv->d_gctl;
+    p.slot_n = sv->slot_n;
+    cudaError_t le = cudaSuccess;
+    mf_launch_kernel(p, sv->ngroups * sv->G, sv->threads, sv->stream, sv->G > 1, &le);
+    if (le != cudaSuccess) return fail(MF_ERR_CUDA, "server launch: %s", cudaGetErrorString(le));
+    CK(cudaEventRecord(sv->done_ev, sv->stream));
+    sv->running = true;
+    return MF_OK;
+}
+
+// Device status of the last launch once it has ended (0: none).
+static int server_error(mf_server *sv) {
+    int herr = 0;
+    if (cudaMemcpy(&herr, sv->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return MFD_TIMEOUT;
+    return herr;
+}
+
+// Launch the persistent kernel if it is not running (after reporting an
+// error of the last launch).
+static int server_ensure_running(mf_server *sv) {
+    if (server_alive(sv)) return MF_OK;
+    int herr = server_error(sv);
+    if (herr) return fail(status_from_err(herr), "server kernel aborted (status %d)", herr);
+    return server_launch(sv);
+}
+
+// Advance first_open over finished tickets; free the arena space of
+// finished update batches (oldest first).
+static void server_advance(mf_server *sv) {
+    while (sv->first_open < sv->submitted &&
+           *(volatile int *)&sv->h_done[sv->first_open % sv->cap] == 1)
+        ++sv->first_open;
+    while (!sv->upd_live.empty() && sv->upd_live.front().first < sv->first_open) {
+        sv->upd_lo = sv->upd_live.front().second;
+        sv->upd_live.pop_front();
+    }
+    if (sv->upd_live.empty()) sv->upd_lo = sv->upd_hi = 0;  // no batch in use: restart at 0
+}
+
+// Admission of residual slots by free HBM: while more requests are open
+// than slots exist, allocate another slot if it fits.
+static void server_admit_slots(mf_server *sv) {
+    server_advance(sv);
+    const long long open = sv->submitted - sv->first_open;
+    while (sv->nslots < sv->max_slots && open > sv->nslots) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess || (double)fr * 0.85 < (double)sv->slot_size) break;
+        void *m = nullptr;
+        if (mf_dmalloc_async_raw(&m, sv->slot_size, sv->side) != cudaSuccess ||
+            cudaStreamSynchronize(sv->side) != cudaSuccess) {
+            cudaGetLastError();
+            if (m) mf_dfree_async(m, sv->side);
+            break;
+        }
+        sv->slot_mem.push_back(m);
+        sv->h_slot_tab[sv->nslots] = carve_slot((char *)m, sv->slot_n, sv->slot_arcs, sv->slot_nhub);
+        std::atomic_thread_fence(std::memory_order_seq_cst);
+        *(volatile int *)&sv->h_slot_ready[sv->nslots] = 1;  // the group clears it before use
+        ++sv->nslots;
+    }
+}
+
+// Reserve the ring entry of the next ticket (its previous ticket finished).
+static int server_reserve(mf_server *sv, int &e) {
+    server_advance(sv);
+    const long long k = sv->submitted;
+    e = (int)(k % sv->cap);
+    if (k - sv->first_open >= sv->cap)
+        return fail(MF_ERR_NOMEM, "server ring full: %d requests open (ticket %lld not finished)", sv->cap,
+                    sv->first_open);
+    return MF_OK;
+}
+
+static int server_publish(mf_server *sv, int e, long long *ticket) {
+    const long long k = sv->submitted;
+    sv->tk_of[e] = k;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    sv->submitted = k + 1;
+    *(volatile unsigned long long *)sv->h_tail = (unsigned long long)sv->submitted;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    if (ticket) *ticket = k;
+    server_admit_slots(sv);
+    return server_ensure_running(sv);
 }
 
 extern "C" {
@@ -1867,8 +1993,7 @@ int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int ma
     mf_server *sv = new mf_server();
     if (opts) sv->opts = *opts;
     else mf_opts_default(&sv->opts);
-    int nmax = 0, hmax = 0;
-    i64 amax = 0, arcs_sum = 0, n_sum = 0;
+    i64 arcs_sum = 0, n_sum = 0;
     std::vector<DGraph> dg(ngraphs);
     for (int i = 0; i < ngraphs; ++i) {
         mf_graph *g = graphs[i];
@@ -1877,9 +2002,9 @@ int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int ma
             return fail(MF_ERR_ARG, "graph %d is NULL", i);
         }
         sv->graphs.push_back(g);
-        nmax = std::max(nmax, g->n);
-        amax = std::max(amax, g->arcs);
-        hmax = std::max(hmax, g->nhub);
+        sv->slot_n = std::max(sv->slot_n, g->n);
+        sv->slot_arcs = std::max(sv->slot_arcs, g->arcs);
+        sv->slot_nhub = std::max(sv->slot_nhub, g->nhub);
         arcs_sum += g->arcs;
         n_sum += g->n;
         int rc0 = ensure_kept_cache(g, sv->opts);
@@ -1898,50 +2023,57 @@ int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int ma
         return rc;
     }
     sv->G = sv->opts.group_ctas > 0 ? sv->opts.group_ctas : 8;
-    int groups = std::max(1, di.sms * di.bps / sv->G);
-    size_t fr = 0, tot = 0;
-    cudaMemGetInfo(&fr, &tot);
-    size_t per = slot_bytes(nmax, amax, hmax);
-    int fit = (int)((fr * 0.85) / (double)per);
-    int ns = std::min(groups, fit);
-    if (max_slots > 0) ns = std::min(ns, max_slots);
-    if (ns < 1) {
-        delete sv;
-        return fail(MF_ERR_NOMEM, "admission: no HBM for one residual slot (%zu bytes)", per);
-    }
-    sv->nslots = ns;
-    sv->pool.n = nmax;
-    sv->pool.arcs = amax;
-    sv->pool.nhub = hmax;
-    rc = sv->pool.grow(ns);
-    if (rc) {
-        sv->pool.release();
-        delete sv;
-        return rc;
-    }
+    sv->ngroups = std::max(1, di.sms * di.bps / sv->G);
+    sv->max_slots = max_slots > 0 ? std::min(max_slots, sv->ngroups) : sv->ngroups;
+    sv->slot_size = slot_bytes(sv->slot_n, sv->slot_arcs, sv->slot_nhub);
+    sv->cap = SRV_RING_DEFAULT;
+    if (const char *e = getenv("MF_SERVER_RING")) sv->cap = std::max(16, atoi(e));
+    sv->upd_cap = SRV_UPD_DEFAULT;
+    if (const char *e = getenv("MF_SERVER_UPDATE_ARENA")) sv->upd_cap = std::max(1024LL, atoll(e));
+    sv->tk_of.assign(sv->cap, -1);
+    sv->nq_sub.assign(ngraphs, 0);
+    sv->nupd_sub.assign(ngraphs, 0);
+    sv->updated.assign(ngraphs, 0);
+    auto bail = [&](int code, const char *what) {
+        mf_server_destroy(sv);
+        return fail(code, "server creation: %s", what);
+    };
     if (mf_dmalloc(&sv->d_graphs, sizeof(DGraph) * ngraphs) != cudaSuccess ||
-        cudaMemcpy(sv->d_graphs, dg.data(), sizeof(DGraph) * ngraphs, cudaMemcpyHostToDevice) != cudaSuccess) {
-        sv->pool.release();
-        delete sv;
-        return fail(MF_ERR_NOMEM, "server graph table");
-    }
-    sv->cap = 1 << 20;
-    bool ok = mf_hostalloc(&sv->h_tail, sizeof(int) * 2, cudaHostAllocMapped) == cudaSuccess &&
+        mf_dmalloc(&sv->d_gstate, sizeof(GState) * ngraphs) != cudaSuccess ||
+        mf_dmalloc(&sv->d_gctl, sizeof(GroupCtl) * sv->ngroups) != cudaSuccess ||
+        mf_dmalloc(&sv->d_srv, sizeof(SrvCtl)) != cudaSuccess || mf_dmalloc(&sv->d_err, sizeof(int)) != cudaSuccess)
+        return bail(MF_ERR_NOMEM, "device tables");
+    bool ok = mf_hostalloc(&sv->h_tail, sizeof(unsigned long long) * 2, cudaHostAllocMapped) == cudaSuccess &&
               mf_hostalloc(&sv->h_done, sizeof(int) * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
-              mf_hostalloc(&sv->h_req, sizeof(int4) * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
+              mf_hostalloc(&sv->h_req, sizeof(RingReq) * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
               mf_hostalloc(&sv->h_t0, sizeof(u64) * 2 * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
               mf_hostalloc(&sv->h_out, sizeof(QOut) * sv->cap, cudaHostAllocMapped) == cudaSuccess &&
-              mf_dmalloc(&sv->d_qnext, sizeof(int) * 2) == cudaSuccess;
-    if (!ok) {
-        mf_server_destroy(sv);
-        return fail(MF_ERR_NOMEM, "server ring allocation failed");
-    }
-    sv->h_stop = sv->h_tail + 1;
-    sv->d_err = sv->d_qnext + 1;
-    memset(sv->h_tail, 0, sizeof(int) * 2);
+              mf_hostalloc(&sv->h_slot_tab, sizeof(DSlot) * sv->ngroups, cudaHostAllocMapped) == cudaSuccess &&
+              mf_hostalloc(&sv->h_slot_ready, sizeof(int) * sv->ngroups, cudaHostAllocMapped) == cudaSuccess &&
+              mf_hostalloc(&sv->h_upd, sizeof(UpdEntry) * sv->upd_cap, cudaHostAllocMapped) == cudaSuccess;
+    if (!ok) return bail(MF_ERR_NOMEM, "mapped ring allocation failed");
+    sv->h_stop = reinterpret_cast<int *>(sv->h_tail + 1);
+    memset(sv->h_tail, 0, sizeof(unsigned long long) * 2);
     memset(sv->h_done, 0, sizeof(int) * sv->cap);
-    cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);
-    cudaEventCreateWithFlags(&sv->done_ev, cudaEventDisableTiming);
+    memset(sv->h_slot_ready, 0, sizeof(int) * sv->ngroups);
+    if (cudaMemcpy(sv->d_graphs, dg.data(), sizeof(DGraph) * ngraphs, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(sv->d_gstate, 0, sizeof(GState) * ngraphs) != cudaSuccess ||
+        cudaMemset(sv->d_srv, 0, sizeof(SrvCtl)) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&sv->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sv->done_ev, cudaEventDisableTiming) != cudaSuccess)
+        return bail(MF_ERR_CUDA, "device set-up failed");
+    // the first slots (more are admitted as requests open up)
+    const long long want = std::min(SRV_INITIAL_SLOTS, sv->max_slots);
+    sv->submitted = want;  // admit as if `want` requests were open
+    sv->first_open = 0;
+    server_admit_slots(sv);
+    sv->submitted = 0;
+    sv->first_open = 0;
+    if (sv->nslots < 1) {
+        mf_server_destroy(sv);
+        return fail(MF_ERR_NOMEM, "admission: no HBM for one residual slot (%zu bytes)", sv->slot_size);
+    }
     *out = sv;
     return MF_OK;
 }
@@ -1955,64 +2087,125 @@ int mf_server_slots(const mf_server *sv, int *slots) {
 int mf_server_submit(mf_server *sv, int graph, int32_t s, int32_t t, long long *ticket) {
     if (!sv) return fail(MF_ERR_ARG, "server is NULL");
     if (graph < 0 || graph >= (int)sv->graphs.size()) return fail(MF_ERR_ARG, "graph index %d", graph);
-    if (sv->submitted >= sv->cap) return fail(MF_ERR_NOMEM, "server ring full (%d requests)", sv->cap);
+    int e = 0;
+    int rc = server_reserve(sv, e);
+    if (rc) return rc;
     mf_graph *g = sv->graphs[graph];
     int si = -1, ti = -1;
     to_internal(g, s, t, si, ti);
-    long long k = sv->submitted;
-    sv->h_req[k] = make_int4(si, ti, graph, 0);
-    sv->h_done[k] = 0;
-    std::atomic_thread_fence(std::memory_order_seq_cst);
-    sv->submitted = k + 1;
-    *(volatile int *)sv->h_tail = (int)sv->submitted;
-    std::atomic_thread_fence(std::memory_order_seq_cst);
-    if (ticket) *ticket = k;
-    if (!server_alive(sv)) {
-        int rc = server_launch(sv);
-        if (rc) return rc;
+    RingReq r{};
+    r.kind = RQ_QUERY;
+    r.graph = graph;
+    r.s = si;
+    r.t = ti;
+    r.epoch = sv->nupd_sub[graph];
+    sv->h_req[e] = r;
+    sv->h_done[e] = 0;
+    sv->nq_sub[graph]++;
+    return server_publish(sv, e, ticket);
+}
+
+int mf_server_update(mf_server *sv, int graph, int nb, const int32_t *u, const int32_t *v,
+                     const int64_t *delta, long long *ticket) {
+    if (!sv) return fail(MF_ERR_ARG, "server is NULL");
+    if (graph < 0 || graph >= (int)sv->graphs.size()) return fail(MF_ERR_ARG, "graph index %d", graph);
+    if (nb < 0 || (nb > 0 && (!u || !v || !delta))) return fail(MF_ERR_ARG, "bad update arrays");
+    mf_graph *g = sv->graphs[graph];
+    // fold the changes of each (u, v) pair, in order, into cap -> max(a, cap + b)
+    std::map<std::pair<int, int>, std::pair<i64, i64>> fold;
+    std::vector<std::pair<int, int>> order;
+    for (int i = 0; i < nb; ++i) {
+        if (u[i] < 0 || u[i] >= g->n || v[i] < 0 || v[i] >= g->n || u[i] == v[i]) continue;
+        const std::pair<int, int> key(g->new_id[u[i]], g->new_id[v[i]]);
+        auto it = fold.find(key);
+        if (it == fold.end()) {
+            fold[key] = std::make_pair((i64)0, (i64)delta[i]);
+            order.push_back(key);
+        } else {
+            const i64 a = it->second.first, b = it->second.second;
+            it->second = std::make_pair(std::max<i64>(0, a + delta[i]), b + delta[i]);
+        }
     }
-    return MF_OK;
+    const long long n = (long long)order.size();
+    if (n > sv->upd_cap)
+        return fail(MF_ERR_ARG, "update batch of %lld arcs exceeds the server's update arena (%lld)", n,
+                    sv->upd_cap);
+    int e = 0;
+    int rc = server_reserve(sv, e);
+    if (rc) return rc;
+    // arena space: a batch is contiguous; wait (bounded) for older batches
+    long long off = 0;
+    for (auto t0 = std::chrono::steady_clock::now();;) {
+        server_advance(sv);
+        off = sv->upd_hi;
+        if (off % sv->upd_cap + n > sv->upd_cap) off += sv->upd_cap - off % sv->upd_cap;
+        if (off + n - sv->upd_lo <= sv->upd_cap) break;
+        rc = server_ensure_running(sv);
+        if (rc) return rc;
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+        if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(60))
+            return fail(MF_ERR_TIMEOUT, "server update arena stayed full for 60 s");
+    }
+    const long long phys = off % sv->upd_cap;
+    for (long long i = 0; i < n; ++i) {
+        const auto &kv = *fold.find(order[i]);
+        UpdEntry x;
+        x.u = kv.first.first;
+        x.v = kv.first.second;
+        x.a = kv.second.first;
+        x.b = kv.second.second;
+        sv->h_upd[phys + i] = x;
+    }
+    sv->upd_hi = off + n;
+    sv->upd_live.push_back(std::make_pair(sv->submitted, sv->upd_hi));
+    RingReq r{};
+    r.kind = RQ_UPDATE;
+    r.graph = graph;
+    r.s = r.t = -1;
+    r.epoch = sv->nupd_sub[graph];
+    r.upd_n = (int)n;
+    r.upd_off = phys;
+    r.need_done = (unsigned long long)sv->nq_sub[graph];
+    sv->h_req[e] = r;
+    sv->h_done[e] = 0;
+    sv->nupd_sub[graph]++;
+    sv->updated[graph] = 1;
+    return server_publish(sv, e, ticket);
 }
 
 int mf_server_poll(mf_server *sv, long long ticket, int *done, int64_t *flow, double *latency_ms,
                    int *status) {
     if (!sv || ticket < 0 || ticket >= sv->submitted) return fail(MF_ERR_ARG, "bad ticket");
-    int d = *(volatile int *)&sv->h_done[ticket];
+    const int e = (int)(ticket % sv->cap);
+    if (sv->tk_of[e] != ticket) return fail(MF_ERR_ARG, "ticket %lld expired (its ring entry was reused)", ticket);
+    int d = *(volatile int *)&sv->h_done[e];
     if (d != 1) {
-        if (!server_alive(sv)) {
-            int herr = 0;
-            cudaMemcpy(&herr, sv->d_err, sizeof(int), cudaMemcpyDeviceToHost);
-            if (herr) return fail(status_from_err(herr), "server kernel aborted (status %d)", herr);
-            int rc = server_launch(sv);
-            if (rc) return rc;
-        }
+        int rc = server_ensure_running(sv);
+        if (rc) return rc;
         if (done) *done = 0;
         return MF_OK;
     }
     std::atomic_thread_fence(std::memory_order_seq_cst);
-    const QOut &q = sv->h_out[ticket];
+    const QOut &q = sv->h_out[e];
     if (done) *done = 1;
     if (flow) *flow = q.flow;
     if (status) *status = status_from_err(q.status);
     if (latency_ms) {
         volatile u64 *t0 = sv->h_t0;
-        *latency_ms = (double)(t0[2 * ticket + 1] - t0[2 * ticket]) * 1e-6;
+        *latency_ms = (double)(t0[2 * e + 1] - t0[2 * e]) * 1e-6;
     }
     return MF_OK;
 }
 
 int mf_server_drain(mf_server *sv) {
     if (!sv) return fail(MF_ERR_ARG, "server is NULL");
-    for (long long k = 0; k < sv->submitted; ++k) {
-        for (;;) {
-            int done = 0;
-            int rc = mf_server_poll(sv, k, &done, nullptr, nullptr, nullptr);
-            if (rc) return rc;
-            if (done) break;
-            std::this_thread::sleep_for(std::chrono::microseconds(20));
-        }
+    for (;;) {
+        server_advance(sv);
+        if (sv->first_open >= sv->submitted) return MF_OK;
+        int rc = server_ensure_running(sv);
+        if (rc) return rc;
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
-    return MF_OK;
 }
 
 int mf_server_destroy(mf_server *sv) {
@@ -2020,16 +2213,33 @@ int mf_server_destroy(mf_server *sv) {
     if (sv->h_stop) *(volatile int *)sv->h_stop = 1;
     std::atomic_thread_fence(std::memory_order_seq_cst);
     if (sv->stream) cudaStreamSynchronize(sv->stream);
-    sv->pool.release();
+    // capacities changed under the graphs' kept-set caches: drop them (the
+    // next solve on the graph rebuilds its cache)
+    for (size_t i = 0; i < sv->graphs.size() && i < sv->updated.size(); ++i) {
+        if (!sv->updated[i]) continue;
+        mf_graph *g = sv->graphs[i];
+        free_kept_cache(g);
+        g->kc_tried = false;
+        upload_dgraph(g);
+    }
+    for (void *m : sv->slot_mem) mf_dfree_async(m, sv->side ? sv->side : sv->stream);
+    if (sv->side) cudaStreamSynchronize(sv->side);
     mf_dfree(sv->d_graphs);
-    mf_dfree(sv->d_qnext);
+    mf_dfree(sv->d_gstate);
+    mf_dfree(sv->d_gctl);
+    mf_dfree(sv->d_srv);
+    mf_dfree(sv->d_err);
     mf_hfree(sv->h_tail);
     mf_hfree(sv->h_done);
     mf_hfree(sv->h_req);
     mf_hfree(sv->h_t0);
     mf_hfree(sv->h_out);
+    mf_hfree(sv->h_slot_tab);
+    mf_hfree(sv->h_slot_ready);
+    mf_hfree(sv->h_upd);
     if (sv->done_ev) cudaEventDestroy(sv->done_ev);
     if (sv->stream) cudaStreamDestroy(sv->stream);
+    if (sv->side) cudaStreamDestroy(sv->side);
     delete sv;
     return MF_OK;
 }

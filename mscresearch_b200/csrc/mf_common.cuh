@@ -28,6 +28,9 @@ __device__ __forceinline__ unsigned char ldro_u8(const unsigned char *p) { retur
 __device__ __forceinline__ int ldcg(const int *p) { return __ldcg(p); }
 __device__ __forceinline__ unsigned ldcg(const unsigned *p) { return __ldcg(p); }
 __device__ __forceinline__ i64 ldcg(const i64 *p) { return __ldcg(p); }
+// Capacities: read through L2 (coherent), since a serving launch applies
+// capacity updates to the graph it reads while it runs.
+__device__ __forceinline__ i64 ldcap(const i64 *p) { return __ldcg(p); }
 
 // ---------------------------------------------------------------------------
 // Self-check builds (-DMF_CHECKS, libmfb200_chk.so): every warp records the

@@ -126,6 +126,7 @@ struct QCtx {
     // per-warp counters (flushed at the end of the query)
     i64 w_arcs, w_verts, w_push;
     int bu_factor;  // direction switch of the searches (KOpts::bu_factor)
+    bool no_cache;  // the graph's kept-set cache is stale (a served capacity update)
 
     __device__ bool sync() { return gsync(G, bar, err, lim); }
     // a vertex with arcs [b, e1) that for_giants covers
@@ -579,7 +580,7 @@ __device__ bool reach_all(QCtx &c, int x, int dir, unsigned *st, unsigned S, int
     const i64 *cap = c.cap;
     const int *rev = c.rev;
     auto td = [&](int v, int e, int w, int) -> bool {
-        i64 ce = ldro(&cap[dir ? ldro(&rev[e]) : e]);
+        i64 ce = ldcap(&cap[dir ? ldro(&rev[e]) : e]);
         unsigned mw = ldcg(&st[w]);
         if (ce <= 0 || mw >= S) return false;
         return atomicMax(&st[w], S) < S;
@@ -592,7 +593,7 @@ __device__ bool reach_all(QCtx &c, int x, int dir, unsigned *st, unsigned S, int
         return ldcg(&st[w]) < S ? w : -1;
     };
     auto par = [&](int w, int e, int y, int) -> bool {
-        return ldcg(&st[y]) >= S && ldro(&cap[dir ? e : ldro(&rev[e])]) > 0;
+        return ldcg(&st[y]) >= S && ldcap(&cap[dir ? e : ldro(&rev[e])]) > 0;
     };
     auto set = [&](int w, int) -> bool {
         st[w] = S;
@@ -617,7 +618,7 @@ __device__ bool reach_within(QCtx &c, int x, int dir, unsigned S, unsigned M, co
     const int *rev = c.rev;
     auto td = [&](int v, int e, int w, int) -> bool {
         unsigned mw = ldcg(&mark[w]);
-        i64 ce = ldro(&cap[dir ? ldro(&rev[e]) : e]);
+        i64 ce = ldcap(&cap[dir ? ldro(&rev[e]) : e]);
         if (mw != S || ce <= 0) return false;
         return atomicCAS(&mark[w], S, M) == S;
     };
@@ -630,7 +631,7 @@ __device__ bool reach_within(QCtx &c, int x, int dir, unsigned S, unsigned M, co
         return ldcg(&mark[w]) == S ? w : -1;
     };
     auto par = [&](int w, int e, int y, int) -> bool {
-        return ldcg(&mark[y]) == M && ldro(&cap[dir ? e : ldro(&rev[e])]) > 0;
+        return ldcg(&mark[y]) == M && ldcap(&cap[dir ? e : ldro(&rev[e])]) > 0;
     };
     auto set = [&](int w, int) -> bool {
         mark[w] = M;
@@ -760,7 +761,7 @@ __device__ bool prune_ext(QCtx &c, int s, int t, unsigned S, unsigned M, int &nv
     int f0 = 0, b0 = 0;
     if (!c.sync_tails(xb, f0, b0)) return false;
     auto xs = [&](int v, int e, int w, int) -> bool {
-        i64 ce = ldro(&cap[e]);
+        i64 ce = ldcap(&cap[e]);
         unsigned mw = ldcg(&mark[w]);
         if (ce <= 0 || mw >= S || (ldro_u8(&fb[w]) & KC_F)) return false;
         return atomicMax(&mark[w], S) < S;
@@ -772,7 +773,7 @@ __device__ bool prune_ext(QCtx &c, int s, int t, unsigned S, unsigned M, int &nv
     int yf0 = 0, yb0 = 0;
     if (!c.sync_tails(yb, yf0, yb0)) return false;
     auto ys = [&](int v, int e, int w, int) -> bool {
-        i64 cr = ldro(&cap[ldro(&rev[e])]);
+        i64 cr = ldcap(&cap[ldro(&rev[e])]);
         unsigned qw = ldcg(&qm[w]);
         if (cr <= 0 || qw >= S || (ldro_u8(&fb[w]) & KC_B)) return false;
         return atomicMax(&qm[w], S) < S;
@@ -838,10 +839,10 @@ __device__ bool fix_extra_arcs(QCtx &c, unsigned M, int nv) {
         for (int e = b + c.lane; e < e1; e += 32) {
             int w = ldro(&c.col[e]);
             bool kw = ldcg(&c.st.mark[w]) >= M;
-            c.st.res[e] = kw ? ldro(&c.cap[e]) : 0;
+            c.st.res[e] = kw ? ldcap(&c.cap[e]) : 0;
             if (kw) {
                 int r = ldro(&c.rev[e]);
-                c.st.res[r] = ldro(&c.cap[r]);
+                c.st.res[r] = ldcap(&c.cap[r]);
             }
         }
     }
@@ -851,10 +852,10 @@ __device__ bool fix_extra_arcs(QCtx &c, unsigned M, int nv) {
         [&](int, int e) {
             int w = ldro(&c.col[e]);
             bool kw = ldcg(&c.st.mark[w]) >= M;
-            c.st.res[e] = kw ? ldro(&c.cap[e]) : 0;
+            c.st.res[e] = kw ? ldcap(&c.cap[e]) : 0;
             if (kw) {
                 int r = ldro(&c.rev[e]);
-                c.st.res[r] = ldro(&c.cap[r]);
+                c.st.res[r] = ldcap(&c.cap[r]);
             }
         });
     return c.sync();
@@ -910,7 +911,7 @@ __device__ bool init_state(QCtx &c, int nv, unsigned M, bool count_mask = true) 
         i64 swept = 0;
         for (i64 k = gt; k < nq4; k += gT) {
             const int4 w = __ldg(&col4[k]);
-            const longlong2 ca = __ldg(&cap2[2 * k]), cb = __ldg(&cap2[2 * k + 1]);
+            const longlong2 ca = __ldcg(&cap2[2 * k]), cb = __ldcg(&cap2[2 * k + 1]);
             longlong2 ra, rb;
             ra.x = ldcg(&mark[w.x]) >= M ? ca.x : 0;
             ra.y = ldcg(&mark[w.y]) >= M ? ca.y : 0;
@@ -921,7 +922,7 @@ __device__ bool init_state(QCtx &c, int nv, unsigned M, bool count_mask = true) 
             swept += 4;
         }
         for (i64 e = 4 * nq4 + gt; e < A; e += gT) {
-            c.st.res[e] = ldcg(&mark[ldro(&c.col[e])]) >= M ? ldro(&c.cap[e]) : 0;
+            c.st.res[e] = ldcg(&mark[ldro(&c.col[e])]) >= M ? ldcap(&c.cap[e]) : 0;
             ++swept;
         }
         c.w_arcs += swept;
@@ -944,13 +945,13 @@ __device__ bool init_state(QCtx &c, int nv, unsigned M, bool count_mask = true) 
         if (c.giant(b, e1)) continue;
         for (int e = b + c.lane; e < e1; e += 32) {
             int w = ldro(&c.col[e]);
-            c.st.res[e] = (ldcg(&c.st.mark[w]) >= M) ? ldro(&c.cap[e]) : 0;
+            c.st.res[e] = (ldcg(&c.st.mark[w]) >= M) ? ldcap(&c.cap[e]) : 0;
         }
     }
     if (count_mask && c.lane == 0 && mask_arcs) atomic_add_i64(&c.st.acc[ACC_TOT + T_MASKARCS], mask_arcs);
     for_giants(
         c, [&](int v) { return ldcg(&c.st.mark[v]) >= M; }, [&](int, int, int) {},
-        [&](int, int e) { c.st.res[e] = (ldcg(&c.st.mark[ldro(&c.col[e])]) >= M) ? ldro(&c.cap[e]) : 0; });
+        [&](int, int e) { c.st.res[e] = (ldcg(&c.st.mark[ldro(&c.col[e])]) >= M) ? ldcap(&c.cap[e]) : 0; });
     return c.sync();
 }
 
@@ -1965,7 +1966,7 @@ __device__ bool certify(QCtx &c, int s, int t, int nv, unsigned M, i64 flow, QOu
         int nb = r < 0;
         if (ldcg(&c.st.mark[w]) >= M) {
             int re = ldro(&c.rev[e]);
-            if (r + ldcg(&c.st.res[re]) != ldro(&c.cap[e]) + ldro(&c.cap[re])) ++nb;
+            if (r + ldcg(&c.st.res[re]) != ldcap(&c.cap[e]) + ldcap(&c.cap[re])) ++nb;
         }
         return nb;
     };
@@ -1998,7 +1999,7 @@ __device__ bool certify(QCtx &c, int s, int t, int nv, unsigned M, i64 flow, QOu
         if (ldcg(&qm[w]) == Z) return false;
         int re = ldro(&rev[e]);  // arc w->v
         bool kept = ldcg(&mark[w]) >= M && ldcg(&mark[v]) >= M;
-        i64 r = kept ? ldcg(&res[re]) : ldro(&cap[re]);
+        i64 r = kept ? ldcg(&res[re]) : ldcap(&cap[re]);
         if (r <= 0) return false;
         return atomicMax(&qm[w], Z) < Z;
     };
@@ -2006,7 +2007,7 @@ __device__ bool certify(QCtx &c, int s, int t, int nv, unsigned M, i64 flow, QOu
     // cut capacity over all vertices
     i64 cut = 0;
     auto cut_arc = [&](int e) -> i64 {
-        i64 cp = ldro(&cap[e]);
+        i64 cp = ldcap(&cap[e]);
         return (cp > 0 && ldcg(&qm[ldro(&c.col[e])]) == Z) ? cp : 0;
     };
     for (int v = c.gw; v < c.n; v += c.gW) {
@@ -2037,14 +2038,14 @@ __device__ bool write_full_residual(QCtx &c, unsigned M, i64 *out) {
         for (int e = b + c.lane; e < e1; e += 32) {
             int w = ldro(&c.col[e]);
             bool kept = kv && ldcg(&c.st.mark[w]) >= M;
-            out[e] = kept ? ldcg(&c.st.res[e]) : ldro(&c.cap[e]);
+            out[e] = kept ? ldcg(&c.st.res[e]) : ldcap(&c.cap[e]);
         }
     }
     for_giants(
         c, [&](int) { return true; }, [&](int, int, int) {},
         [&](int v, int e) {
             bool kept = ldcg(&c.st.mark[v]) >= M && ldcg(&c.st.mark[ldro(&c.col[e])]) >= M;
-            out[e] = kept ? ldcg(&c.st.res[e]) : ldro(&c.cap[e]);
+            out[e] = kept ? ldcg(&c.st.res[e]) : ldcap(&c.cap[e]);
         });
     return c.sync();
 }
@@ -2091,7 +2092,7 @@ __device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int
         if (!c.sync_tails(nb, f0, b0)) return false;
         auto bwd = [&](int v, int e, int w, int) -> bool {
             if (ldcg(&mark[w]) != S) return false;
-            if (ldro(&cap[ldro(&rev[e])]) <= 0) return false;
+            if (ldcap(&cap[ldro(&rev[e])]) <= 0) return false;
             return atomicCAS(&mark[w], S, Mn) == S;
         };
         // bottom-up candidates: the forward-reached vertices not reached yet
@@ -2104,7 +2105,7 @@ __device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int
             return ldcg(&mark[w]) == S ? w : -1;
         };
         auto par = [&](int w, int e, int y, int) -> bool {
-            return ldcg(&mark[y]) == Mn && ldro(&cap[e]) > 0;  // arc w -> y, y reaches t
+            return ldcg(&mark[y]) == Mn && ldcap(&cap[e]) > 0;  // arc w -> y, y reaches t
         };
         auto set = [&](int w, int) -> bool {
             mark[w] = Mn;
@@ -2142,10 +2143,10 @@ __device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int
     auto open_arc = [&](int e) {
         int w = ldro(&c.col[e]);
         if (ldcg(&mark[w]) == Mn) {
-            c.st.res[e] = ldro(&cap[e]);
+            c.st.res[e] = ldcap(&cap[e]);
             if (ldcg(&claim[w]) == O) {
                 int re = ldro(&rev[e]);
-                c.st.res[re] = ldro(&cap[re]);
+                c.st.res[re] = ldcap(&cap[re]);
             }
         } else {
             c.st.res[e] = 0;
@@ -2232,7 +2233,7 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
         M = ++c.clock;
         const DGraph &g = *c.gr;
         // kc_case 1: s and t in the cached component; 2: s in B, t in F
-        const bool use_kc = p.mode != KM_KEPTSET && o.prune_mode == 1 && o.use_cache && g.kc_in;
+        const bool use_kc = p.mode != KM_KEPTSET && o.prune_mode == 1 && o.use_cache && g.kc_in && !c.no_cache;
         int kc_case = 0;
         if (use_kc) {
             if (ldro_u8(&g.kc_in[s]) && ldro_u8(&g.kc_in[t])) kc_case = 1;
@@ -2357,7 +2358,7 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
         } else {
             i64 *out = (i64 *)p.dbg;
             int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
-            for (i64 e = gt; e < (i64)ldro(&c.row[c.n]); e += gT) out[e] = ldro(&c.cap[e]);
+            for (i64 e = gt; e < (i64)ldro(&c.row[c.n]); e += gT) out[e] = ldcap(&c.cap[e]);
             if (!c.sync()) return;
         }
     }
@@ -2395,6 +2396,284 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
     c.sync();
 }
 
+// Points the context at graph gi (its CSR, giants, kept-set cache).
+__device__ __forceinline__ void bind_graph(QCtx &c, const KParams &p, int gi) {
+    const DGraph &g = p.graphs[gi];
+    c.n = g.n;
+    c.R = g.R;
+    c.row = g.row;
+    c.col = g.col;
+    c.rev = g.rev;
+    c.rof = g.region_of;
+    c.cap = g.cap;
+    c.gr = &p.graphs[gi];
+    c.giants = g.giants;
+    c.ngiant = g.giants ? g.ngiant : 0;
+}
+
+// ---------------------------------------------------------------------------
+// Serving loop (KParams::ring_tail != NULL).  Each group owns the slot the
+// host published for it in slot_tab (a group still without one is parked
+// until the host admits another slot, or until no group is serving), then
+// claims requests in ticket order from a shared 64-bit counter.
+//
+// Ordering.  A query on graph g waits until the update batches submitted
+// before it on g are applied (GState::epoch); an update batch waits until
+// every query submitted before it on g has finished (GState::done_q) and the
+// batches before it are applied.  Every wait is for a smaller ticket, and
+// tickets are claimed in order, so the smallest unfinished ticket never
+// waits: no wait can close a cycle.  Every wait is also bounded in time.
+//
+// A group that leaves while holding a claimed ticket not yet submitted gives
+// it back (compare-and-swap of the counter from k+1 to k, possible once the
+// groups that claimed after it have given theirs back), so a relaunch
+// resumes at the first unclaimed ticket and no ticket is lost or run twice.
+
+// Zero everything in the slot but the residuals (stamps, clock, lists,
+// control words, bitmaps): a new slot's memory is uninitialized, and a slot
+// whose stamp clock nears 2^31 is reset the same way.
+__device__ bool srv_clear_slot(QCtx &c, const DSlot &sl, int n) {
+    char *b = reinterpret_cast<char *>(sl.ex);
+    char *e = reinterpret_cast<char *>(sl.bits + 5 * (size_t)bitmap_words(n));
+    // the slot layout aligns every array to 256 bytes, so rounding the end up
+    // to 16 bytes stays inside the slot
+    const size_t words = ((size_t)(e - b) + 15) >> 4;
+    int4 *w = reinterpret_cast<int4 *>(b);
+    const int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+    for (size_t k = gt; k < words; k += gT) w[k] = make_int4(0, 0, 0, 0);
+    __threadfence();
+    return c.sync();
+}
+
+// Leader: wait until *word >= want (a bounded wait; false on timeout or a
+// raised error word).
+__device__ bool srv_wait_ge(const KParams &p, const int *word, int want) {
+    const u64 t0 = globaltimer_ns();
+    unsigned spins = 0;
+    while (*(volatile const int *)word < want) {
+        if (*(volatile int *)p.err) return false;
+        __nanosleep(1000);
+        if ((++spins & 63u) == 0 && globaltimer_ns() - t0 > p.bar_limit_ns) {
+            atomicCAS(p.err, 0, MFD_TIMEOUT);
+            return false;
+        }
+    }
+    __threadfence();
+    return true;
+}
+
+// One capacity-update batch, a warp per entry: resolve u -> v to its first
+// forward arc (the shorter of the two arc lists is scanned, as in the
+// host-side resolution), then cap = max(a, cap + b).  Entries name distinct
+// (u, v) pairs, so no two warps write one arc.
+__device__ bool srv_apply_updates(QCtx &c, const KParams &p, int gi, long long off, int nu) {
+    const DGraph &g = p.graphs[gi];
+    i64 *cap = const_cast<i64 *>(g.cap);
+    for (int i = c.gw; i < nu; i += c.gW) {
+        const UpdEntry *up = p.srv_upd + off + i;
+        const int x = *(volatile const int *)&up->u, y = *(volatile const int *)&up->v;
+        const i64 ua = *(volatile const i64 *)&up->a, ub = *(volatile const i64 *)&up->b;
+        if (x < 0 || y < 0 || x >= g.n || y >= g.n) continue;
+        const bool by_head = ldro(&g.row[y + 1]) - ldro(&g.row[y]) < ldro(&g.row[x + 1]) - ldro(&g.row[x]);
+        const int w = by_head ? y : x, other = by_head ? x : y;
+        const int b = ldro(&g.row[w]), e1 = ldro(&g.row[w + 1]);
+        int a = INT_MAX;
+        for (int eb = b; eb < e1; eb += 32) {
+            const int e = eb + c.lane;
+            int cand = INT_MAX;
+            if (e < e1 && ldro(&g.col[e]) == other && (ldro_u8(&g.fwd[e]) != 0) != by_head)
+                cand = by_head ? ldro(&g.rev[e]) : e;
+            const int m = __reduce_min_sync(MF_FULL, cand);
+            if (m != INT_MAX) {
+                a = m;
+                break;
+            }
+        }
+        if (a != INT_MAX && c.lane == 0) {
+            const i64 cur = ldcap(&cap[a]);
+            cap[a] = max(ua, cur + ub);
+        }
+    }
+    __threadfence();
+    return c.sync();
+}
+
+__device__ void serve_loop(QCtx &c, const KParams &p, int gid) {
+    GroupCtl *gc = p.gctl + gid;
+    c.bar = &gc->bar;
+    const unsigned long long NONE = ~0ull;
+    // ---- wait for a slot
+    if (c.leader) {
+        int r = 0;
+        unsigned spins = 0;
+        u64 idle_since = 0;  // first time no group was seen serving (0: one was)
+        for (;;) {
+            r = p.slot_ready[gid];
+            if (r > 0) break;
+            if (*p.ring_stop) {
+                r = -1;
+                break;
+            }
+            __nanosleep(4000);
+            if ((++spins & 15u) == 0) {
+                // nobody serving for a millisecond: the launch is ending
+                if (ldcg(&p.srv->live) > 0) {
+                    idle_since = 0;
+                } else {
+                    const u64 now = globaltimer_ns();
+                    if (!idle_since) idle_since = now;
+                    else if (now - idle_since > 1000000ull) {
+                        r = -1;
+                        break;
+                    }
+                }
+            }
+        }
+        if (r > 0) {
+            __threadfence_system();
+            const volatile unsigned *src = reinterpret_cast<const volatile unsigned *>(&p.slot_tab[gid]);
+            unsigned *dst = reinterpret_cast<unsigned *>(&gc->slot);
+            for (int i = 0; i < (int)(sizeof(DSlot) / 4); ++i) dst[i] = src[i];
+            atomicAdd(&p.srv->live, 1);
+        }
+        gc->w[0] = r;
+        __threadfence();
+    }
+    if (!gsync(c.G, c.bar, c.err, c.lim)) return;
+    const int ready = ldcg(&gc->w[0]);
+    if (ready < 0) return;
+    c.st = gc->slot;
+    if (ready == 1) {
+        if (!srv_clear_slot(c, c.st, p.slot_n)) return;
+        if (c.leader) {
+            __threadfence_system();
+            p.slot_ready[gid] = 2;
+        }
+    }
+    c.clock = ldcg(c.st.clock);
+    c.no_cache = false;
+    for (;;) {
+        // ---- claim the next ticket (leader), broadcast through gctl
+        if (c.leader) {
+            unsigned long long q = NONE;
+            if (!*p.ring_stop) {
+                q = atomicAdd(&p.srv->next, 1ull);
+                const u64 t0 = globaltimer_ns();
+                unsigned spins = 0;
+                for (;;) {
+                    if (q < *p.ring_tail) break;
+                    const bool leave = *p.ring_stop || globaltimer_ns() - t0 > p.idle_limit_ns;
+                    // give the ticket back before leaving; if a later ticket
+                    // is claimed, wait until its holder has given it back
+                    if (leave && atomicCAS(&p.srv->next, q + 1, q) == q + 1) {
+                        q = NONE;
+                        break;
+                    }
+                    __nanosleep(2000);
+                    if ((++spins & 1023u) == 0 && globaltimer_ns() - t0 > p.idle_limit_ns + p.bar_limit_ns) {
+                        atomicCAS(p.err, 0, MFD_TIMEOUT);
+                        q = NONE;
+                        break;
+                    }
+                }
+            }
+            gc->q = q;
+            if (q != NONE) {
+                __threadfence_system();
+                const int e = (int)(q % (unsigned long long)p.ring_cap);
+                const volatile RingReq *rq = reinterpret_cast<const volatile RingReq *>(p.ring_req + e);
+                gc->w[0] = rq->kind;
+                gc->w[1] = rq->graph;
+                gc->w[2] = rq->s;
+                gc->w[3] = rq->t;
+                gc->w[4] = rq->epoch;
+                gc->w[5] = rq->upd_n;
+                const long long off = rq->upd_off;
+                const unsigned long long need = rq->need_done;
+                p.ring_done[e] = 2;
+                p.ring_t0[2 * e] = globaltimer_ns();
+                // the update waits for the earlier queries on its graph and
+                // batches; a query waits for the batches before it
+                GState *gs = p.gstate + rq->graph;
+                bool ok = true;
+                if (gc->w[0] == RQ_UPDATE) {
+                    ok = srv_wait_ge(p, &gs->epoch, gc->w[4]);
+                    const u64 tw = globaltimer_ns();
+                    unsigned sp = 0;
+                    while (ok && *(volatile unsigned long long *)&gs->done_q < need) {
+                        if (*(volatile int *)p.err) ok = false;
+                        __nanosleep(1000);
+                        if ((++sp & 63u) == 0 && globaltimer_ns() - tw > p.bar_limit_ns) {
+                            atomicCAS(p.err, 0, MFD_TIMEOUT);
+                            ok = false;
+                        }
+                    }
+                    __threadfence();
+                    *reinterpret_cast<long long *>(&gc->w[6]) = off;
+                } else {
+                    ok = srv_wait_ge(p, &gs->epoch, gc->w[4]);
+                    gc->w[6] = ldcg(&gs->no_cache);
+                }
+                (void)ok;  // a failed wait has raised the error word
+            }
+            __threadfence();
+        }
+        if (!gsync(c.G, c.bar, c.err, c.lim)) return;
+        const unsigned long long q = *(volatile unsigned long long *)&gc->q;
+        if (q == NONE) break;
+        const int e = (int)(q % (unsigned long long)p.ring_cap);
+        const int kind = ldcg(&gc->w[0]), gi = ldcg(&gc->w[1]);
+        if (kind == RQ_UPDATE) {
+            const long long off = __ldcg(reinterpret_cast<const long long *>(&gc->w[6]));
+            if (!srv_apply_updates(c, p, gi, off, ldcg(&gc->w[5]))) return;
+            if (c.leader) {
+                GState *gs = p.gstate + gi;
+                gs->no_cache = 1;
+                __threadfence();
+                atomicExch(&gs->epoch, ldcg(&gc->w[4]) + 1);
+                QOut z = {};
+                z.t_begin = z.t_done = globaltimer_ns();
+                p.out[e] = z;
+            }
+        } else {
+            const int s = ldcg(&gc->w[2]), t = ldcg(&gc->w[3]);
+            bind_graph(c, p, gi);
+            c.no_cache = ldcg(&gc->w[6]) != 0;
+            c.q_begin = globaltimer_ns();
+            if (s < 0 || t < 0 || s >= c.n || t >= c.n || s == t) {
+                if (c.leader) {
+                    QOut z = {};
+                    z.t_begin = z.t_done = c.q_begin;
+                    p.out[e] = z;
+                }
+            } else {
+                solve_query(c, p, e, s, t);
+                if (c.leader) *c.st.clock = c.clock;
+            }
+            if (*(volatile int *)p.err) return;
+            if (c.leader) {
+                __threadfence();
+                atomicAdd(&p.gstate[gi].done_q, 1ull);
+            }
+        }
+        if (*(volatile int *)p.err) return;
+        if (c.leader) {
+            __threadfence_system();
+            p.ring_t0[2 * e + 1] = globaltimer_ns();
+            __threadfence_system();
+            p.ring_done[e] = 1;
+        }
+        // stamps are compared against the slot's 32-bit clock: reset the
+        // slot long before it could wrap
+        if (c.clock > (1u << 30)) {
+            if (!srv_clear_slot(c, c.st, p.slot_n)) return;
+            c.clock = 0;
+        }
+        if (!gsync(c.G, c.bar, c.err, c.lim)) return;
+    }
+    if (c.leader) atomicSub(&p.srv->live, 1);
+}
+
 __global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
     QCtx c;
     c.G = p.G;
@@ -2412,75 +2691,29 @@ __global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
     c.w_arcs = c.w_verts = c.w_push = 0;
     c.t_start = globaltimer_ns();
     c.time_limit = p.time_limit_ns;
+    c.no_cache = false;
+    MF_TRACE(1, gid);
+    if (p.ring_tail) {
+        serve_loop(c, p, gid);
+        return;
+    }
     DSlot gslot = p.slots[gid];
     c.bar = gslot.bar;
-    MF_TRACE(1, gid);
     for (;;) {
         // take a query (group leader), broadcast through the group slot
         int *qcell = gslot.cnt + CNT_Q;
-        if (c.leader) {
-            int q;
-            if (p.ring_tail) {
-                q = atomicAdd(p.q_next, 1);
-                u64 t0 = globaltimer_ns();
-                unsigned spins = 0;
-                for (;;) {
-                    if (q < *p.ring_tail) break;
-                    if (*p.ring_stop) {
-                        q = INT_MAX;
-                        break;
-                    }
-                    __nanosleep(2000);
-                    if ((++spins & 63u) == 0 && globaltimer_ns() - t0 > p.idle_limit_ns) {
-                        q = INT_MAX;
-                        break;
-                    }
-                }
-                if (q != INT_MAX) {
-                    __threadfence_system();
-                    volatile const int *rq = reinterpret_cast<volatile const int *>(p.ring_req + q);
-                    gslot.cnt[CNT_RS] = rq[0];
-                    gslot.cnt[CNT_RT] = rq[1];
-                    gslot.cnt[CNT_RG] = rq[2];
-                    p.ring_done[q] = 2;
-                    p.ring_t0[2 * q] = globaltimer_ns();
-                }
-            } else {
-                q = atomicAdd(p.q_next, 1);
-            }
-            *qcell = q;
-        }
+        if (c.leader) *qcell = atomicAdd(p.q_next, 1);
         if (!gsync(c.G, c.bar, c.err, c.lim)) return;
         int q = ldcg(qcell);
-        int nlimit = p.ring_tail ? INT_MAX - 1 : p.nq;
-        if (q >= nlimit) break;
-        int s, t, gi, si;
-        if (p.ring_tail) {
-            s = ldcg(&gslot.cnt[CNT_RS]);
-            t = ldcg(&gslot.cnt[CNT_RT]);
-            gi = ldcg(&gslot.cnt[CNT_RG]);
-            si = gid;
-        } else {
-            s = p.q_s[q];
-            t = p.q_t[q];
-            gi = p.q_g ? p.q_g[q] : 0;
-            si = p.q_slot ? p.q_slot[q] : gid;
-        }
-        DGraph g = p.graphs[gi];
-        c.n = g.n;
-        c.R = g.R;
-        c.row = g.row;
-        c.col = g.col;
-        c.rev = g.rev;
-        c.rof = g.region_of;
-        c.cap = g.cap;
-        c.gr = &p.graphs[gi];
-        c.giants = g.giants;
-        c.ngiant = g.giants ? g.ngiant : 0;
+        if (q >= p.nq) break;
+        const int s = p.q_s[q], t = p.q_t[q];
+        const int gi = p.q_g ? p.q_g[q] : 0;
+        const int si = p.q_slot ? p.q_slot[q] : gid;
+        bind_graph(c, p, gi);
         c.st = p.slots[si];
         c.clock = ldcg(c.st.clock);
         c.q_begin = globaltimer_ns();
-        if (s < 0 || t < 0 || s >= g.n || t >= g.n || (s == t && p.mode != KM_KEPTSET)) {
+        if (s < 0 || t < 0 || s >= c.n || t >= c.n || (s == t && p.mode != KM_KEPTSET)) {
             if (c.leader) {
                 QOut z = {};
                 z.t_begin = z.t_done = c.q_begin;
@@ -2493,12 +2726,6 @@ __global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
             if (c.leader) *c.st.clock = c.clock;
         }
         if (*(volatile int *)p.err) return;
-        if (p.ring_tail && c.leader) {
-            __threadfence_system();
-            p.ring_t0[2 * q + 1] = globaltimer_ns();
-            __threadfence_system();
-            p.ring_done[q] = 1;
-        }
         if (!gsync(c.G, c.bar, c.err, c.lim)) return;
     }
 }

@@ -35,6 +35,7 @@ struct DGraph {
     // loops then take every vertex themselves).
     const int *giants;
     int ngiant;
+    const unsigned char *fwd;  // arcs: 1 = forward arc of an input edge (capacity updates)
 };
 
 // Vertices with more arcs than this are "giants": loops that give each
@@ -172,6 +173,60 @@ struct KcOut {
 #define KC_F 1
 #define KC_B 2
 
+// ---- continuous-batching server ---------------------------------------------
+// One request in the server's ring (host-written, mapped).  kind 0: an (s,t)
+// query on `graph` that must see the graph after `epoch` capacity-update
+// batches on it; kind 1: the update batch number `epoch` of `graph`, whose
+// upd_n entries start at upd_off in the update arena, applied once the
+// graph's first `need_done` queries (all queries submitted before it) are
+// done.
+struct RingReq {
+    int kind;
+    int graph;
+    int s, t;
+    int epoch;
+    int upd_n;
+    long long upd_off;
+    unsigned long long need_done;
+    long long pad;
+};
+#define RQ_QUERY 0
+#define RQ_UPDATE 1
+
+// One capacity change in an update batch: the first forward arc u -> v
+// (internal ids) gets capacity max(a, cap + b).  The host folds every change
+// of one (u, v) pair in a batch into one entry: a sequence of "cap += d,
+// clamped at 0" steps composes to exactly this form.
+struct UpdEntry {
+    int u, v;
+    i64 a, b;
+};
+
+// Per-graph server state (device): update batches applied, queries done,
+// kept-set cache invalid (set by the first update).
+struct GState {
+    int epoch;
+    int no_cache;
+    unsigned long long done_q;
+};
+
+// Per-group server control block (device): the group's barrier (a group
+// may run before it has a slot), broadcast words and its slot.
+struct GroupCtl {
+    GroupBar bar;
+    unsigned long long q;
+    int w[8];
+    DSlot slot;
+};
+
+// Server-wide control (device): the next request to claim, and the count of
+// groups serving (parked groups leave when it reaches 0).
+struct SrvCtl {
+    unsigned long long next;
+    int live;
+    int pad;
+};
+
 struct KParams {
     const DGraph *graphs;
     DSlot *slots;
@@ -196,14 +251,23 @@ struct KParams {
     const int *ov_arc;
     const i64 *ov_cap;
     long long ov_n;
-    // serving ring (mode KM_SOLVE with ring != NULL): requests are read from
-    // ring_req[i] once ring_tail (host-written) exceeds i; completion flags.
-    volatile int *ring_tail;
-    const int4 *ring_req;        // (s, t, graph, unused)
-    volatile int *ring_done;     // 1 when the request finished
-    u64 *ring_t0;                // admission / completion timestamps (ns)
+    // serving ring (mode KM_SOLVE with ring_tail != NULL): request k (a
+    // 64-bit ticket) lives in entry k % ring_cap and may be claimed once the
+    // host-written ring_tail exceeds k.  All host-side arrays are mapped.
+    volatile unsigned long long *ring_tail;
+    const RingReq *ring_req;
+    int ring_cap;
+    volatile int *ring_done;     // per entry: 2 while running, 1 when finished
+    u64 *ring_t0;                // per entry: admission / completion timestamps (ns)
     volatile int *ring_stop;     // host sets 1 to end the persistent kernel
-    u64 idle_limit_ns;
+    u64 idle_limit_ns;           // a group idle this long leaves
+    SrvCtl *srv;
+    GState *gstate;              // per graph
+    GroupCtl *gctl;              // per group
+    const volatile DSlot *slot_tab;   // per group: its slot (mapped)
+    volatile int *slot_ready;    // per group: 0 none yet, 1 new (clear it first), 2 ready
+    int slot_n;                  // vertices the server's slots are sized for
+    const UpdEntry *srv_upd;     // update arena (mapped)
 };
 
 void mf_launch_kernel(const KParams &p, int grid, int threads, cudaStream_t st, bool cooperative,

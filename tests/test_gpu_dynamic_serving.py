@@ -156,6 +156,100 @@ def test_server_results_equal_alone_and_in_the_mix():
         g.close()
 
 
+def test_server_interleaves_updates_and_queries():
+    """Queries and capacity-update batches on two graphs go through one
+    server in a random order, with pauses so some arrive while others run.
+    Every answer equals the oracle's Dinic on its graph as left by exactly the
+    update batches submitted before it; a ring of 64 entries is reused many
+    times over; after the server is gone the graphs solve on the updated
+    capacities (their kept-set caches dropped)."""
+    import os
+    rng = np.random.default_rng(21)
+    graphs, ocsr, fwds, ends = [], [], [], []
+    for i, scale in enumerate((11, 13)):
+        n = 1 << scale
+        u, v, c = mf.gen_rmat(scale, 16 * n, seed=60 + i)
+        graphs.append(mf.Graph.from_edges(n, u, v, c, R=32))
+        g = O.build_csr(n, u, v, c)
+        ocsr.append(g)
+        fwds.append(g.cap > 0)
+        ends.append((u, v, n))
+    old = os.environ.get("MF_SERVER_RING")
+    os.environ["MF_SERVER_RING"] = "64"
+    try:
+        sv = mf.Server(graphs, mf.opts(group_ctas=2), max_slots=6)
+    finally:
+        if old is None:
+            del os.environ["MF_SERVER_RING"]
+        else:
+            os.environ["MF_SERVER_RING"] = old
+    expected, tickets = [], []
+    nupd = 0
+    for k in range(150):
+        gi = int(rng.integers(0, 2))
+        u, v, n = ends[gi]
+        if rng.random() < 0.25:
+            uu, vv, d = make_updates(rng, u, v, int(rng.integers(5, 300)), n)
+            tickets.append(sv.update(gi, uu, vv, d))
+            apply_updates_oracle(ocsr[gi], fwds[gi], uu, vv, d)
+            expected.append(None)
+            nupd += 1
+        else:
+            hub = rng.random() < 0.5
+            deg = np.diff(ocsr[gi].row)
+            if hub:
+                top = np.argsort(-deg)[:max(2, n // 100)]
+                a, b = int(rng.choice(top)), int(rng.choice(top))
+            else:
+                a, b = int(rng.integers(0, n)), int(rng.integers(0, n))
+            tickets.append(sv.submit(gi, a, b))
+            expected.append(O.dinic(ocsr[gi], a, b) if a != b else 0)
+        if k % 5 == 2:
+            time.sleep(0.003)
+        # poll every answer before its ring entry (64) is reused
+        if k % 16 == 15:
+            sv.drain()
+            for tk, ex in zip(tickets[-16:], expected[-16:]):
+                done, f, lat, st = sv.poll(tk)
+                assert done and st == 0
+                if ex is not None:
+                    assert f == ex, (tk, f, ex)
+    sv.drain()
+    for tk, ex in list(zip(tickets, expected))[-(150 % 16):]:
+        done, f, lat, st = sv.poll(tk)
+        assert done and st == 0
+        if ex is not None:
+            assert f == ex, (tk, f, ex)
+    assert nupd >= 20 and 1 <= sv.slots <= 6
+    # an expired ticket is reported as such
+    with pytest.raises(mf.MaxflowError):
+        sv.poll(tickets[0])
+    sv.close()
+    for gi, g in enumerate(graphs):
+        n = ends[gi][2]
+        for a, b in [(0, 1), (3, n - 1), (n // 2, 7)]:
+            assert g.solve(a, b)[0] == O.dinic(ocsr[gi], a, b)
+        g.close()
+
+
+def test_server_admits_slots_as_requests_open():
+    """The server starts with a few slots and admits more (from free HBM)
+    while requests queue up; every answer stays exact."""
+    n = 1 << 14
+    u, v, c = mf.gen_rmat(14, 16 * n, seed=77)
+    s, t = mf.gen_queries_hub(n, u, v, 48, 16, seed=78)
+    g = O.build_csr(n, u, v, c)
+    exp = [O.dinic(g, a, b) for a, b in zip(s, t)]
+    with mf.Graph.from_edges(n, u, v, c, R=32) as eg:
+        with mf.Server([eg], mf.opts(group_ctas=2)) as sv:
+            first = sv.slots
+            assert 1 <= first <= 4
+            tks = [sv.submit(0, a, b) for a, b in zip(s, t)]
+            sv.drain()
+            assert [sv.poll(tk)[1] for tk in tks] == exp
+            assert sv.slots > first
+
+
 def test_autotune_consistent():
     n = 1 << 12
     u, v, c = mf.gen_rmat(12, 16 * n, seed=3)
