@@ -1861,6 +1861,7 @@ struct mf_server {
     cudaStream_t stream = nullptr, side = nullptr;
     cudaEvent_t done_ev = nullptr;
     bool running = false;
+    bool launched = false;  // a launch has happened (its error word is meaningful)
 };
 
 static bool server_alive(mf_server *sv) {
@@ -1906,11 +1907,13 @@ static int server_launch(mf_server *sv) {
     if (le != cudaSuccess) return fail(MF_ERR_CUDA, "server launch: %s", cudaGetErrorString(le));
     CK(cudaEventRecord(sv->done_ev, sv->stream));
     sv->running = true;
+    sv->launched = true;
     return MF_OK;
 }
 
 // Device status of the last launch once it has ended (0: none).
 static int server_error(mf_server *sv) {
+    if (!sv->launched) return 0;
     int herr = 0;
     if (cudaMemcpy(&herr, sv->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return MFD_TIMEOUT;
     return herr;
@@ -2059,6 +2062,7 @@ int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int ma
     if (cudaMemcpy(sv->d_graphs, dg.data(), sizeof(DGraph) * ngraphs, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(sv->d_gstate, 0, sizeof(GState) * ngraphs) != cudaSuccess ||
         cudaMemset(sv->d_srv, 0, sizeof(SrvCtl)) != cudaSuccess ||
+        cudaMemset(sv->d_err, 0, sizeof(int)) != cudaSuccess ||
         cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&sv->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&sv->done_ev, cudaEventDisableTiming) != cudaSuccess)
