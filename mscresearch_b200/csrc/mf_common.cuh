@@ -28,9 +28,16 @@ __device__ __forceinline__ unsigned char ldro_u8(const unsigned char *p) { retur
 __device__ __forceinline__ int ldcg(const int *p) { return __ldcg(p); }
 __device__ __forceinline__ unsigned ldcg(const unsigned *p) { return __ldcg(p); }
 __device__ __forceinline__ i64 ldcg(const i64 *p) { return __ldcg(p); }
-// Capacities: read through L2 (coherent), since a serving launch applies
-// capacity updates to the graph it reads while it runs.
+// Capacities.  The serving kernel (mf_serve_kernel.cu, MF_SERVE_TU) applies
+// capacity updates to the graphs it reads while it runs, so it reads them
+// through L2 (coherent); every other launch treats them as read-only.
+#ifdef MF_SERVE_TU
 __device__ __forceinline__ i64 ldcap(const i64 *p) { return __ldcg(p); }
+__device__ __forceinline__ longlong2 ldcap2(const longlong2 *p) { return __ldcg(p); }
+#else
+__device__ __forceinline__ i64 ldcap(const i64 *p) { return __ldg(p); }
+__device__ __forceinline__ longlong2 ldcap2(const longlong2 *p) { return __ldg(p); }
+#endif
 
 // ---------------------------------------------------------------------------
 // Self-check builds (-DMF_CHECKS, libmfb200_chk.so): every warp records the

@@ -911,7 +911,7 @@ __device__ bool init_state(QCtx &c, int nv, unsigned M, bool count_mask = true) 
         i64 swept = 0;
         for (i64 k = gt; k < nq4; k += gT) {
             const int4 w = __ldg(&col4[k]);
-            const longlong2 ca = __ldcg(&cap2[2 * k]), cb = __ldcg(&cap2[2 * k + 1]);
+            const longlong2 ca = ldcap2(&cap2[2 * k]), cb = ldcap2(&cap2[2 * k + 1]);
             longlong2 ra, rb;
             ra.x = ldcg(&mark[w.x]) >= M ? ca.x : 0;
             ra.y = ldcg(&mark[w.y]) >= M ? ca.y : 0;
@@ -2411,6 +2411,7 @@ __device__ __forceinline__ void bind_graph(QCtx &c, const KParams &p, int gi) {
     c.ngiant = g.giants ? g.ngiant : 0;
 }
 
+#ifdef MF_SERVE_TU
 // ---------------------------------------------------------------------------
 // Serving loop (KParams::ring_tail != NULL).  Each group owns the slot the
 // host published for it in slot_tab (a group still without one is parked
@@ -2674,11 +2675,13 @@ __device__ void serve_loop(QCtx &c, const KParams &p, int gid) {
     if (c.leader) atomicSub(&p.srv->live, 1);
 }
 
-__global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
-    QCtx c;
+#endif  // MF_SERVE_TU
+
+// Per-thread context of a launch: group geometry, limits, counters.
+__device__ __forceinline__ int init_ctx(QCtx &c, const KParams &p) {
     c.G = p.G;
     c.crank = blockIdx.x % p.G;
-    int gid = blockIdx.x / p.G;
+    const int gid = blockIdx.x / p.G;
     c.wpc = blockDim.x >> 5;
     c.warp = threadIdx.x >> 5;
     c.gw = c.crank * c.wpc + c.warp;
@@ -2692,11 +2695,17 @@ __global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
     c.t_start = globaltimer_ns();
     c.time_limit = p.time_limit_ns;
     c.no_cache = false;
+    return gid;
+}
+
+#ifndef MF_SERVE_TU
+// Batched / single / session solves: groups take query indices from a
+// device counter until nq are taken.  (Serving has its own kernel below, so
+// each kernel inlines one copy of the solve.)
+__global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
+    QCtx c;
+    const int gid = init_ctx(c, p);
     MF_TRACE(1, gid);
-    if (p.ring_tail) {
-        serve_loop(c, p, gid);
-        return;
-    }
     DSlot gslot = p.slots[gid];
     c.bar = gslot.bar;
     for (;;) {
@@ -2730,6 +2739,33 @@ __global__ void __launch_bounds__(512, 2) mf_kernel(KParams p) {
     }
 }
 
+#else  // MF_SERVE_TU
+// Serving (KParams::ring_tail != NULL): see serve_loop.
+__global__ void __launch_bounds__(512, 2) mf_serve_kernel(KParams p) {
+    QCtx c;
+    const int gid = init_ctx(c, p);
+    MF_TRACE(1, gid);
+    serve_loop(c, p, gid);
+}
+
+cudaError_t serve_launch_impl(const KParams &p, int grid, int threads, cudaStream_t st, bool cooperative) {
+    void *args[] = {(void *)&p};
+    if (cooperative)
+        return cudaLaunchCooperativeKernel((void *)mf_serve_kernel, dim3(grid), dim3(threads), args, 0, st);
+    return cudaLaunchKernel((void *)mf_serve_kernel, dim3(grid), dim3(threads), args, 0, st);
+}
+
+int serve_occupancy_impl(int threads) {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, mf_serve_kernel) != cudaSuccess || threads > fa.maxThreadsPerBlock) return 0;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mf_serve_kernel, threads, 0) != cudaSuccess) return 0;
+    return nb;
+}
+#endif  // MF_SERVE_TU
+
+#ifndef MF_SERVE_TU
+
 #ifdef MF_CHECKS
 static unsigned *h_chk_trace = nullptr;
 static int *h_chk_bad = nullptr;
@@ -2762,20 +2798,25 @@ void mf_launch_kernel(const KParams &p, int grid, int threads, cudaStream_t st, 
 #ifdef MF_CHECKS
     mf_chk_install(grid * threads / 32);
 #endif
+    if (p.ring_tail) {
+        *err = mf_launch_serve_kernel(p, grid, threads, st, cooperative);
+        return;
+    }
     void *args[] = {(void *)&p};
     if (cooperative)
         *err = cudaLaunchCooperativeKernel((void *)mf_kernel, dim3(grid), dim3(threads), args, 0, st);
-    else {
-        mf_kernel<<<grid, threads, 0, st>>>(p);
-        *err = cudaGetLastError();
-    }
+    else
+        *err = cudaLaunchKernel((void *)mf_kernel, dim3(grid), dim3(threads), args, 0, st);
 }
 
+// Co-resident CTAs per SM that both kernels allow (every launch size is
+// derived from it).
 int mf_kernel_max_blocks_per_sm(int threads) {
     cudaFuncAttributes fa;
     if (cudaFuncGetAttributes(&fa, mf_kernel) != cudaSuccess || threads > fa.maxThreadsPerBlock) return 0;
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mf_kernel, threads, 0) != cudaSuccess)
-        return 0;
-    return nb;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mf_kernel, threads, 0) != cudaSuccess) return 0;
+    const int ns = mf_serve_kernel_max_blocks_per_sm(threads);
+    return nb < ns ? nb : ns;
 }
+#endif  // MF_SERVE_TU

@@ -273,3 +273,7 @@ struct KParams {
 void mf_launch_kernel(const KParams &p, int grid, int threads, cudaStream_t st, bool cooperative,
                       cudaError_t *err);
 int mf_kernel_max_blocks_per_sm(int threads);
+// mf_serve_kernel.cu: the serving kernel (the solver compiled with coherent
+// capacity loads).
+cudaError_t mf_launch_serve_kernel(const KParams &p, int grid, int threads, cudaStream_t st, bool cooperative);
+int mf_serve_kernel_max_blocks_per_sm(int threads);
