@@ -72,6 +72,10 @@ typedef struct mf_opts {
     int schedule;          /* batched solves: 1 = start the queries expected to cost most first
                               (s and t in the cached component, then larger min(deg s, deg t));
                               0 = input order.  Results are in input order either way. */
+    int relabel_early_stop; /* 1 = a global relabel's search ends once every active vertex has its
+                               exact height (vertices it did not reach stay at height n until the
+                               next relabel; a search that cannot reach every active vertex runs to
+                               the end, so the relabel that ends a solve is exact) */
 } mf_opts;
 
 /* Per-query statistics (all counts exact device counters). */

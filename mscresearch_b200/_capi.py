@@ -42,6 +42,7 @@ class MfOpts(C.Structure):
         ("verbose", C.c_int),
         ("use_kept_cache", C.c_int),
         ("schedule", C.c_int),
+        ("relabel_early_stop", C.c_int),
     ]
 
 

@@ -528,6 +528,8 @@ KOpts resolve_opts(const mf_opts &o, int avg_deg) {
     k.bu_factor = 56;
     if (const char *e = getenv("MF_BU_FACTOR")) k.bu_factor = std::max(1, atoi(e));
     k.iter_max = o.iter_max > 0 ? o.iter_max : 20000000;
+    k.gr_stop = o.relabel_early_stop;
+    if (const char *e = getenv("MF_RELABEL_EARLY_STOP")) k.gr_stop = atoi(e);
     return k;
 }
 
@@ -909,6 +911,7 @@ void mf_opts_default(mf_opts *o) {
     o->verbose = 0;
     o->use_kept_cache = 1;
     o->schedule = 1;
+    o->relabel_early_stop = 1;
 }
 
 const char *mf_last_error_string(void) { return g_err.c_str(); }

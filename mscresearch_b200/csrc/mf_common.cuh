@@ -140,6 +140,8 @@ struct GroupBar {
     unsigned gen;
     int snap;      // values captured by the last arriver (gsync_snap)
     int snap2;
+    int snap3;
+    int pad;
 };
 
 // gsync_snap additionally returns, to every thread of the group, the values
@@ -148,15 +150,17 @@ struct GroupBar {
 // the barrier early may already be appending).
 __device__ __forceinline__ bool gsync_impl(int G, GroupBar *bar, int *err, u64 limit_ns,
                                            const int *src, const int *src2, int *snap_out,
-                                           int *snap2_out) {
+                                           int *snap2_out, const int *src3 = nullptr,
+                                           int *snap3_out = nullptr) {
     __shared__ int s_ok;
-    __shared__ int s_snap, s_snap2;
+    __shared__ int s_snap, s_snap2, s_snap3;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
         if (G == 1 && src) {
             s_snap = *(volatile const int *)src;
             s_snap2 = *(volatile const int *)src2;
+            if (src3) s_snap3 = *(volatile const int *)src3;
         }
         if (G > 1) {
             volatile unsigned *vgen = &bar->gen;
@@ -168,6 +172,7 @@ __device__ __forceinline__ bool gsync_impl(int G, GroupBar *bar, int *err, u64 l
                     __threadfence();
                     *(volatile int *)&bar->snap = *(volatile const int *)src;
                     *(volatile int *)&bar->snap2 = *(volatile const int *)src2;
+                    if (src3) *(volatile int *)&bar->snap3 = *(volatile const int *)src3;
                 }
                 atomicExch(&bar->arrive, 0u);
                 __threadfence();
@@ -192,6 +197,7 @@ __device__ __forceinline__ bool gsync_impl(int G, GroupBar *bar, int *err, u64 l
             if (src) {
                 s_snap = *(volatile int *)&bar->snap;
                 s_snap2 = *(volatile int *)&bar->snap2;
+                if (src3) s_snap3 = *(volatile int *)&bar->snap3;
             }
         }
         if (*(volatile int *)err) ok = 0;
@@ -202,6 +208,7 @@ __device__ __forceinline__ bool gsync_impl(int G, GroupBar *bar, int *err, u64 l
         *snap_out = s_snap;
         *snap2_out = s_snap2;
     }
+    if (snap3_out) *snap3_out = s_snap3;
     return s_ok != 0;
 }
 

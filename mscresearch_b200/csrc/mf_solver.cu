@@ -55,6 +55,8 @@
 #define NBANKS 8
 #define CNT_BACK 16
 #define CNT_HUBCH 30  // total chunks of the current hub pass
+#define CNT_ACT 40    // global relabel: active vertices to label
+#define CNT_FOUND 41  // global relabel: active vertices labelled so far
 #define CNT_Q 8      // query handed to the group
 #define CNT_FLAG 9   // misc uniform flag
 #define CNT_RS 10    // serving: request source / sink / graph
@@ -135,6 +137,11 @@ struct QCtx {
     // as of the barrier
     __device__ bool sync_tails(int bank, int &ft, int &bt) {
         return gsync_snap(G, bar, err, lim, &st.cnt[bank], &st.cnt[CNT_BACK + bank], &ft, &bt);
+    }
+    // the same, also returning the value of the control word cnt[w3] as of
+    // the barrier
+    __device__ bool sync_tails3(int bank, int &ft, int &bt, int w3, int &v3) {
+        return gsync_impl(G, bar, err, lim, &st.cnt[bank], &st.cnt[CNT_BACK + bank], &ft, &bt, &st.cnt[w3], &v3);
     }
     __device__ int take_bank() {
         int b = seq & (NBANKS - 1);
@@ -434,7 +441,7 @@ struct NoLevelHook {
 #define SOLO_MAX 96         // a hub-free top-down frontier at most this large runs solo
 #define SOLO_LEVELS 1024    // levels per solo episode at most
 #define CNT_SOLO 32         // cnt[32..38]: state published by a solo episode
-static_assert(CNT_SOLO >= CNT_BACK + NBANKS && CNT_SOLO > CNT_HUBCH && CNT_SOLO + 7 <= CNT_WORDS,
+static_assert(CNT_SOLO >= CNT_BACK + NBANKS && CNT_SOLO > CNT_HUBCH && CNT_SOLO + 8 <= CNT_ACT && CNT_FOUND < CNT_WORDS,
               "solo state must not overlap the other control words");
 
 // Direction-optimizing BFS: a level runs bottom-up when the frontier holds
@@ -452,11 +459,15 @@ static_assert(CNT_SOLO >= CNT_BACK + NBANKS && CNT_SOLO > CNT_HUBCH && CNT_SOLO 
 // the previous level's frontier.
 template <class Claim, class UF, class UB, class Par, class Set, class Hook = NoLevelHook>
 __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, int nuf, UF uf, int nub,
-                        UB ub, Par par, Set set, Hook on_level = Hook{}, int *levels_out = nullptr) {
+                        UB ub, Par par, Set set, Hook on_level = Hook{}, int *levels_out = nullptr,
+                        int stop_at = -1) {
+    // stop_at >= 0: the search ends after the first level by which the
+    // control word cnt[CNT_FOUND] (raised by cl / set) has reached stop_at
     int flo = 0, blo = 0, pflo = 0, pblo = 0, level = 0, nbu = 0, nsolo = 0;
+    bool stopped = stop_at == 0;
     const long long nu = (long long)nuf + nub;
     const int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
-    while (flo < fhi || blo < bhi) {
+    while (!stopped && (flo < fhi || blo < bhi)) {
         const long long visited = (long long)fhi + bhi;
         const long long fsize = (long long)(fhi - flo) + (bhi - blo);
         // bottom-up sweeps the whole universe, so the frontier must also be a
@@ -480,6 +491,14 @@ __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, i
                     blo = bhi;
                     bhi = bt;
                     ++level;
+                    // only this CTA claims during a solo episode, and its
+                    // claims are complete at the block barrier above
+                    bool done = stop_at > 0 && ldcg(&c.st.cnt[CNT_FOUND]) >= stop_at;
+                    __syncthreads();
+                    if (done) {
+                        stopped = true;
+                        break;
+                    }
                     const long long fs = (long long)(fhi - flo) + (bhi - blo);
                     const long long vis = (long long)fhi + bhi;
                     if (fs == 0 || fs > SOLO_MAX || bhi != blo || (nu > vis && fs * c.bu_factor > nu - vis && fs * 64 > nu))
@@ -494,6 +513,7 @@ __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, i
                     o[4] = level;
                     o[5] = pflo;
                     o[6] = pblo;
+                    o[7] = stopped ? 1 : 0;
                 }
             }
             if (!c.sync()) return false;
@@ -506,6 +526,7 @@ __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, i
             level = ldcg(&o[4]);
             pflo = ldcg(&o[5]);
             pblo = ldcg(&o[6]);
+            stopped = ldcg(&o[7]) != 0;
             continue;
         }
         MF_TRACE(10, level);
@@ -516,7 +537,13 @@ __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, i
         } else
             td_level(c, Q, bank, flo, fhi, blo, bhi, level, cl, c.gw, c.gW);
         int ft = 0, bt = 0;
-        if (!c.sync_tails(bank, ft, bt)) return false;
+        if (stop_at > 0) {
+            int found = 0;
+            if (!c.sync_tails3(bank, ft, bt, CNT_FOUND, found)) return false;
+            stopped = found >= stop_at;
+        } else if (!c.sync_tails(bank, ft, bt)) {
+            return false;
+        }
         pflo = flo;
         pblo = blo;
         flo = fhi;
@@ -983,7 +1010,7 @@ __device__ bool preflow(QCtx &c, int s) {
 // (atomicOr on the visited word).  Bottom-up: an unvisited kept vertex w
 // takes level + 1 when one of its residual arcs reaches the frontier map.
 // Claims write the height and the next frontier bit.
-__device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &depth) {
+__device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &depth, int stop_at) {
     const int W = bitmap_words(c.n);
     unsigned *vis = c.st.bits + W, *F = c.st.bits + 2 * W;
     const int *rev = c.rev;
@@ -991,6 +1018,11 @@ __device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &de
     int *h = c.st.h;
     const int *vl = c.st.vlist;
     auto fmap = [&](int level) -> unsigned * { return F + (size_t)(level % 3) * W; };
+    // with stop_at >= 0, every labelled vertex holding excess is counted in
+    // cnt[CNT_FOUND] (the search ends once all active vertices are labelled)
+    const i64 *ex = c.st.ex;
+    int *found = c.st.cnt + CNT_FOUND;
+    const bool count = stop_at > 0;
     auto relab = [&](int v, int e, int w, int level) -> bool {
         const unsigned bit = 1u << (w & 31);
         unsigned vw = ldcg(&vis[w >> 5]);
@@ -999,6 +1031,7 @@ __device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &de
         if (atomicOr(&vis[w >> 5], bit) & bit) return false;
         h[w] = level + 1;
         atomicOr(&fmap(level + 1)[w >> 5], bit);
+        if (count && ldcg(&ex[w]) > 0) atomicAdd(found, 1);
         return true;
     };
     auto unvisited = [&](int w) -> bool { return !((ldcg(&vis[w >> 5]) >> (w & 31)) & 1u); };
@@ -1021,6 +1054,7 @@ __device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &de
         h[w] = level + 1;
         atomicOr(&vis[w >> 5], bit);
         atomicOr(&fmap(level + 1)[w >> 5], bit);
+        if (count && ldcg(&ex[w]) > 0) atomicAdd(found, 1);
         return true;
     };
     // at level L the previous frontier's bits leave map (L - 1) % 3, which
@@ -1038,7 +1072,8 @@ __device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &de
             atomicAnd(&z[v >> 5], ~(1u << (v & 31)));
         }
     };
-    return bfs_dir(c, c.st.qa, bank, fhi, bhi, relab, c.vf, uf, nv - c.vf, ub, par, set, clear_prev, &depth);
+    return bfs_dir(c, c.st.qa, bank, fhi, bhi, relab, c.vf, uf, nv - c.vf, ub, par, set, clear_prev, &depth,
+                   stop_at);
 }
 
 // Kept-vertex bitmap of the query (bit v: mark[v] >= M), read by every
@@ -1064,7 +1099,7 @@ __device__ bool build_kept_bits(QCtx &c, unsigned M) {
 // Returns counts in naf / nab (active front / back) and nd (deficits).
 __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int blockv, int srcv,
                                bool deficit_seeds, int *L, int lbk, int &naf, int &nab, int &nd,
-                               i64 *&ab, int &depth) {
+                               i64 *&ab, int &depth, bool early_stop) {
     MF_TRACE(40, nv);
     int qbk = c.take_bank();
     const int n = c.n;
@@ -1081,18 +1116,26 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
             F0[W + wd] = 0;
             F0[2 * W + wd] = 0;
         }
+        if (c.leader) {
+            c.st.cnt[CNT_ACT] = 0;
+            c.st.cnt[CNT_FOUND] = 0;
+        }
     }
     if (!c.sync()) return false;
     MF_TRACE(42, nv);
-    // seeds
+    // seeds (and, for an early stop, the count of active vertices: the
+    // vertices the search labels and that hold excess)
+    int nact = 0;
     for (int base = c.gw * 32; base < nv; base += c.gW * 32) {
         int i = base + c.lane;
-        bool seed = false;
+        bool seed = false, act = false;
         int v = 0;
         if (i < nv) {
             v = c.vat(i);
+            const i64 ev = ldcg(&c.st.ex[v]);
             if (v == sinkv) seed = true;
-            else if (deficit_seeds && v != blockv && v != srcv && ldcg(&c.st.ex[v]) < 0) seed = true;
+            else if (deficit_seeds && v != blockv && v != srcv && ev < 0) seed = true;
+            act = !seed && v != blockv && ev > 0;
             if (seed) {
                 atomicOr(&vis[v >> 5], 1u << (v & 31));
                 atomicOr(&F0[v >> 5], 1u << (v & 31));
@@ -1100,12 +1143,20 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
             // every kept vertex starts the search at height n (unreached)
             c.st.h[v] = seed ? 0 : n;
         }
+        nact += __popc(__ballot_sync(MF_FULL, act));
         append2(c, seed, v, c.st.qa, qbk);
     }
+    if (early_stop && c.lane == 0 && nact) atomicAdd(&c.st.cnt[CNT_ACT], nact);
     int f0 = 0, b0 = 0;
     if (!c.sync_tails(qbk, f0, b0)) return false;
     MF_TRACE(43, f0 + b0);
-    if (!relabel_bfs(c, nv, qbk, f0, b0, depth)) return false;
+    // Early stop: once every active vertex holds its exact height the
+    // search ends; vertices it did not reach keep height n, which no push
+    // can reach (a push needs a vertex one level higher), until the next
+    // relabel.  A search that cannot reach some active vertex runs to the
+    // end as before, so the relabel that ends a phase stays exact.
+    const int stop_at = early_stop ? ldcg(&c.st.cnt[CNT_ACT]) : -1;
+    if (!relabel_bfs(c, nv, qbk, f0, b0, depth, stop_at)) return false;
     int *h = c.st.h;
 
     // Active list in decreasing height: the search queue (every reached
@@ -1694,8 +1745,10 @@ __device__ bool rm_pass(QCtx &c, int nv, unsigned M, int hlo, int hhi, int s, in
             i64 d = 0;
             if (e < e1) {
                 int w = ldro(&c.col[e]);
-                if (ldcg(&c.st.mark[w]) >= M && ldcg(&c.st.h[w]) > hv + 1 &&
-                    ldcg(&c.st.ex[w]) <= 0) {
+                // heads at height n (not reached by the last relabel's
+                // search) are left alone: nothing can push into them
+                const int hw = ldcg(&c.st.mark[w]) >= M ? ldcg(&c.st.h[w]) : 0;
+                if (hw > hv + 1 && hw < n && ldcg(&c.st.ex[w]) <= 0) {
                     int re = ldro(&c.rev[e]);
                     if (ldcg(&c.st.res[re]) > 0) {
                         d = (i64)atomicExch(reinterpret_cast<u64 *>(&c.st.res[re]), 0ull);
@@ -1755,7 +1808,8 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
         int lbk = c.take_bank();
         u64 t0 = globaltimer_ns();
         i64 a0 = c.w_arcs;
-        if (!global_relabel(c, nv, M, sinkv, blockv, s, defseeds, L, lbk, naf, nab, nd, ab, gr_depth)) return false;
+        if (!global_relabel(c, nv, M, sinkv, blockv, s, defseeds, L, lbk, naf, nab, nd, ab, gr_depth, o.gr_stop))
+            return false;
         c.tm_relabel += globaltimer_ns() - t0;
         if (c.leader) {
             u64 t1 = globaltimer_ns();
@@ -2332,7 +2386,7 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
             i64 *ab = nullptr;
             int lbk = c.take_bank();
             int depth = 0;
-            if (!global_relabel(c, nv, M, t, s, s, true, c.st.qb, lbk, naf, nab, nd, ab, depth)) return;
+            if (!global_relabel(c, nv, M, t, s, s, true, c.st.qb, lbk, naf, nab, nd, ab, depth, false)) return;
             int *hd = (int *)p.dbg;
             int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
             for (int v = gt; v < c.n; v += gT)

@@ -108,6 +108,7 @@ struct KOpts {
     int use_cache;
     int bu_factor;  // bottom-up when frontier x bu_factor > unvisited (and >= 1/64 of all)
     i64 iter_max;
+    int gr_stop;    // global relabels end once every active vertex is labelled
 };
 
 // Per-query outputs.

@@ -231,6 +231,38 @@ void or_partition(int n, int R, const i64 *so, const i64 *si, const int *dout, c
     free(vi);
 }
 
+/* The same packing with the reference's own score arithmetic: libm log and
+ * sqrt (std::log / std::sqrt, RA:1147-1151) instead of or_det_log.  Ties in
+ * the decreasing-score order are again broken by increasing id.  Used only
+ * to measure how far the deterministic log moves the partition. */
+void or_partition_libm(int n, int R, const i64 *so, const i64 *si, const int *dout, const int *din,
+                       int *part, double *score_out) {
+    or_vinfo *vi = (or_vinfo *)malloc(sizeof(or_vinfo) * (size_t)(n > 0 ? n : 1));
+    for (int x = 0; x < n; ++x) {
+        double dso = (double)so[x], dsi = (double)si[x], ddo = (double)dout[x], ddi = (double)din[x];
+        double num = log(dso * ddo + 1.0) + log(dsi * ddi + 1.0);
+        double den = log(sqrt(ddo * ddi) + 1.0);
+        vi[x].s = den > 0.0 ? num / den : 1.0;
+        vi[x].v = x;
+        if (score_out) score_out[x] = vi[x].s;
+    }
+    qsort(vi, (size_t)n, sizeof(or_vinfo), or_vinfo_cmp);
+    double *load = (double *)calloc((size_t)R, sizeof(double));
+    for (int i = 0; i < n; ++i) {
+        int best = 0;
+        double bl = load[0];
+        for (int r = 1; r < R; ++r)
+            if (load[r] < bl) {
+                bl = load[r];
+                best = r;
+            }
+        part[vi[i].v] = best;
+        load[best] += vi[i].s;
+    }
+    free(load);
+    free(vi);
+}
+
 /* Region-contiguous renumbering (RA:1193-1214) and CSR scatter with rev
  * remap (RA:1216-1259).  region_start has R+1 entries ([start,end) = entries
  * r, r+1).  Within a region vertices keep increasing old id; within a row

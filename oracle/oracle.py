@@ -35,6 +35,7 @@ _sig = {
     "or_det_log": (C.c_double, [C.c_double]),
     "or_score": (C.c_double, [C.c_longlong, C.c_longlong, C.c_int, C.c_int]),
     "or_partition": (None, [C.c_int, C.c_int, i64p, i64p, i32p, i32p, i32p, f64p]),
+    "or_partition_libm": (None, [C.c_int, C.c_int, i64p, i64p, i32p, i32p, i32p, f64p]),
     "or_reorder": (None, [C.c_int, C.c_int, i32p, i32p, i32p, i64p, i32p, i32p, i32p, i32p, i32p, i32p, i64p, i32p]),
     "or_prune_mask": (C.c_int, [C.c_int, i32p, i32p, i64p, i32p, C.c_int, C.c_int, C.c_int, u8p]),
     "or_induced_subgraph": (C.c_longlong, [C.c_int, i32p, i32p, i64p, i32p, u8p, C.POINTER(C.c_int), i32p, i32p, i32p, i32p, i64p, i32p]),
@@ -133,6 +134,16 @@ def partition(g, R):
     score = np.zeros(g.n, np.float64)
     _lib.or_partition(g.n, R, _p(so, C.c_int64), _p(si, C.c_int64), _p(do, C.c_int32), _p(di, C.c_int32),
                       _p(part, C.c_int32), _p(score, C.c_double))
+    return part, score
+
+
+def partition_libm(g, R):
+    """The partition with the reference's libm log (RA:1147-1151)."""
+    so, si, do, di = degree_stats(g)
+    part = np.zeros(g.n, np.int32)
+    score = np.zeros(g.n, np.float64)
+    _lib.or_partition_libm(g.n, R, _p(so, C.c_int64), _p(si, C.c_int64), _p(do, C.c_int32), _p(di, C.c_int32),
+                           _p(part, C.c_int32), _p(score, C.c_double))
     return part, score
 
 

@@ -233,3 +233,33 @@ def test_reference_mismatch_classifier_on_golden_logs(d):
     bad = [i for i in range(len(exp)) if ref[i] != exp[i]]
     cls = bench.classify_reference_mismatches(open(log).read(), g.n, g.arcs, bad)
     assert all(c == "stale-topology" for c in cls.values()), cls
+
+
+def test_partition_against_reference_libm_log():
+    """The engine's partition (and the oracle's restatement it is pinned to)
+    evaluates the score's logarithm with a fixed IEEE sequence so that host
+    and device agree bit for bit; the reference uses libm std::log
+    (RA:1147-1151).  The scores agree to a few ulp, and on the golden graphs
+    and R-MAT 2^14 every vertex lands in the same region under both (ties in
+    the score order broken by id in both; the reference's std::sort leaves
+    their order unspecified).  Flows do not depend on the partition: the max
+    flow is a property of the graph alone."""
+    import mscresearch_b200 as mf
+    graphs = []
+    for d in CASES:
+        g, _, _, _ = load_case(d)
+        graphs.append((os.path.basename(d), g))
+    u, v, c = mf.gen_rmat(14, 16 << 14, seed=4)
+    graphs.append(("rmat14", O.build_csr(1 << 14, u, v, c)))
+    for name, g in graphs:
+        for R in (16, 128):
+            if R > g.n:
+                continue
+            p1, s1 = O.partition(g, R)
+            p2, s2 = O.partition_libm(g, R)
+            rel = np.abs(s1 - s2) / np.maximum(1e-300, np.abs(s2))
+            assert rel.max() < 1e-14, (name, R, rel.max())
+            diff = int((p1 != p2).sum())
+            print("partition %s R=%d: %d of %d vertices in another region (max score rel. diff %.1e)"
+                  % (name, R, diff, g.n, rel.max()))
+            assert diff == 0, (name, R, diff)
