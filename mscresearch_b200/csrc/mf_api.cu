@@ -144,7 +144,10 @@ struct SlotPool {
                 return fail(MF_ERR_NOMEM, "residual slot allocation (%zu bytes) failed: %s", bytes,
                             cudaGetErrorString(e));
             }
+            // the legacy-stream clear and table upload below are waited for:
+            // the solves run on non-blocking streams that do not wait on them
             e = cudaMemset(base, 0, bytes);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(0);
             if (e != cudaSuccess) {
                 mf_dfree(base);
                 return fail(MF_ERR_CUDA, "residual slot clear failed: %s", cudaGetErrorString(e));
@@ -161,6 +164,7 @@ struct SlotPool {
             dev_cap = (int)host.size();
         }
         CK(cudaMemcpy(dev, host.data(), sizeof(DSlot) * host.size(), cudaMemcpyHostToDevice));
+        CK(cudaStreamSynchronize(0));
         return MF_OK;
     }
     void release() {
@@ -298,6 +302,19 @@ struct mf_graph {
     long launches = 0;
 };
 
+namespace {
+cudaError_t up(const mf_graph *g, void *dst, const void *src, size_t n) {
+    return n ? cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, g->stream) : cudaSuccess;
+}
+cudaError_t zero(const mf_graph *g, void *dst, size_t n) {
+    return n ? cudaMemsetAsync(dst, 0, n, g->stream) : cudaSuccess;
+}
+cudaError_t down(const mf_graph *g, void *dst, const void *src, size_t n) {
+    cudaError_t e = n ? cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, g->stream) : cudaSuccess;
+    return e == cudaSuccess ? cudaStreamSynchronize(g->stream) : e;
+}
+}  // namespace
+
 struct mf_session {
     mf_graph *g = nullptr;
     int nq = 0;
@@ -308,6 +325,15 @@ struct mf_session {
 };
 
 namespace {
+
+// Copies and clears of graph data, ordered on the graph's stream.  The
+// stream is non-blocking (it does not wait on the legacy default stream),
+// so a plain cudaMemcpy / cudaMemset -- which run on the legacy stream, the
+// former even returning before a pageable upload's DMA has landed -- would
+// not be ordered before the kernels launched on it afterwards.
+cudaError_t up(const mf_graph *g, void *dst, const void *src, size_t n);
+cudaError_t zero(const mf_graph *g, void *dst, size_t n);
+cudaError_t down(const mf_graph *g, void *dst, const void *src, size_t n);
 
 void free_kept_cache(mf_graph *g) {
     mf_dfree(g->kc_in);
@@ -373,7 +399,7 @@ DGraph make_dgraph(const mf_graph *g) {
 
 int upload_dgraph(mf_graph *g) {
     DGraph dg = make_dgraph(g);
-    CK(cudaMemcpy(g->d_graph, &dg, sizeof(DGraph), cudaMemcpyHostToDevice));
+    CK(up(g, g->d_graph, &dg, sizeof(DGraph)));
     return MF_OK;
 }
 
@@ -407,9 +433,9 @@ int partition_into(mf_graph *g, int R, int *row, int *col, i64 *cap, int *rev, u
     CK(cudaStreamSynchronize(g->stream));
     std::vector<int> nid(n), sc_part(n);
     std::vector<double> sc(n);
-    CK(cudaMemcpy(nid.data(), out.new_id, sizeof(int) * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(sc.data(), out.score, sizeof(double) * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(sc_part.data(), out.part, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(down(g, nid.data(), out.new_id, sizeof(int) * n));
+    CK(down(g, sc.data(), out.score, sizeof(double) * n));
+    CK(down(g, sc_part.data(), out.part, sizeof(int) * n));
     // compose: caller -> input index -> internal
     std::vector<int> new_id(n), old_id(n);
     g->score_caller.assign(n, 0.0);
@@ -443,7 +469,7 @@ int finalize_graph(mf_graph *g) {
     int best = 0;
     {
         std::vector<int> rw(n + 1), hl, gl;
-        CK(cudaMemcpy(rw.data(), g->row, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+        CK(down(g, rw.data(), g->row, sizeof(int) * (n + 1)));
         for (int x = 1; x < n; ++x)
             if (rw[x + 1] - rw[x] > rw[best + 1] - rw[best]) best = x;
         g->deg_host.resize(n);
@@ -455,12 +481,12 @@ int finalize_graph(mf_graph *g) {
         g->nhub = (int)hl.size();
         if (!hl.empty()) {
             CK(mf_dmalloc(&g->hubs, sizeof(int) * hl.size()));
-            CK(cudaMemcpy(g->hubs, hl.data(), sizeof(int) * hl.size(), cudaMemcpyHostToDevice));
+            CK(up(g, g->hubs, hl.data(), sizeof(int) * hl.size()));
         }
         g->ngiant = (int)gl.size();
         if (!gl.empty()) {
             CK(mf_dmalloc(&g->giants, sizeof(int) * gl.size()));
-            CK(cudaMemcpy(g->giants, gl.data(), sizeof(int) * gl.size(), cudaMemcpyHostToDevice));
+            CK(up(g, g->giants, gl.data(), sizeof(int) * gl.size()));
         }
     }
     g->pivot = best;
@@ -646,7 +672,7 @@ int launch(mf_graph *g, SlotPool &pool, int nq, const int *s_int, const int *t_i
     // clock housekeeping: reset slots whose stamp clock passed 2^30
     if ((g->launches & 15) == 0) {
         std::vector<unsigned> clk(ns);
-        CK(cudaMemcpy(clk.data(), g->d_clocks, sizeof(unsigned) * ns, cudaMemcpyDeviceToHost));
+        CK(down(g, clk.data(), g->d_clocks, sizeof(unsigned) * ns));
         for (int i = 0; i < ns; ++i)
             if (clk[i] > (1u << 30)) k_reset_slot<<<256, 256, 0, g->stream>>>(pool.host[i], pool.n);
         CK(cudaStreamSynchronize(g->stream));
@@ -936,6 +962,8 @@ int mf_graph_create_from_edges(int n, long long m, const int32_t *u, const int32
                          cudaMemcpy(dv, v, sizeof(int) * m, cudaMemcpyHostToDevice) != cudaSuccess ||
                          cudaMemcpy(dc, cap, sizeof(i64) * m, cudaMemcpyHostToDevice) != cudaSuccess)) {
         rc = fail(MF_ERR_CUDA, "edge upload failed");
+    } else if (cudaStreamSynchronize(0) != cudaSuccess) {  // the uploads' DMA has landed
+        rc = fail(MF_ERR_CUDA, "edge upload failed");
     } else {
         rc = graph_from_device_edges(n, m, du, dv, dc, R, out);
     }
@@ -1078,12 +1106,12 @@ int mf_graph_info(const mf_graph *g, int *n, long long *arcs, int *R) {
 int mf_graph_export(const mf_graph *g, int32_t *row, int32_t *col, int64_t *cap, int32_t *rev,
                     int32_t *new_id, int32_t *region_start, double *score, int32_t *part) {
     if (!g) return fail(MF_ERR_ARG, "graph is NULL");
-    if (row) CK(cudaMemcpy(row, g->row, sizeof(int) * ((size_t)g->n + 1), cudaMemcpyDeviceToHost));
-    if (col && g->arcs) CK(cudaMemcpy(col, g->col, sizeof(int) * g->arcs, cudaMemcpyDeviceToHost));
-    if (cap && g->arcs) CK(cudaMemcpy(cap, g->cap, sizeof(i64) * g->arcs, cudaMemcpyDeviceToHost));
-    if (rev && g->arcs) CK(cudaMemcpy(rev, g->rev, sizeof(int) * g->arcs, cudaMemcpyDeviceToHost));
+    if (row) CK(down(g, row, g->row, sizeof(int) * ((size_t)g->n + 1)));
+    if (col && g->arcs) CK(down(g, col, g->col, sizeof(int) * g->arcs));
+    if (cap && g->arcs) CK(down(g, cap, g->cap, sizeof(i64) * g->arcs));
+    if (rev && g->arcs) CK(down(g, rev, g->rev, sizeof(int) * g->arcs));
     if (region_start)
-        CK(cudaMemcpy(region_start, g->region_start, sizeof(int) * ((size_t)g->R + 1), cudaMemcpyDeviceToHost));
+        CK(down(g, region_start, g->region_start, sizeof(int) * ((size_t)g->R + 1)));
     if (new_id) memcpy(new_id, g->new_id.data(), sizeof(int) * g->n);
     if (score) memcpy(score, g->score_caller.data(), sizeof(double) * g->n);
     if (part) memcpy(part, g->part_caller.data(), sizeof(int) * g->n);
@@ -1189,14 +1217,14 @@ static int build_kept_cache(mf_graph *g, const mf_opts &o) {
     CK(mf_dmalloc(&g->kc_in, n));
     CK(mf_dmalloc(&g->kc_img, sizeof(int) * (size_t)n));
     CK(mf_dmalloc(&g->kc_res, sizeof(i64) * (size_t)std::max<i64>(g->arcs, 1)));
-    CK(cudaMemset(g->kc_in, 0, n));
+    CK(zero(g, g->kc_in, n));
     CK(mf_dmalloc(&g->kc_fb, n));
     ko.img = g->kc_img;
     ko.in = g->kc_in;
     ko.fb = g->kc_fb;
     KcOut *dko = nullptr;
     CK(mf_dmalloc(&dko, sizeof(KcOut)));
-    if (cudaMemcpy(dko, &ko, sizeof(KcOut), cudaMemcpyHostToDevice) != cudaSuccess) {
+    if (up(g, dko, &ko, sizeof(KcOut)) != cudaSuccess) {
         mf_dfree(dko);
         return fail(MF_ERR_CUDA, "kept-set cache set-up copy failed");
     }
@@ -1210,7 +1238,7 @@ static int build_kept_cache(mf_graph *g, const mf_opts &o) {
     unsigned long long *darcs = nullptr;
     DevScope tmp;
     CK(tmp.alloc(&darcs, sizeof(unsigned long long)));
-    CK(cudaMemset(darcs, 0, sizeof(unsigned long long)));
+    CK(zero(g, darcs, sizeof(unsigned long long)));
     k_kept_res<<<g->dev.sms * 8, 256, 0, g->stream>>>(n, g->row, g->col, g->cap, g->kc_in, g->kc_res, darcs);
     unsigned long long ka = 0;
     CK(cudaMemcpyAsync(&ka, darcs, sizeof(ka), cudaMemcpyDeviceToHost, g->stream));
@@ -1219,7 +1247,7 @@ static int build_kept_cache(mf_graph *g, const mf_opts &o) {
     g->kc_valid = out.mask_n >= 2;
     if (g->kc_valid) {
         g->kc_in_host.resize(n);
-        CK(cudaMemcpy(g->kc_in_host.data(), g->kc_in, n, cudaMemcpyDeviceToHost));
+        CK(down(g, g->kc_in_host.data(), g->kc_in, n));
     }
     if (!g->kc_valid) {
         bool tried = true;
@@ -1349,10 +1377,9 @@ int mf_solve_batch_override(mf_graph *g, int nq, const int32_t *s, const int32_t
             rc = fail(MF_ERR_NOMEM, "override buffers (%zu capacities) do not fit", ovn);
             break;
         }
-        if (cudaMemcpy(du, iu.data(), sizeof(int) * nb, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(dv, iv.data(), sizeof(int) * nb, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(dov, caps, sizeof(i64) * ovn, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemset(dbad, 0, sizeof(int)) != cudaSuccess) {
+        if (up(g, du, iu.data(), sizeof(int) * nb) != cudaSuccess ||
+            up(g, dv, iv.data(), sizeof(int) * nb) != cudaSuccess ||
+            up(g, dov, caps, sizeof(i64) * ovn) != cudaSuccess || zero(g, dbad, sizeof(int)) != cudaSuccess) {
             rc = fail(MF_ERR_CUDA, "override upload failed");
             break;
         }
@@ -1407,15 +1434,15 @@ int mf_graph_save(const mf_graph *g, const char *path) {
     std::vector<int> row(n + 1), col(A), rev(A), rs(R + 1), ro(n);
     std::vector<i64> cap(A);
     std::vector<unsigned char> fwd(A);
-    CK(cudaMemcpy(row.data(), g->row, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+    CK(down(g, row.data(), g->row, sizeof(int) * (n + 1)));
     if (A) {
-        CK(cudaMemcpy(col.data(), g->col, sizeof(int) * A, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(cap.data(), g->cap, sizeof(i64) * A, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(rev.data(), g->rev, sizeof(int) * A, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(fwd.data(), g->fwd, A, cudaMemcpyDeviceToHost));
+        CK(down(g, col.data(), g->col, sizeof(int) * A));
+        CK(down(g, cap.data(), g->cap, sizeof(i64) * A));
+        CK(down(g, rev.data(), g->rev, sizeof(int) * A));
+        CK(down(g, fwd.data(), g->fwd, A));
     }
-    CK(cudaMemcpy(rs.data(), g->region_start, sizeof(int) * (R + 1), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(ro.data(), g->region_of, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(down(g, rs.data(), g->region_start, sizeof(int) * (R + 1)));
+    CK(down(g, ro.data(), g->region_of, sizeof(int) * n));
     CacheHead h{};
     memcpy(h.magic, kCacheMagic, 8);
     h.version = 1;
@@ -1511,9 +1538,9 @@ int mf_graph_load_binary(const char *path, mf_graph **out) {
         for (int r = 0; r < R && rc == MF_OK; ++r)
             if (rs[r] > rs[r + 1]) rc = fail(MF_ERR_IO, "%s: region starts decrease at %d", path, r);
         if (rc) break;
-        if (cudaMemcpy(g->row, row.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(g->region_start, rs.data(), sizeof(int) * (R + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemset(dbad, 0, sizeof(int)) != cudaSuccess) {
+        if (up(g, g->row, row.data(), sizeof(int) * (n + 1)) != cudaSuccess ||
+            up(g, g->region_start, rs.data(), sizeof(int) * (R + 1)) != cudaSuccess ||
+            zero(g, dbad, sizeof(int)) != cudaSuccess) {
             rc = fail(MF_ERR_CUDA, "graph upload failed");
             break;
         }
@@ -1556,13 +1583,13 @@ int mf_debug_prune_mask(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, 
     if (!g || !mask) return fail(MF_ERR_ARG, "bad arguments");
     unsigned char *d = nullptr;
     CK(mf_dmalloc(&d, g->n));
-    CK(cudaMemset(d, 0, g->n));
+    CK(zero(g, d, g->n));
     int64_t f = 0;
     mf_stats st;
     int rc = solve_common(g, 1, &s, &t, opts, &f, &st, KM_PRUNE, d, true);
     if (rc == MF_OK) {
         std::vector<unsigned char> h(g->n);
-        cudaMemcpy(h.data(), d, g->n, cudaMemcpyDeviceToHost);
+        down(g, h.data(), d, g->n);
         int k = 0;
         for (int x = 0; x < g->n; ++x) {
             mask[x] = (s < 0 || t < 0 || s >= g->n || t >= g->n) ? 0 : h[g->new_id[x]];
@@ -1583,7 +1610,7 @@ int mf_debug_initial_heights(mf_graph *g, int32_t s, int32_t t, const mf_opts *o
     int rc = solve_common(g, 1, &s, &t, opts, &f, &st, KM_HEIGHTS, d, true);
     if (rc == MF_OK) {
         std::vector<int> h(g->n);
-        cudaMemcpy(h.data(), d, sizeof(int) * g->n, cudaMemcpyDeviceToHost);
+        down(g, h.data(), d, sizeof(int) * g->n);
         for (int x = 0; x < g->n; ++x) heights[x] = h[g->new_id[x]];
     }
     mf_dfree(d);
@@ -1598,7 +1625,7 @@ int mf_solve_residual(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, in
     int64_t f = 0;
     mf_stats st;
     int rc = solve_common(g, 1, &s, &t, opts, &f, stats ? stats : &st, KM_RESIDUAL, d, true);
-    if (rc == MF_OK && g->arcs) cudaMemcpy(res, d, sizeof(i64) * g->arcs, cudaMemcpyDeviceToHost);
+    if (rc == MF_OK && g->arcs) down(g, res, d, sizeof(i64) * g->arcs);
     if (flow) *flow = f;
     mf_dfree(d);
     return rc;
@@ -1629,8 +1656,8 @@ static int resolve_updates(mf_graph *g, int nb, const int32_t *u, const int32_t 
     CK(tmp.alloc(&dv, sizeof(int) * nb));
     CK(tmp.alloc(&darc, sizeof(int) * nb));
     CK(tmp.alloc(&dcap, sizeof(i64) * nb));
-    CK(cudaMemcpy(du, ui.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(dv, vi.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
+    CK(up(g, du, ui.data(), sizeof(int) * nb));
+    CK(up(g, dv, vi.data(), sizeof(int) * nb));
     k_find_arcs<<<(unsigned)((nb + 7) / 8), 256, 0, g->stream>>>(nb, du, dv, g->row, g->col, g->rev, g->fwd, g->cap, darc, dcap);
     std::vector<int> arc(nb);
     std::vector<i64> capv(nb);
@@ -1674,7 +1701,7 @@ static int apply_updates(mf_graph *g, const std::vector<ArcUpdate> &ups, ArcUpda
     }
     ArcUpdate *d = nullptr;
     CK(mf_dmalloc(&d, sizeof(ArcUpdate) * ups.size()));
-    CK(cudaMemcpy(d, ups.data(), sizeof(ArcUpdate) * ups.size(), cudaMemcpyHostToDevice));
+    CK(up(g, d, ups.data(), sizeof(ArcUpdate) * ups.size()));
     k_apply_caps<<<((int)ups.size() + 255) / 256, 256, 0, g->stream>>>((int)ups.size(), d, g->cap);
     CK(cudaStreamSynchronize(g->stream));
     *d_out = d;
@@ -2065,7 +2092,7 @@ int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int ma
     if (cudaMemcpy(sv->d_graphs, dg.data(), sizeof(DGraph) * ngraphs, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(sv->d_gstate, 0, sizeof(GState) * ngraphs) != cudaSuccess ||
         cudaMemset(sv->d_srv, 0, sizeof(SrvCtl)) != cudaSuccess ||
-        cudaMemset(sv->d_err, 0, sizeof(int)) != cudaSuccess ||
+        cudaMemset(sv->d_err, 0, sizeof(int)) != cudaSuccess || cudaStreamSynchronize(0) != cudaSuccess ||
         cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&sv->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&sv->done_ev, cudaEventDisableTiming) != cudaSuccess)
