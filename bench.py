@@ -386,12 +386,13 @@ def run_mix(args):
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     import mscresearch_b200 as mf
     rng = np.random.default_rng(1234)
-    graphs, sizes = [], []
+    graphs, sizes, edges = [], [], []
     for k, sc in enumerate(MIX_SCALES):
         n = 1 << sc
         u, v, c = mf.gen_rmat(sc, 16 * n, seed=100 + k)
         graphs.append(mf.Graph.from_edges(n, u, v, c, R=min(128, n)))
         sizes.append(n)
+        edges.append((u, v, c))
     ranks = rng.permutation(len(graphs))
     w = 1.0 / np.arange(1, len(graphs) + 1) ** 1.1
     p_graph = np.zeros(len(graphs))
@@ -441,6 +442,65 @@ def run_mix(args):
         sv.close()
         runs.append({"arrival_rate_qps": round(rate, 1), "qps": round(nreq / wall, 2),
                      "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "slots": slots, "exact": exact})
+    # served with capacity updates: ~10% of the requests are update batches
+    # (256 changes of +-U[1,100] on random edges of the request's graph),
+    # the rest queries, at twice the plain loop's rate.  Every answer is
+    # checked against an in-order replay on a second copy of the graphs
+    # (mf_update_caps then mf_solve, in submission order).
+    upd_run = None
+    if args.mix_update_share > 0:
+        rate = 2.0 * plain_qps
+        kinds = rng.random(nreq) < args.mix_update_share
+        batches = {}
+        for k in np.nonzero(kinds)[0]:
+            u, v, c = edges[gi[k]]
+            idx = rng.integers(0, len(u), 256)
+            d = rng.integers(1, 101, 256) * np.where(rng.random(256) < 0.5, -1, 1)
+            batches[k] = (u[idx], v[idx], d)
+        sv = mf.Server(graphs, o)
+        gaps = rng.exponential(1.0 / rate, nreq)
+        sub_t, tickets, done_t = [], [], {}
+        t0 = time.perf_counter()
+        nxt = t0
+        for k in range(nreq):
+            nxt += gaps[k]
+            while time.perf_counter() < nxt:
+                for tk in tickets:
+                    if tk not in done_t and sv.poll(tk)[0]:
+                        done_t[tk] = time.perf_counter()
+            sub_t.append(time.perf_counter())
+            if kinds[k]:
+                tickets.append(sv.update(int(gi[k]), *batches[k]))
+            else:
+                tickets.append(sv.submit(int(gi[k]), int(qs[k]), int(qt[k])))
+        while len(done_t) < nreq:
+            for tk in tickets:
+                if tk not in done_t and sv.poll(tk)[0]:
+                    done_t[tk] = time.perf_counter()
+        wall = time.perf_counter() - t0
+        served_f = [sv.poll(tk)[1] for tk in tickets]
+        slots = sv.slots
+        sv.close()
+        # replay
+        replay = []
+        for k, (u, v, c) in enumerate(edges):
+            replay.append(mf.Graph.from_edges(sizes[k], u, v, c, R=min(128, sizes[k])))
+        exact = True
+        for k in range(nreq):
+            if kinds[k]:
+                replay[gi[k]].update_caps(*batches[k])
+            elif replay[gi[k]].solve(int(qs[k]), int(qt[k]))[0] != served_f[k]:
+                exact = False
+        for g in replay:
+            g.close()
+        qlat = [(done_t[tk] - sub_t[i]) * 1e3 for i, tk in enumerate(tickets) if not kinds[i]]
+        ulat = [(done_t[tk] - sub_t[i]) * 1e3 for i, tk in enumerate(tickets) if kinds[i]]
+        upd_run = {"arrival_rate_rps": round(rate, 1), "requests": nreq, "update_batches": int(kinds.sum()),
+                   "changes_per_batch": 256, "rps": round(nreq / wall, 2),
+                   "query_p50_ms": pct(qlat, 50), "query_p99_ms": pct(qlat, 99),
+                   "update_p50_ms": pct(ulat, 50), "update_p99_ms": pct(ulat, 99), "slots": slots,
+                   "exact": exact}
+        assert exact, "served answers with updates differ from the in-order replay"
     best = max(runs, key=lambda r: r["qps"])
     res = {"metric": "exact max-flow queries/sec + p50/p99 latency, serving mix vs plain loop",
            "value": best["qps"], "unit": "queries/s", "n_gpus": 1, "higher_is_better": True,
@@ -451,6 +511,8 @@ def run_mix(args):
                       "group_ctas": o.group_ctas},
            "plain": {"qps": round(plain_qps, 2), "p50_ms": pct(plain_ms, 50), "p99_ms": pct(plain_ms, 99)},
            "served": runs}
+    if upd_run:
+        res["served_with_updates"] = upd_run
     for g in graphs:
         g.close()
     if rank == 0:
@@ -762,6 +824,8 @@ def main():
     ap.add_argument("--grid-w", type=int, default=2048)
     ap.add_argument("--grid-sets", type=int, default=64)
     ap.add_argument("--mix-requests", type=int, default=512)
+    ap.add_argument("--mix-update-share", type=float, default=0.1,
+                    help="mix: share of requests that are capacity-update batches in the extra served run")
     ap.add_argument("--mix-rates", type=float, nargs="+", default=[0.5, 1.0, 2.0, 4.0],
                     help="arrival rates as multiples of the plain loop's throughput")
     args = ap.parse_args()

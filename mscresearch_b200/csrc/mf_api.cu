@@ -20,6 +20,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <condition_variable>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -1892,6 +1893,16 @@ struct mf_server {
     cudaEvent_t done_ev = nullptr;
     bool running = false;
     bool launched = false;  // a launch has happened (its error word is meaningful)
+    // slot admission runs on its own host thread, so a submit never waits
+    // for an allocation: the submitting thread raises `want` (slots the open
+    // requests could use) and the admission thread allocates up to it
+    int device = 0;
+    std::atomic<int> nslots_pub{0};  // slots published (mf_server_slots)
+    std::atomic<long long> want{0};
+    std::atomic<bool> admit_stop{false};
+    std::mutex admit_mu;
+    std::condition_variable admit_cv;
+    std::thread admit_thr;
 };
 
 static bool server_alive(mf_server *sv) {
@@ -1903,7 +1914,7 @@ static bool server_alive(mf_server *sv) {
 }
 
 static int server_launch(mf_server *sv) {
-    if (sv->nslots < 1) return fail(MF_ERR_NOMEM, "server: no residual slot admitted");
+    if (sv->nslots_pub.load() < 1) return fail(MF_ERR_NOMEM, "server: no residual slot admitted");
     CK(cudaMemsetAsync(sv->d_gctl, 0, sizeof(GroupCtl) * sv->ngroups, sv->stream));
     CK(cudaMemsetAsync(&sv->d_srv->live, 0, sizeof(int), sv->stream));
     CK(cudaMemsetAsync(sv->d_err, 0, sizeof(int), sv->stream));
@@ -1971,12 +1982,12 @@ static void server_advance(mf_server *sv) {
     if (sv->upd_live.empty()) sv->upd_lo = sv->upd_hi = 0;  // no batch in use: restart at 0
 }
 
-// Admission of residual slots by free HBM: while more requests are open
-// than slots exist, allocate another slot if it fits.
-static void server_admit_slots(mf_server *sv) {
-    server_advance(sv);
-    const long long open = sv->submitted - sv->first_open;
-    while (sv->nslots < sv->max_slots && open > sv->nslots) {
+// Admission of residual slots by free HBM: allocate slots (each only if
+// cudaMemGetInfo shows room for it under the 85 % rule) until `want` are
+// admitted; returns the slots admitted.  Runs on the admission thread (or
+// at creation, before that thread exists).
+static int server_grow_slots(mf_server *sv, long long want) {
+    while (sv->nslots < sv->max_slots && want > sv->nslots) {
         size_t fr = 0, tot = 0;
         if (cudaMemGetInfo(&fr, &tot) != cudaSuccess || (double)fr * 0.85 < (double)sv->slot_size) break;
         void *m = nullptr;
@@ -1991,6 +2002,41 @@ static void server_admit_slots(mf_server *sv) {
         std::atomic_thread_fence(std::memory_order_seq_cst);
         *(volatile int *)&sv->h_slot_ready[sv->nslots] = 1;  // the group clears it before use
         ++sv->nslots;
+        sv->nslots_pub.store(sv->nslots);
+    }
+    return sv->nslots;
+}
+
+static void server_admit_loop(mf_server *sv) {
+    cudaSetDevice(sv->device);
+    std::unique_lock<std::mutex> lk(sv->admit_mu);
+    for (;;) {
+        sv->admit_cv.wait(lk, [&] { return sv->admit_stop.load() || sv->want.load() > sv->nslots_pub.load(); });
+        if (sv->admit_stop.load()) return;
+        const long long want = sv->want.load();
+        lk.unlock();
+        const int before = sv->nslots;
+        server_grow_slots(sv, want);
+        lk.lock();
+        // no room (or the cap): wait for a larger want rather than retrying
+        if (sv->nslots == before && !sv->admit_stop.load()) {
+            sv->admit_cv.wait_for(lk, std::chrono::milliseconds(20));
+            if (sv->want.load() <= want) sv->want.store(sv->nslots);
+        }
+    }
+}
+
+// Called on every submit: more requests are open than slots exist -> ask
+// the admission thread for more.
+static void server_admit_slots(mf_server *sv) {
+    server_advance(sv);
+    const long long open = std::min<long long>(sv->submitted - sv->first_open, sv->max_slots);
+    if (open > sv->nslots_pub.load() && open > sv->want.load()) {
+        {
+            std::lock_guard<std::mutex> lk(sv->admit_mu);
+            sv->want.store(open);
+        }
+        sv->admit_cv.notify_one();
     }
 }
 
@@ -2098,23 +2144,21 @@ int mf_server_create(mf_graph **graphs, int ngraphs, const mf_opts *opts, int ma
         cudaEventCreateWithFlags(&sv->done_ev, cudaEventDisableTiming) != cudaSuccess)
         return bail(MF_ERR_CUDA, "device set-up failed");
     // the first slots (more are admitted as requests open up)
-    const long long want = std::min(SRV_INITIAL_SLOTS, sv->max_slots);
-    sv->submitted = want;  // admit as if `want` requests were open
-    sv->first_open = 0;
-    server_admit_slots(sv);
-    sv->submitted = 0;
-    sv->first_open = 0;
+    cudaGetDevice(&sv->device);
+    server_grow_slots(sv, std::min(SRV_INITIAL_SLOTS, sv->max_slots));
     if (sv->nslots < 1) {
         mf_server_destroy(sv);
         return fail(MF_ERR_NOMEM, "admission: no HBM for one residual slot (%zu bytes)", sv->slot_size);
     }
+    sv->want.store(sv->nslots);
+    sv->admit_thr = std::thread(server_admit_loop, sv);
     *out = sv;
     return MF_OK;
 }
 
 int mf_server_slots(const mf_server *sv, int *slots) {
     if (!sv || !slots) return fail(MF_ERR_ARG, "bad arguments");
-    *slots = sv->nslots;
+    *slots = sv->nslots_pub.load();
     return MF_OK;
 }
 
@@ -2244,6 +2288,14 @@ int mf_server_drain(mf_server *sv) {
 
 int mf_server_destroy(mf_server *sv) {
     if (!sv) return MF_OK;
+    if (sv->admit_thr.joinable()) {
+        {
+            std::lock_guard<std::mutex> lk(sv->admit_mu);
+            sv->admit_stop.store(true);
+        }
+        sv->admit_cv.notify_one();
+        sv->admit_thr.join();
+    }
     if (sv->h_stop) *(volatile int *)sv->h_stop = 1;
     std::atomic_thread_fence(std::memory_order_seq_cst);
     if (sv->stream) cudaStreamSynchronize(sv->stream);
