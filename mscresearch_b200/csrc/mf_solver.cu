@@ -460,7 +460,7 @@ static_assert(CNT_SOLO >= CNT_BACK + NBANKS && CNT_SOLO > CNT_HUBCH && CNT_SOLO 
 template <class Claim, class UF, class UB, class Par, class Set, class Hook = NoLevelHook>
 __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, int nuf, UF uf, int nub,
                         UB ub, Par par, Set set, Hook on_level = Hook{}, int *levels_out = nullptr,
-                        int stop_at = -1) {
+                        int stop_at = -1, bool *stopped_out = nullptr) {
     // stop_at >= 0: the search ends after the first level by which the
     // control word cnt[CNT_FOUND] (raised by cl / set) has reached stop_at
     int flo = 0, blo = 0, pflo = 0, pblo = 0, level = 0, nbu = 0, nsolo = 0;
@@ -553,6 +553,7 @@ __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, i
         ++level;
     }
     if (levels_out) *levels_out = level;
+    if (stopped_out) *stopped_out = stopped;
     if (c.leader) {
         i64 *tot = c.st.acc + ACC_TOT;
         tot[T_LEVELS] += level;
@@ -1010,7 +1011,8 @@ __device__ bool preflow(QCtx &c, int s) {
 // (atomicOr on the visited word).  Bottom-up: an unvisited kept vertex w
 // takes level + 1 when one of its residual arcs reaches the frontier map.
 // Claims write the height and the next frontier bit.
-__device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &depth, int stop_at) {
+__device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &depth, int stop_at,
+                            bool &stopped) {
     const int W = bitmap_words(c.n);
     unsigned *vis = c.st.bits + W, *F = c.st.bits + 2 * W;
     const int *rev = c.rev;
@@ -1073,7 +1075,7 @@ __device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &de
         }
     };
     return bfs_dir(c, c.st.qa, bank, fhi, bhi, relab, c.vf, uf, nv - c.vf, ub, par, set, clear_prev, &depth,
-                   stop_at);
+                   stop_at, &stopped);
 }
 
 // Kept-vertex bitmap of the query (bit v: mark[v] >= M), read by every
@@ -1097,9 +1099,21 @@ __device__ bool build_kept_bits(QCtx &c, unsigned M) {
 // keep height n, and the active list (excess > 0, height < n, not
 // the phase sink or blocked vertex) is compacted into L (front / back).
 // Returns counts in naf / nab (active front / back) and nd (deficits).
+// Dead vertices (height n + 1).  In phase A, a vertex that a complete
+// search did not reach cannot reach the sink again: every vertex it can
+// reach was unreached too, so sits at height >= n, where no push can enter
+// it (a push needs a vertex one level higher) and RM leaves it alone; its
+// residual reach therefore never grows.  keep_dead: dead marks from earlier
+// relabels of this phase stand (else every kept vertex starts at n);
+// mark_dead: the previous relabel's search was complete and its visited
+// bitmap is intact, so the kept vertices it left unvisited become dead.
+// Dead vertices are pre-marked visited (no search touches them) and are not
+// counted among the active vertices an early stop waits for.  complete
+// (out): this search was not stopped early.
 __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int blockv, int srcv,
                                bool deficit_seeds, int *L, int lbk, int &naf, int &nab, int &nd,
-                               i64 *&ab, int &depth, bool early_stop) {
+                               i64 *&ab, int &depth, bool early_stop, bool keep_dead = false,
+                               bool mark_dead = false, bool *complete = nullptr) {
     MF_TRACE(40, nv);
     int qbk = c.take_bank();
     const int n = c.n;
@@ -1109,12 +1123,16 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
     {
         int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
         for (int wd = gt; wd < W; wd += gT) {
-            unsigned x = ~ldcg(&kept[wd]);
+            const unsigned kw = ldcg(&kept[wd]);
+            unsigned x = ~kw;
             if (blockv >= 0 && wd == (blockv >> 5)) x |= 1u << (blockv & 31);
+            // the third frontier map (first written at level 1) carries the
+            // kept vertices the previous complete search left unvisited to
+            // the seeds pass below
+            F0[2 * W + wd] = mark_dead ? (kw & ~ldcg(&vis[wd])) : 0u;
             vis[wd] = x;
             F0[wd] = 0;
             F0[W + wd] = 0;
-            F0[2 * W + wd] = 0;
         }
         if (c.leader) {
             c.st.cnt[CNT_ACT] = 0;
@@ -1135,13 +1153,18 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
             const i64 ev = ldcg(&c.st.ex[v]);
             if (v == sinkv) seed = true;
             else if (deficit_seeds && v != blockv && v != srcv && ev < 0) seed = true;
-            act = !seed && v != blockv && ev > 0;
+            bool dead = false;
+            if (keep_dead && !seed && v != blockv)
+                dead = ldcg(&c.st.h[v]) > n || (mark_dead && ((ldcg(&F0[2 * W + (v >> 5)]) >> (v & 31)) & 1u));
+            act = !seed && !dead && v != blockv && ev > 0;
             if (seed) {
                 atomicOr(&vis[v >> 5], 1u << (v & 31));
                 atomicOr(&F0[v >> 5], 1u << (v & 31));
+            } else if (dead) {
+                atomicOr(&vis[v >> 5], 1u << (v & 31));
             }
-            // every kept vertex starts the search at height n (unreached)
-            c.st.h[v] = seed ? 0 : n;
+            // every other kept vertex starts the search at height n (unreached)
+            c.st.h[v] = seed ? 0 : (dead ? n + 1 : n);
         }
         nact += __popc(__ballot_sync(MF_FULL, act));
         append2(c, seed, v, c.st.qa, qbk);
@@ -1149,6 +1172,13 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
     if (early_stop && c.lane == 0 && nact) atomicAdd(&c.st.cnt[CNT_ACT], nact);
     int f0 = 0, b0 = 0;
     if (!c.sync_tails(qbk, f0, b0)) return false;
+    if (mark_dead) {
+        // the third frontier map is written from level 1 on (a solo episode
+        // may reach it without a group barrier): clear it and wait
+        int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+        for (int wd = gt; wd < W; wd += gT) F0[2 * W + wd] = 0;
+        if (!c.sync()) return false;
+    }
     MF_TRACE(43, f0 + b0);
     // Early stop: once every active vertex holds its exact height the
     // search ends; vertices it did not reach keep height n, which no push
@@ -1156,7 +1186,9 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
     // relabel.  A search that cannot reach some active vertex runs to the
     // end as before, so the relabel that ends a phase stays exact.
     const int stop_at = early_stop ? ldcg(&c.st.cnt[CNT_ACT]) : -1;
-    if (!relabel_bfs(c, nv, qbk, f0, b0, depth, stop_at)) return false;
+    bool stopped = false;
+    if (!relabel_bfs(c, nv, qbk, f0, b0, depth, stop_at, stopped)) return false;
+    if (complete) *complete = !stopped;
     int *h = c.st.h;
 
     // Active list in decreasing height: the search queue (every reached
@@ -1798,6 +1830,10 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
     i64 round = 0;
     i64 mask_arcs = ldcg(&c.st.acc[ACC_TOT + T_MASKARCS]);
     int gr_depth = 0;  // levels of the last global relabel's search
+    // dead marks (see global_relabel): phase A only, from the second relabel
+    // of the phase on; new ones only after a complete search
+    int dead_phase = -1;      // phase of the last relabel (-1: none in this call)
+    bool last_complete = false;
     for (;;) {
         int sinkv = (phase == PH_A) ? t : (phase == PH_B ? -1 : s);
         int blockv = (phase == PH_C) ? t : s;
@@ -1808,8 +1844,11 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
         int lbk = c.take_bank();
         u64 t0 = globaltimer_ns();
         i64 a0 = c.w_arcs;
-        if (!global_relabel(c, nv, M, sinkv, blockv, s, defseeds, L, lbk, naf, nab, nd, ab, gr_depth, o.gr_stop))
+        const bool keep_dead = o.gr_stop && phase == PH_A && dead_phase == PH_A;
+        if (!global_relabel(c, nv, M, sinkv, blockv, s, defseeds, L, lbk, naf, nab, nd, ab, gr_depth, o.gr_stop,
+                            keep_dead, keep_dead && last_complete, &last_complete))
             return false;
+        dead_phase = phase;
         c.tm_relabel += globaltimer_ns() - t0;
         if (c.leader) {
             u64 t1 = globaltimer_ns();
@@ -2113,6 +2152,8 @@ __device__ bool write_full_residual(QCtx &c, unsigned M, i64 *out) {
 // 4. each updated arc inside the kept set adjusts its residual, cancelling
 // flow above the new capacity (tail gains excess, head loses it); 5. s
 // re-saturates.
+__device__ bool repair_deltas(QCtx &c, const KParams &p, unsigned Mn, unsigned O);
+
 __device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int &nv, bool &t_reach) {
     int *meta = c.st.meta;
     int vf_old = ldcg(&meta[4]);
@@ -2127,6 +2168,29 @@ __device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int
     unsigned *mark = c.st.mark, *claim = c.st.claim;
     const i64 *cap = c.cap;
     const int *rev = c.rev;
+    // The kept set fwd(s) & bwd(t) follows arcs with capacity > 0, so it can
+    // only grow through an arc whose capacity went from 0 to positive.  With
+    // no such update the old kept set is a superset of the new one, which
+    // gives the same maximum flow (every s-t path lies inside the new set):
+    // it is kept as it is and both searches are skipped.
+    int gt0 = c.crank * blockDim.x + threadIdx.x, gT0 = c.G * blockDim.x;
+    if (c.leader) c.st.cnt[CNT_FLAG] = 0;
+    if (!c.sync()) return false;
+    for (int i = gt0; i < p.nupd; i += gT0)
+        if (p.upd[i].old_cap <= 0 && p.upd[i].new_cap > 0) atomicOr(&c.st.cnt[CNT_FLAG], 1);
+    if (!c.sync()) return false;
+    const bool grows = ldcg(&c.st.cnt[CNT_FLAG]) != 0;
+    if (!grows) {
+        for (int i = gt0; i < nv_old; i += gT0) mark[c.vat(i)] = Mn;
+        t_reach = ldcg(&meta[5]) != 0;
+        nv = nv_old;
+        if (c.leader) c.st.acc[ACC_TOT + T_MASKARCS] = ldcg(&meta[6]);
+        if (!c.sync()) return false;
+        if (!repair_deltas(c, p, Mn, O)) return false;
+        M = Mn;
+        if (!t_reach) return true;
+        return preflow(c, s);
+    }
     // the kept set under the new capacities, fwd(s) & bwd(t), by two
     // direction-optimizing searches (a top-down-only pair examined every
     // arc of fwd(s) twice: ~270 M arcs for a hub query on R-MAT 2^22)
@@ -2221,9 +2285,22 @@ __device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int
     for_giants(
         c, [&](int v) { return ldcg(&mark[v]) == Mn && ldcg(&claim[v]) != O; }, [&](int, int, int) {},
         [&](int, int e) { open_arc(e); });
+    if (c.leader) atomic_add_i64(&c.st.acc[ACC_TOT + T_MASKARCS], ldcg(&meta[6]));
     if (c.lane == 0 && add_arcs) atomic_add_i64(&c.st.acc[ACC_TOT + T_MASKARCS], add_arcs);
     if (!c.sync()) return false;
-    // capacity deltas on kept arcs (forward arcs of changed edges)
+    if (!repair_deltas(c, p, Mn, O)) return false;
+    M = Mn;
+    if (!t_reach) return true;
+    return preflow(c, s);
+}
+
+// Capacity deltas on kept arcs (forward arcs of changed edges) whose ends
+// were both kept before (claim O) and are kept now (mark Mn): a rise adds
+// residual; a fall below the arc's flow cancels the excess flow, leaving
+// the surplus as excess at the tail and a deficit at the head.
+__device__ bool repair_deltas(QCtx &c, const KParams &p, unsigned Mn, unsigned O) {
+    unsigned *mark = c.st.mark, *claim = c.st.claim;
+    const int *rev = c.rev;
     int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
     for (int i = gt; i < p.nupd; i += gT) {
         ArcUpdate u = p.upd[i];
@@ -2248,10 +2325,7 @@ __device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int
             atomic_add_i64(&c.st.ex[w], -over);
         }
     }
-    if (!c.sync()) return false;
-    M = Mn;
-    if (!t_reach) return true;
-    return preflow(c, s);
+    return c.sync();
 }
 
 // ---------------------------------------------------------------------------
@@ -2446,6 +2520,8 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
         c.st.meta[2] = s;
         c.st.meta[3] = t;
         c.st.meta[4] = c.vf;
+        c.st.meta[5] = t_reach ? 1 : 0;
+        c.st.meta[6] = (int)min(tot[T_MASKARCS], (i64)INT_MAX);
     }
     c.sync();
 }
