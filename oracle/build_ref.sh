@@ -3,10 +3,14 @@
 # (read-only) into oracle/_ref/ra_ref, for sm_100a, with the device shim
 # above.  Nothing is copied out of the reference tree; the only output is the
 # executable.  Test infrastructure only: the engine never runs it.
-#   usage: oracle/build_ref.sh [reference_root]
+#   usage: oracle/build_ref.sh REFERENCE_ROOT   (or MF_REFERENCE_ROOT set)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${MF_REFERENCE_ROOT:-}}"
+if [ -z "$REF" ]; then
+  echo "build_ref: give the reference project's root (argument or MF_REFERENCE_ROOT)" >&2
+  exit 0
+fi
 SRC="$REF/Region_Aware_PR_with_Pruning_BoundaryCore.cu"
 if [ ! -f "$SRC" ]; then
   echo "build_ref: $SRC not found; keeping any prebuilt oracle/_ref/ra_ref" >&2
