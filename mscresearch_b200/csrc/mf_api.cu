@@ -266,6 +266,12 @@ struct mf_graph {
     int *giants = nullptr;  // device: their internal ids
     std::vector<int> deg_host;                // internal id -> arcs
     std::vector<unsigned char> kc_in_host;    // internal id -> in the cached component
+    // grow-only device buffers of capacity-update batches (resolution arrays;
+    // resolved records), kept so that a batch allocates nothing
+    void *upd_scratch = nullptr;
+    size_t upd_scratch_bytes = 0;
+    ArcUpdate *upd_recs = nullptr;
+    size_t upd_recs_cap = 0;
     // kept-set cache (see DGraph)
     unsigned char *kc_in = nullptr;
     unsigned char *kc_fb = nullptr;
@@ -336,6 +342,15 @@ cudaError_t up(const mf_graph *g, void *dst, const void *src, size_t n);
 cudaError_t zero(const mf_graph *g, void *dst, size_t n);
 cudaError_t down(const mf_graph *g, void *dst, const void *src, size_t n);
 
+// Marks the kept-set cache stale (capacities changed) and keeps its buffers
+// for the rebuild: freeing and re-allocating ~9 bytes per arc on every
+// update batch cost a device-wide synchronization and tens of ms.
+void invalidate_kept_cache(mf_graph *g) {
+    g->kc_valid = false;
+    g->kc_tried = false;
+    g->kc_in_host.clear();
+}
+
 void free_kept_cache(mf_graph *g) {
     mf_dfree(g->kc_in);
     mf_dfree(g->kc_fb);
@@ -352,6 +367,12 @@ void free_kept_cache(mf_graph *g) {
 
 void free_graph_arrays(mf_graph *g) {
     free_kept_cache(g);
+    mf_dfree(g->upd_scratch);
+    g->upd_scratch = nullptr;
+    g->upd_scratch_bytes = 0;
+    mf_dfree(g->upd_recs);
+    g->upd_recs = nullptr;
+    g->upd_recs_cap = 0;
     mf_dfree(g->row);
     mf_dfree(g->col);
     mf_dfree(g->rev);
@@ -1215,11 +1236,12 @@ static int build_kept_cache(mf_graph *g, const mf_opts &o) {
     g->kc_tried = true;
     int n = g->n;
     KcOut ko{};
-    CK(mf_dmalloc(&g->kc_in, n));
-    CK(mf_dmalloc(&g->kc_img, sizeof(int) * (size_t)n));
-    CK(mf_dmalloc(&g->kc_res, sizeof(i64) * (size_t)std::max<i64>(g->arcs, 1)));
+    // buffers kept from an invalidated cache are reused
+    if (!g->kc_in) CK(mf_dmalloc(&g->kc_in, n));
+    if (!g->kc_img) CK(mf_dmalloc(&g->kc_img, sizeof(int) * (size_t)n));
+    if (!g->kc_res) CK(mf_dmalloc(&g->kc_res, sizeof(i64) * (size_t)std::max<i64>(g->arcs, 1)));
     CK(zero(g, g->kc_in, n));
-    CK(mf_dmalloc(&g->kc_fb, n));
+    if (!g->kc_fb) CK(mf_dmalloc(&g->kc_fb, n));
     ko.img = g->kc_img;
     ko.in = g->kc_in;
     ko.fb = g->kc_fb;
@@ -1650,13 +1672,17 @@ static int resolve_updates(mf_graph *g, int nb, const int32_t *u, const int32_t 
         ui[i] = ok ? g->new_id[u[i]] : -1;
         vi[i] = ok ? g->new_id[v[i]] : -1;
     }
-    int *du = nullptr, *dv = nullptr, *darc = nullptr;
-    i64 *dcap = nullptr;
-    DevScope tmp;
-    CK(tmp.alloc(&du, sizeof(int) * nb));
-    CK(tmp.alloc(&dv, sizeof(int) * nb));
-    CK(tmp.alloc(&darc, sizeof(int) * nb));
-    CK(tmp.alloc(&dcap, sizeof(i64) * nb));
+    // du | dv | darc (int) then dcap (i64), in the graph's update scratch
+    const size_t need = sizeof(i64) * (size_t)nb + 3 * sizeof(int) * (size_t)nb + 16;
+    if (g->upd_scratch_bytes < need) {
+        mf_dfree(g->upd_scratch);
+        g->upd_scratch = nullptr;
+        g->upd_scratch_bytes = 0;
+        CK(mf_dmalloc(&g->upd_scratch, need));
+        g->upd_scratch_bytes = need;
+    }
+    i64 *dcap = reinterpret_cast<i64 *>(g->upd_scratch);
+    int *du = reinterpret_cast<int *>(dcap + nb), *dv = du + nb, *darc = dv + nb;
     CK(up(g, du, ui.data(), sizeof(int) * nb));
     CK(up(g, dv, vi.data(), sizeof(int) * nb));
     k_find_arcs<<<(unsigned)((nb + 7) / 8), 256, 0, g->stream>>>(nb, du, dv, g->row, g->col, g->rev, g->fwd, g->cap, darc, dcap);
@@ -1694,14 +1720,21 @@ static int resolve_updates(mf_graph *g, int nb, const int32_t *u, const int32_t 
 static int apply_updates(mf_graph *g, const std::vector<ArcUpdate> &ups, ArcUpdate **d_out) {
     *d_out = nullptr;
     if (ups.empty()) return MF_OK;
-    // capacities change reachability: drop the kept-set cache (rebuilt lazily)
+    // capacities change reachability: the kept-set cache goes stale (rebuilt
+    // lazily, in the same buffers)
     if (g->kc_valid || g->kc_tried) {
-        free_kept_cache(g);
+        invalidate_kept_cache(g);
         int rc = upload_dgraph(g);
         if (rc) return rc;
     }
-    ArcUpdate *d = nullptr;
-    CK(mf_dmalloc(&d, sizeof(ArcUpdate) * ups.size()));
+    if (g->upd_recs_cap < ups.size()) {
+        mf_dfree(g->upd_recs);
+        g->upd_recs = nullptr;
+        g->upd_recs_cap = 0;
+        CK(mf_dmalloc(&g->upd_recs, sizeof(ArcUpdate) * ups.size()));
+        g->upd_recs_cap = ups.size();
+    }
+    ArcUpdate *d = g->upd_recs;  // owned by the graph: valid until its next update batch
     CK(up(g, d, ups.data(), sizeof(ArcUpdate) * ups.size()));
     k_apply_caps<<<((int)ups.size() + 255) / 256, 256, 0, g->stream>>>((int)ups.size(), d, g->cap);
     CK(cudaStreamSynchronize(g->stream));
@@ -1719,7 +1752,6 @@ int mf_update_caps(mf_graph *g, int nb, const int32_t *u, const int32_t *v, cons
     if (rc) return rc;
     ArcUpdate *d = nullptr;
     rc = apply_updates(g, ups, &d);
-    mf_dfree(d);
     return rc;
 }
 
@@ -1816,7 +1848,6 @@ int mf_session_update(mf_session *ss, int nb, const int32_t *u, const int32_t *v
     if (const char *e = getenv("MF_REPAIR_MAX_UPDATES")) lim = atoll(e);
     if ((long long)ups.size() > lim) rc = session_run(ss, KM_SOLVE, nullptr, 0, flows, stats);
     else rc = session_run(ss, KM_REPAIR, d, (int)ups.size(), flows, stats);
-    mf_dfree(d);
     return rc;
 }
 
@@ -2304,8 +2335,7 @@ int mf_server_destroy(mf_server *sv) {
     for (size_t i = 0; i < sv->graphs.size() && i < sv->updated.size(); ++i) {
         if (!sv->updated[i]) continue;
         mf_graph *g = sv->graphs[i];
-        free_kept_cache(g);
-        g->kc_tried = false;
+        invalidate_kept_cache(g);
         upload_dgraph(g);
     }
     for (void *m : sv->slot_mem) mf_dfree_async(m, sv->side ? sv->side : sv->stream);
