@@ -578,6 +578,10 @@ KOpts resolve_opts(const mf_opts &o, int avg_deg) {
     k.iter_max = o.iter_max > 0 ? o.iter_max : 20000000;
     k.gr_stop = o.relabel_early_stop;
     if (const char *e = getenv("MF_RELABEL_EARLY_STOP")) k.gr_stop = atoi(e);
+    // relabel searches go bottom-up when the frontier's arcs exceed bu_arcs
+    // per unvisited vertex (MF_BU_ARCS overrides it; 0 = vertex counts only)
+    k.bu_arcs = 8;
+    if (const char *e = getenv("MF_BU_ARCS")) k.bu_arcs = std::max(0, atoi(e));
     return k;
 }
 

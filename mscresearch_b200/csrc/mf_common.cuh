@@ -141,7 +141,7 @@ struct GroupBar {
     int snap;      // values captured by the last arriver (gsync_snap)
     int snap2;
     int snap3;
-    int pad;
+    int snap4;
 };
 
 // gsync_snap additionally returns, to every thread of the group, the values
@@ -151,9 +151,10 @@ struct GroupBar {
 __device__ __forceinline__ bool gsync_impl(int G, GroupBar *bar, int *err, u64 limit_ns,
                                            const int *src, const int *src2, int *snap_out,
                                            int *snap2_out, const int *src3 = nullptr,
-                                           int *snap3_out = nullptr) {
+                                           int *snap3_out = nullptr, const int *src4 = nullptr,
+                                           int *snap4_out = nullptr) {
     __shared__ int s_ok;
-    __shared__ int s_snap, s_snap2, s_snap3;
+    __shared__ int s_snap, s_snap2, s_snap3, s_snap4;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
@@ -161,6 +162,7 @@ __device__ __forceinline__ bool gsync_impl(int G, GroupBar *bar, int *err, u64 l
             s_snap = *(volatile const int *)src;
             s_snap2 = *(volatile const int *)src2;
             if (src3) s_snap3 = *(volatile const int *)src3;
+            if (src4) s_snap4 = *(volatile const int *)src4;
         }
         if (G > 1) {
             volatile unsigned *vgen = &bar->gen;
@@ -173,6 +175,7 @@ __device__ __forceinline__ bool gsync_impl(int G, GroupBar *bar, int *err, u64 l
                     *(volatile int *)&bar->snap = *(volatile const int *)src;
                     *(volatile int *)&bar->snap2 = *(volatile const int *)src2;
                     if (src3) *(volatile int *)&bar->snap3 = *(volatile const int *)src3;
+                    if (src4) *(volatile int *)&bar->snap4 = *(volatile const int *)src4;
                 }
                 atomicExch(&bar->arrive, 0u);
                 __threadfence();
@@ -198,6 +201,7 @@ __device__ __forceinline__ bool gsync_impl(int G, GroupBar *bar, int *err, u64 l
                 s_snap = *(volatile int *)&bar->snap;
                 s_snap2 = *(volatile int *)&bar->snap2;
                 if (src3) s_snap3 = *(volatile int *)&bar->snap3;
+                if (src4) s_snap4 = *(volatile int *)&bar->snap4;
             }
         }
         if (*(volatile int *)err) ok = 0;
@@ -209,6 +213,7 @@ __device__ __forceinline__ bool gsync_impl(int G, GroupBar *bar, int *err, u64 l
         *snap2_out = s_snap2;
     }
     if (snap3_out) *snap3_out = s_snap3;
+    if (snap4_out) *snap4_out = s_snap4;
     return s_ok != 0;
 }
 

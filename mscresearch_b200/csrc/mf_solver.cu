@@ -57,6 +57,7 @@
 #define CNT_HUBCH 30  // total chunks of the current hub pass
 #define CNT_ACT 40    // global relabel: active vertices to label
 #define CNT_FOUND 41  // global relabel: active vertices labelled so far
+#define CNT_FARCS 42  // global relabel: arcs of the vertices labelled so far
 #define CNT_Q 8      // query handed to the group
 #define CNT_FLAG 9   // misc uniform flag
 #define CNT_RS 10    // serving: request source / sink / graph
@@ -128,7 +129,9 @@ struct QCtx {
     // per-warp counters (flushed at the end of the query)
     i64 w_arcs, w_verts, w_push;
     int bu_factor;  // direction switch of the searches (KOpts::bu_factor)
+    int bu_arcs;    // and its arc criterion (KOpts::bu_arcs)
     bool no_cache;  // the graph's kept-set cache is stale (a served capacity update)
+    i64 w_farcs;    // arcs of the vertices this thread labelled (relabel searches)
 
     __device__ bool sync() { return gsync(G, bar, err, lim); }
     // a vertex with arcs [b, e1) that for_giants covers
@@ -138,10 +141,11 @@ struct QCtx {
     __device__ bool sync_tails(int bank, int &ft, int &bt) {
         return gsync_snap(G, bar, err, lim, &st.cnt[bank], &st.cnt[CNT_BACK + bank], &ft, &bt);
     }
-    // the same, also returning the value of the control word cnt[w3] as of
-    // the barrier
-    __device__ bool sync_tails3(int bank, int &ft, int &bt, int w3, int &v3) {
-        return gsync_impl(G, bar, err, lim, &st.cnt[bank], &st.cnt[CNT_BACK + bank], &ft, &bt, &st.cnt[w3], &v3);
+    // the same, also returning the values of the control words cnt[w3] and
+    // cnt[w4] as of the barrier
+    __device__ bool sync_tails4(int bank, int &ft, int &bt, int w3, int &v3, int w4, int &v4) {
+        return gsync_impl(G, bar, err, lim, &st.cnt[bank], &st.cnt[CNT_BACK + bank], &ft, &bt, &st.cnt[w3], &v3,
+                          &st.cnt[w4], &v4);
     }
     __device__ int take_bank() {
         int b = seq & (NBANKS - 1);
@@ -460,11 +464,19 @@ static_assert(CNT_SOLO >= CNT_BACK + NBANKS && CNT_SOLO > CNT_HUBCH && CNT_SOLO 
 template <class Claim, class UF, class UB, class Par, class Set, class Hook = NoLevelHook>
 __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, int nuf, UF uf, int nub,
                         UB ub, Par par, Set set, Hook on_level = Hook{}, int *levels_out = nullptr,
-                        int stop_at = -1, bool *stopped_out = nullptr) {
+                        int stop_at = -1, bool *stopped_out = nullptr, bool arcs_rule = false) {
     // stop_at >= 0: the search ends after the first level by which the
-    // control word cnt[CNT_FOUND] (raised by cl / set) has reached stop_at
+    // control word cnt[CNT_FOUND] (raised by cl / set) has reached stop_at.
+    // arcs_rule: cl / set add the arcs of every vertex they claim to the
+    // thread's w_farcs; the level's total (cnt[CNT_FARCS], snapshotted at the
+    // level barrier) is the next frontier's arc count, and a frontier with
+    // more than bu_arcs arcs per unvisited vertex also goes bottom-up (a few
+    // hub vertices can carry more arcs than the whole unvisited universe
+    // would cost to test)
     int flo = 0, blo = 0, pflo = 0, pblo = 0, level = 0, nbu = 0, nsolo = 0;
     bool stopped = stop_at == 0;
+    long long ffarcs = 0;  // arcs of the current frontier (0: unknown)
+    int farcs_prev = 0;
     const long long nu = (long long)nuf + nub;
     const int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
     while (!stopped && (flo < fhi || blo < bhi)) {
@@ -473,7 +485,8 @@ __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, i
         // bottom-up sweeps the whole universe, so the frontier must also be a
         // sizeable share of it (a small frontier near the end of a deep
         // search is cheaper to expand than nu candidates are to check)
-        const bool bottom_up = nu > visited && fsize * c.bu_factor > nu - visited && fsize * 64 > nu;
+        const bool bottom_up = nu > visited && ((fsize * c.bu_factor > nu - visited && fsize * 64 > nu) ||
+                                                (arcs_rule && ffarcs > (long long)c.bu_arcs * (nu - visited)));
         if (!bottom_up && c.G > 1 && fsize <= SOLO_MAX && bhi == blo) {
             if (c.crank == 0) {
                 const int wpc = blockDim.x >> 5;
@@ -481,6 +494,11 @@ __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, i
                     MF_TRACE(11, level);
                     on_level(level, pflo, flo, pblo, blo, threadIdx.x, blockDim.x);
                     td_level(c, Q, bank, flo, fhi, blo, bhi, level, cl, c.warp, wpc);
+                    if (arcs_rule) {
+                        const i64 x = warp_sum_i64(c.w_farcs);
+                        c.w_farcs = 0;
+                        if (c.lane == 0 && x) atomicAdd(&c.st.cnt[CNT_FARCS], (int)x);
+                    }
                     __syncthreads();
                     const int ft = ldcg(&c.st.cnt[bank]), bt = ldcg(&c.st.cnt[CNT_BACK + bank]);
                     __syncthreads();
@@ -527,6 +545,8 @@ __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, i
             pflo = ldcg(&o[5]);
             pblo = ldcg(&o[6]);
             stopped = ldcg(&o[7]) != 0;
+            ffarcs = 0;  // solo frontiers are small; the vertex rule decides
+            farcs_prev = ldcg(&c.st.cnt[CNT_FARCS]);  // stable: nobody claims until the next level
             continue;
         }
         MF_TRACE(10, level);
@@ -537,10 +557,17 @@ __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, i
         } else
             td_level(c, Q, bank, flo, fhi, blo, bhi, level, cl, c.gw, c.gW);
         int ft = 0, bt = 0;
-        if (stop_at > 0) {
-            int found = 0;
-            if (!c.sync_tails3(bank, ft, bt, CNT_FOUND, found)) return false;
-            stopped = found >= stop_at;
+        if (arcs_rule) {
+            const i64 x = warp_sum_i64(c.w_farcs);
+            c.w_farcs = 0;
+            if (c.lane == 0 && x) atomicAdd(&c.st.cnt[CNT_FARCS], (int)x);
+        }
+        if (stop_at > 0 || arcs_rule) {
+            int found = 0, farcs = 0;
+            if (!c.sync_tails4(bank, ft, bt, CNT_FOUND, found, CNT_FARCS, farcs)) return false;
+            if (stop_at > 0) stopped = found >= stop_at;
+            ffarcs = (long long)farcs - farcs_prev;
+            farcs_prev = farcs;
         } else if (!c.sync_tails(bank, ft, bt)) {
             return false;
         }
@@ -1025,6 +1052,7 @@ __device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &de
     const i64 *ex = c.st.ex;
     int *found = c.st.cnt + CNT_FOUND;
     const bool count = stop_at > 0;
+    const bool arcs_rule = c.bu_arcs > 0;
     auto relab = [&](int v, int e, int w, int level) -> bool {
         const unsigned bit = 1u << (w & 31);
         unsigned vw = ldcg(&vis[w >> 5]);
@@ -1034,6 +1062,7 @@ __device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &de
         h[w] = level + 1;
         atomicOr(&fmap(level + 1)[w >> 5], bit);
         if (count && ldcg(&ex[w]) > 0) atomicAdd(found, 1);
+        if (arcs_rule) c.w_farcs += c.deg(w);
         return true;
     };
     auto unvisited = [&](int w) -> bool { return !((ldcg(&vis[w >> 5]) >> (w & 31)) & 1u); };
@@ -1057,6 +1086,7 @@ __device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &de
         atomicOr(&vis[w >> 5], bit);
         atomicOr(&fmap(level + 1)[w >> 5], bit);
         if (count && ldcg(&ex[w]) > 0) atomicAdd(found, 1);
+        if (arcs_rule) c.w_farcs += c.deg(w);
         return true;
     };
     // at level L the previous frontier's bits leave map (L - 1) % 3, which
@@ -1074,8 +1104,9 @@ __device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &de
             atomicAnd(&z[v >> 5], ~(1u << (v & 31)));
         }
     };
+    c.w_farcs = 0;
     return bfs_dir(c, c.st.qa, bank, fhi, bhi, relab, c.vf, uf, nv - c.vf, ub, par, set, clear_prev, &depth,
-                   stop_at, &stopped);
+                   stop_at, &stopped, arcs_rule);
 }
 
 // Kept-vertex bitmap of the query (bit v: mark[v] >= M), read by every
@@ -1137,6 +1168,7 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
         if (c.leader) {
             c.st.cnt[CNT_ACT] = 0;
             c.st.cnt[CNT_FOUND] = 0;
+            c.st.cnt[CNT_FARCS] = 0;
         }
     }
     if (!c.sync()) return false;
@@ -2820,6 +2852,8 @@ __device__ __forceinline__ int init_ctx(QCtx &c, const KParams &p) {
     c.err = p.err;
     c.lim = p.bar_limit_ns;
     c.bu_factor = p.o.bu_factor;
+    c.bu_arcs = p.o.bu_arcs;
+    c.w_farcs = 0;
     c.leader = (c.crank == 0 && threadIdx.x == 0);
     c.w_arcs = c.w_verts = c.w_push = 0;
     c.t_start = globaltimer_ns();

@@ -109,6 +109,8 @@ struct KOpts {
     int bu_factor;  // bottom-up when frontier x bu_factor > unvisited (and >= 1/64 of all)
     i64 iter_max;
     int gr_stop;    // global relabels end once every active vertex is labelled
+    int bu_arcs;    // relabel searches also go bottom-up when the frontier has more than
+                    // bu_arcs arcs per unvisited vertex (0: vertex counts only)
 };
 
 // Per-query outputs.
