@@ -2471,7 +2471,19 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
                 i64 A = ldro(&c.row[c.n]);
                 i64 nvec = A >> 1;
                 int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
-                for (i64 k = gt; k < nvec; k += gT) dst[k] = __ldg(&src[k]);
+                // four independent loads in flight per thread (the arrays
+                // may alias as far as the compiler knows, so a plain loop
+                // waits out one load latency per vector)
+                i64 k = gt;
+                for (; k + 3 * (i64)gT < nvec; k += 4 * (i64)gT) {
+                    const longlong2 x0 = __ldg(&src[k]), x1 = __ldg(&src[k + gT]);
+                    const longlong2 x2 = __ldg(&src[k + 2 * (i64)gT]), x3 = __ldg(&src[k + 3 * (i64)gT]);
+                    dst[k] = x0;
+                    dst[k + gT] = x1;
+                    dst[k + 2 * (i64)gT] = x2;
+                    dst[k + 3 * (i64)gT] = x3;
+                }
+                for (; k < nvec; k += gT) dst[k] = __ldg(&src[k]);
                 if (gt == 0 && (A & 1)) c.st.res[A - 1] = ldro(&g.kc_res[A - 1]);
                 if (c.lane == 0 && c.gw == 0) c.w_verts += nv;
                 if (!c.sync()) return;
