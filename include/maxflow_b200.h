@@ -76,6 +76,10 @@ typedef struct mf_opts {
                                exact height (vertices it did not reach stay at height n until the
                                next relabel; a search that cannot reach every active vertex runs to
                                the end, so the relabel that ends a solve is exact) */
+    int local_relabel;     /* k > 0: after every k-th discharge round between global relabels, when
+                              the round's active heights span at most 128 levels, relabel the regions
+                              holding active vertices by a depth-bounded search (RA:1583-1720;
+                              heights only rise; RM is off while it is on); 0 = off (default) */
 } mf_opts;
 
 /* Per-query statistics (all counts exact device counters). */
@@ -108,6 +112,7 @@ typedef struct mf_stats {
     long long levels;         /* search levels (prune, global relabels, certificate) */
     long long levels_bottom_up; /* of which bottom-up */
     long long levels_solo;    /* of which run by a single CTA */
+    long long local_relabels; /* local relabels (mf_opts.local_relabel) */
 } mf_stats;
 
 void mf_opts_default(mf_opts *o);

@@ -43,6 +43,7 @@ class MfOpts(C.Structure):
         ("use_kept_cache", C.c_int),
         ("schedule", C.c_int),
         ("relabel_early_stop", C.c_int),
+        ("local_relabel", C.c_int),
     ]
 
 
@@ -75,6 +76,7 @@ class MfStats(C.Structure):
         ("levels", C.c_longlong),
         ("levels_bottom_up", C.c_longlong),
         ("levels_solo", C.c_longlong),
+        ("local_relabels", C.c_longlong),
     ]
 
 

@@ -582,6 +582,8 @@ KOpts resolve_opts(const mf_opts &o, int avg_deg) {
     // per unvisited vertex (MF_BU_ARCS overrides it; 0 = vertex counts only)
     k.bu_arcs = 8;
     if (const char *e = getenv("MF_BU_ARCS")) k.bu_arcs = std::max(0, atoi(e));
+    k.local_rl = std::max(0, o.local_relabel);
+    if (const char *e = getenv("MF_LOCAL_RELABEL")) k.local_rl = std::max(0, atoi(e));
     return k;
 }
 
@@ -719,6 +721,7 @@ void fill_stats(mf_stats *st, const QOut &q, double ms, u64 launch_t0) {
     st->levels = q.levels;
     st->levels_bottom_up = q.levels_bottom_up;
     st->levels_solo = q.levels_solo;
+    st->local_relabels = q.local_relabels;
     st->finish_ms = launch_t0 ? (double)(q.t_done - launch_t0) * 1e-6 : 0.0;
     st->flow = q.flow;
     st->status = status_from_err(q.status);
@@ -964,6 +967,7 @@ void mf_opts_default(mf_opts *o) {
     o->use_kept_cache = 1;
     o->schedule = 1;
     o->relabel_early_stop = 1;
+    o->local_relabel = 0;
 }
 
 const char *mf_last_error_string(void) { return g_err.c_str(); }

@@ -464,7 +464,8 @@ static_assert(CNT_SOLO >= CNT_BACK + NBANKS && CNT_SOLO > CNT_HUBCH && CNT_SOLO 
 template <class Claim, class UF, class UB, class Par, class Set, class Hook = NoLevelHook>
 __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, int nuf, UF uf, int nub,
                         UB ub, Par par, Set set, Hook on_level = Hook{}, int *levels_out = nullptr,
-                        int stop_at = -1, bool *stopped_out = nullptr, bool arcs_rule = false) {
+                        int stop_at = -1, bool *stopped_out = nullptr, bool arcs_rule = false,
+                        int max_levels = INT_MAX) {
     // stop_at >= 0: the search ends after the first level by which the
     // control word cnt[CNT_FOUND] (raised by cl / set) has reached stop_at.
     // arcs_rule: cl / set add the arcs of every vertex they claim to the
@@ -473,13 +474,15 @@ __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, i
     // more than bu_arcs arcs per unvisited vertex also goes bottom-up (a few
     // hub vertices can carry more arcs than the whole unvisited universe
     // would cost to test)
+    // max_levels: at most this many levels are expanded (a local relabel's
+    // depth bound)
     int flo = 0, blo = 0, pflo = 0, pblo = 0, level = 0, nbu = 0, nsolo = 0;
     bool stopped = stop_at == 0;
     long long ffarcs = 0;  // arcs of the current frontier (0: unknown)
     int farcs_prev = 0;
     const long long nu = (long long)nuf + nub;
     const int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
-    while (!stopped && (flo < fhi || blo < bhi)) {
+    while (!stopped && (flo < fhi || blo < bhi) && level < max_levels) {
         const long long visited = (long long)fhi + bhi;
         const long long fsize = (long long)(fhi - flo) + (bhi - blo);
         // bottom-up sweeps the whole universe, so the frontier must also be a
@@ -519,7 +522,7 @@ __device__ bool bfs_dir(QCtx &c, int *Q, int bank, int fhi, int bhi, Claim cl, i
                     }
                     const long long fs = (long long)(fhi - flo) + (bhi - blo);
                     const long long vis = (long long)fhi + bhi;
-                    if (fs == 0 || fs > SOLO_MAX || bhi != blo || (nu > vis && fs * c.bu_factor > nu - vis && fs * 64 > nu))
+                    if (level >= max_levels || fs == 0 || fs > SOLO_MAX || bhi != blo || (nu > vis && fs * c.bu_factor > nu - vis && fs * 64 > nu))
                         break;
                 }
                 if (threadIdx.x == 0) {
@@ -1038,8 +1041,10 @@ __device__ bool preflow(QCtx &c, int s) {
 // (atomicOr on the visited word).  Bottom-up: an unvisited kept vertex w
 // takes level + 1 when one of its residual arcs reaches the frontier map.
 // Claims write the height and the next frontier bit.
-__device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &depth, int stop_at,
-                            bool &stopped) {
+// Q: the search queue (front / back parts of list bank `bank`).  raise_only:
+// a reached vertex takes max(its height, its distance) (local relabels).
+__device__ bool relabel_bfs(QCtx &c, int *Q, int nv, int bank, int fhi, int bhi, int &depth, int stop_at,
+                            bool &stopped, int max_levels = INT_MAX, bool raise_only = false) {
     const int W = bitmap_words(c.n);
     unsigned *vis = c.st.bits + W, *F = c.st.bits + 2 * W;
     const int *rev = c.rev;
@@ -1059,7 +1064,7 @@ __device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &de
         i64 rr = ldcg(&res[ldro(&rev[e])]);
         if ((vw & bit) || rr <= 0) return false;
         if (atomicOr(&vis[w >> 5], bit) & bit) return false;
-        h[w] = level + 1;
+        h[w] = raise_only ? max(ldcg(&h[w]), level + 1) : level + 1;
         atomicOr(&fmap(level + 1)[w >> 5], bit);
         if (count && ldcg(&ex[w]) > 0) atomicAdd(found, 1);
         if (arcs_rule) c.w_farcs += c.deg(w);
@@ -1082,7 +1087,7 @@ __device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &de
     };
     auto set = [&](int w, int level) -> bool {
         const unsigned bit = 1u << (w & 31);
-        h[w] = level + 1;
+        h[w] = raise_only ? max(ldcg(&h[w]), level + 1) : level + 1;
         atomicOr(&vis[w >> 5], bit);
         atomicOr(&fmap(level + 1)[w >> 5], bit);
         if (count && ldcg(&ex[w]) > 0) atomicAdd(found, 1);
@@ -1091,7 +1096,6 @@ __device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &de
     };
     // at level L the previous frontier's bits leave map (L - 1) % 3, which
     // level L + 1 fills again (cost: the frontier's size, not n)
-    const int *Q = c.st.qa;
     auto clear_prev = [&](int level, int plo, int phi, int pblo, int pbhi, int tid, int nth) {
         if (level == 0) return;
         unsigned *z = fmap(level - 1);
@@ -1105,8 +1109,8 @@ __device__ bool relabel_bfs(QCtx &c, int nv, int bank, int fhi, int bhi, int &de
         }
     };
     c.w_farcs = 0;
-    return bfs_dir(c, c.st.qa, bank, fhi, bhi, relab, c.vf, uf, nv - c.vf, ub, par, set, clear_prev, &depth,
-                   stop_at, &stopped, arcs_rule);
+    return bfs_dir(c, Q, bank, fhi, bhi, relab, c.vf, uf, nv - c.vf, ub, par, set, clear_prev, &depth,
+                   stop_at, &stopped, arcs_rule, max_levels);
 }
 
 // Kept-vertex bitmap of the query (bit v: mark[v] >= M), read by every
@@ -1219,7 +1223,7 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
     // end as before, so the relabel that ends a phase stays exact.
     const int stop_at = early_stop ? ldcg(&c.st.cnt[CNT_ACT]) : -1;
     bool stopped = false;
-    if (!relabel_bfs(c, nv, qbk, f0, b0, depth, stop_at, stopped)) return false;
+    if (!relabel_bfs(c, c.st.qa, nv, qbk, f0, b0, depth, stop_at, stopped)) return false;
     if (complete) *complete = !stopped;
     int *h = c.st.h;
 
@@ -1265,6 +1269,72 @@ __device__ bool global_relabel(QCtx &c, int nv, unsigned M, int sinkv, int block
     if (!c.sync_tails(lbk, naf, nab)) return false;
     nd = (int)ldcg(&ab[A_NDEF]);
     return true;
+}
+
+// ---------------------------------------------------------------------------
+// Local relabel (RA:236-279 init_local_frontier_in_band, RA:519-556
+// compute_active_height_range / compute_region_active, driver RA:1583-1720).
+// Between global relabels, when the active vertices' heights span at most
+// LR_BAND levels: a backward search over the kept vertices of the regions
+// that hold an active vertex (the next worklist N) whose height is below n
+// (RA's band: its margin of n covers every height below n).  Seeds at
+// height 0: the phase sink and, in phases A and B, the deficit vertices of
+// that universe.  At most band + 3 levels are expanded (RA:1683 runs
+// levels 0 .. band + 2).  A vertex the search reaches takes the larger of
+// its height and its distance; one it does not reach, the seeds and the
+// vertices outside the universe keep theirs.  RA's version sets the distance
+// even where it is lower; here heights never fall between global relabels.
+// A raised height may exceed a neighbour's outside the universe by more than
+// one, which is what RM treats as an invalid arc: with both on, RM moved
+// that flow back each time and an R-MAT 2^14 query with relabels every 64
+// rounds ran into the launch time limit (with RA's lowering rule too), so
+// RM is off while local relabels are on.  Exactness does not rest on these
+// labels: only an exact global relabel ends a solve.  N is
+// unchanged; the search queue is Q, a list buffer other than N (the
+// worklist the next round fills).  The search overwrites the visited and
+// frontier bitmaps, so the next global relabel takes no dead marks from
+// them.
+#define LR_BAND 128
+__device__ bool local_relabel(QCtx &c, int nv, int sinkv, int blockv, int srcv, bool deficit_seeds, const int *N,
+                              int nNf, int nNb, int *Q, int band, int &depth) {
+    MF_TRACE(48, band);
+    {
+        const int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+        for (int i = gt; i < nNf + nNb; i += gT) {
+            const int v = i < nNf ? ldcg(&N[i]) : back_at(c, N, i - nNf);
+            c.st.ract[ldro(&c.rof[v])] = 1;
+        }
+    }
+    const int qbk = c.take_bank();
+    if (c.leader) c.st.cnt[CNT_FARCS] = 0;
+    if (!c.sync()) return false;
+    // visited = everything outside the universe, plus the seeds; the seeds
+    // also form the first frontier
+    const int n = c.n, W = bitmap_words(n);
+    unsigned *kept = c.st.bits, *vis = kept + W, *F0 = kept + 2 * W;
+    for (int wd = c.gw; wd < W; wd += c.gW) {
+        const unsigned kw = ldcg(&kept[wd]);
+        const int v = wd * 32 + c.lane;  // below n wherever its kept bit is set
+        bool in = false, seed = false;
+        if ((kw >> c.lane) & 1u) {
+            in = v != blockv && ldcg(&c.st.h[v]) < n && ldcg(&c.st.ract[ldro(&c.rof[v])]) != 0;
+            if (in)
+                seed = v == sinkv || (deficit_seeds && v != srcv && ldcg(&c.st.ex[v]) < 0);
+        }
+        const unsigned inw = __ballot_sync(MF_FULL, in), sw = __ballot_sync(MF_FULL, seed);
+        if (c.lane == 0) {
+            vis[wd] = ~inw | sw;
+            F0[wd] = sw;
+            F0[W + wd] = 0;
+            F0[2 * W + wd] = 0;
+        }
+        append2(c, seed, v, Q, qbk);
+    }
+    int f0 = 0, b0 = 0;
+    if (!c.sync_tails(qbk, f0, b0)) return false;
+    if (f0 + b0 == 0) return true;
+    bool stopped = false;
+    return relabel_bfs(c, Q, nv, qbk, f0, b0, depth, -1, stopped, band + 3, true);
 }
 
 // ---------------------------------------------------------------------------
@@ -2027,7 +2097,8 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
                 qo.hot_sweeps++;
             }
             // RM (RA:1991-2097)
-            bool do_rm = o.use_rm && start_phase != PH_C && nNf + nNb > 0 && (round % rm_freq) == 0 &&
+            bool do_rm = o.use_rm && o.local_rl == 0 && start_phase != PH_C && nNf + nNb > 0 &&
+                         (round % rm_freq) == 0 &&
                          (o.force_rm || frac_high >= 0.5f);
             if (do_rm) {
                 int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
@@ -2071,6 +2142,23 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
                           (force_gr || rounds_since >= gr_freq ||
                            (o.gr_alpha > 0.0 && (double)work_since >= o.gr_alpha * (double)mask_arcs));
             if (gr_due) break;
+            // local relabel between global ones (RA:1583-1720), every
+            // local_rl-th round, when this round's active heights spanned at
+            // most LR_BAND levels
+            if (o.local_rl > 0 && naf + nab > 0 && (rounds_since % o.local_rl) == 0 && hmax >= hmin &&
+                hmax - hmin < LR_BAND) {
+                const u64 tl0 = globaltimer_ns();
+                const i64 la0 = c.w_arcs;
+                int ldepth = 0;
+                if (!local_relabel(c, nv, sinkv, blockv, s, defseeds, L, naf, nab, N, hmax - hmin + 1, ldepth))
+                    return false;
+                last_complete = false;
+                qo.local_relabels++;
+                const u64 dl = globaltimer_ns() - tl0;
+                c.tm_relabel += dl;
+                tr0 += dl;  // rounds time excludes it
+                if (c.lane == 0 && c.w_arcs > la0) atomic_add_i64(&c.st.acc[ACC_TOT + T_RARCS], c.w_arcs - la0);
+            }
         }
         c.tm_rounds += globaltimer_ns() - tr0;
         // relabel (either nothing is active -> exact termination check, or due)

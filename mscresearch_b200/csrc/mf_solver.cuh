@@ -111,6 +111,7 @@ struct KOpts {
     int gr_stop;    // global relabels end once every active vertex is labelled
     int bu_arcs;    // relabel searches also go bottom-up when the frontier has more than
                     // bu_arcs arcs per unvisited vertex (0: vertex counts only)
+    int local_rl;   // local relabel after every local_rl-th round between global ones (0: off)
 };
 
 // Per-query outputs.
@@ -142,7 +143,7 @@ struct QOut {
     int mask_n;
     int status;
     int kept_front;  // kept vertices in vlist's front part
-    int pad;
+    int local_relabels;  // local relabels between global ones
 };
 
 // One capacity change, resolved to an arc (region-ordered index).

@@ -171,8 +171,11 @@ def test_batch_certify_option(rmat14):
     dict(prune_mode=0),
     dict(use_kept_cache=0),
     dict(kernel_cycles=32),
+    dict(local_relabel=1),
+    dict(local_relabel=1, gr_freq=64, gr_work_alpha=0.0, use_rm=1, force_rm=1, rm_freq=2),
+    dict(local_relabel=3, kernel_cycles=2, use_hot_sweep=1, hot_regions=2),
 ], ids=["rm", "path_push", "hot", "relabel_every_round", "rare_relabel", "ref_prune", "no_kept_cache",
-        "k32"])
+        "k32", "local_relabel", "local_relabel_rare_global", "local_relabel_every_3rd_hot"])
 def test_heuristics_stay_exact(rmat14, kw):
     n, u, v, c, g, s, t, eg = rmat14
     exp = oracle_flows(g, s, t)
@@ -180,6 +183,20 @@ def test_heuristics_stay_exact(rmat14, kw):
     assert list(eg.solve_batch(s, t, o)) == exp
     f, st = eg.certify(s[0], t[0], o)
     assert f == exp[0] and st.cut_capacity == f
+
+
+def test_local_relabel_runs_and_stays_exact(rmat14):
+    """opts.local_relabel = 1 with rare global relabels: the region-restricted,
+    depth-bounded relabel of RA:1583-1720 runs between global ones (counted
+    in the stats) and every answer still equals the oracle's Dinic."""
+    n, u, v, c, g, s, t, eg = rmat14
+    exp = oracle_flows(g, s, t)
+    o = mf.opts(local_relabel=1, gr_freq=1000, gr_work_alpha=0.0)
+    flows, sts = eg.solve_batch(s, t, o, with_stats=True)
+    assert list(flows) == exp
+    assert sum(st.local_relabels for st in sts) > 0
+    off = eg.solve_batch(s, t, mf.opts(gr_freq=1000, gr_work_alpha=0.0), with_stats=True)[1]
+    assert sum(st.local_relabels for st in off) == 0
 
 
 def test_random_small_graphs_edge_cases():
