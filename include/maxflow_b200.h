@@ -157,6 +157,23 @@ int mf_graph_export(const mf_graph *g, int32_t *row, int32_t *col, int64_t *cap,
                     int32_t *new_id, int32_t *region_start, double *score, int32_t *part);
 /* Repartition the graph into R regions (rebuilds the region-ordered CSR). */
 int mf_graph_repartition(mf_graph *g, int R);
+/* Strongly connected components of the graph's edges with capacity > 0 (as
+ * they stand after any capacity updates), computed on the device by
+ * trimming, a forward-backward search from the highest-degree vertex and
+ * colour propagation.  Replaces the offline Kosaraju tool
+ * SCC_CONTRACT/scc_contract.cpp:43-96: the same partition, but components
+ * are numbered 0 .. ncomp-1 in the order of their smallest vertex id (the
+ * tool numbers them in its depth-first discovery order).  comp (n entries,
+ * caller ids; may be NULL): component of each vertex.  m_contracted: arcs
+ * of the contracted graph, read with mf_graph_scc_contracted.  Not while a
+ * server changes this graph's capacities. */
+int mf_graph_scc(mf_graph *g, int32_t *comp, int32_t *ncomp, long long *m_contracted);
+/* The contracted graph of the last mf_graph_scc on g (scc_contract.cpp:
+ * 98-128): one arc per ordered pair of distinct components joined by an
+ * edge, its capacity the sum of theirs, in increasing (cu, cv).  max: room
+ * in each array; MF_ERR_ARG when it is too small or mf_graph_scc has not
+ * run. */
+int mf_graph_scc_contracted(const mf_graph *g, int32_t *cu, int32_t *cv, int64_t *cap, long long max);
 
 /* ---- solves ----------------------------------------------------------- */
 

@@ -150,6 +150,22 @@ class Graph:
     def repartition(self, R):
         _check(lib.mf_graph_repartition(self._h, int(R)))
 
+    def scc(self):
+        """Strongly connected components of the edges with capacity > 0,
+        computed on the GPU (SCC_CONTRACT/scc_contract.cpp's partition).
+        Returns (comp, ncomp, (cu, cv, cap)): each vertex's component
+        (numbered by smallest vertex id) and the contracted graph's arcs in
+        increasing (cu, cv)."""
+        n = self.info[0]
+        comp = np.zeros(max(n, 1), np.int32)
+        nc, mc = C.c_int32(), C.c_longlong()
+        _check(lib.mf_graph_scc(self._h, _p(comp, C.c_int32), C.byref(nc), C.byref(mc)))
+        k = mc.value
+        cu, cv, cc = np.zeros(max(k, 1), np.int32), np.zeros(max(k, 1), np.int32), np.zeros(max(k, 1), np.int64)
+        _check(lib.mf_graph_scc_contracted(self._h, _p(cu, C.c_int32), _p(cv, C.c_int32), _p(cc, C.c_int64),
+                                           max(k, 1)))
+        return comp[:n], nc.value, (cu[:k], cv[:k], cc[:k])
+
     def solve(self, s, t, o=None):
         f = C.c_int64()
         st = MfStats()

@@ -94,6 +94,8 @@ SIGNATURES = {
     "mf_graph_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
     "mf_graph_export": (C.c_int, [C.c_void_p, i32p, i32p, i64p, i32p, i32p, i32p, f64p, i32p]),
     "mf_graph_repartition": (C.c_int, [C.c_void_p, C.c_int]),
+    "mf_graph_scc": (C.c_int, [C.c_void_p, i32p, C.POINTER(C.c_int32), C.POINTER(C.c_longlong)]),
+    "mf_graph_scc_contracted": (C.c_int, [C.c_void_p, i32p, i32p, i64p, C.c_longlong]),
     "mf_solve": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(MfOpts), i64p, C.POINTER(MfStats)]),
     "mf_solve_batch": (C.c_int, [C.c_void_p, C.c_int, i32p, i32p, C.POINTER(MfOpts), i64p, C.POINTER(MfStats)]),
     "mf_solve_batch_override": (C.c_int, [C.c_void_p, C.c_int, i32p, i32p, C.c_longlong, i32p, i32p, i64p, C.POINTER(MfOpts), i64p, C.POINTER(MfStats)]),

@@ -28,6 +28,7 @@
 #include "../../include/maxflow_b200.h"
 #include "mf_alloc.h"
 #include "mf_build.cuh"
+#include "mf_scc.cuh"
 #include "mf_solver.cuh"
 
 namespace {
@@ -285,6 +286,8 @@ struct mf_graph {
     std::vector<int> old_id;  // internal id -> caller id
     std::vector<double> score_caller;
     std::vector<int> part_caller;
+    SccOut scc;  // the last mf_graph_scc result (contracted arcs for mf_graph_scc_contracted)
+    bool scc_done = false;
     // region-ordered device CSR
     int *row = nullptr, *col = nullptr, *rev = nullptr, *region_of = nullptr,
         *region_start = nullptr;
@@ -1130,6 +1133,31 @@ int mf_graph_info(const mf_graph *g, int *n, long long *arcs, int *R) {
     if (n) *n = g->n;
     if (arcs) *arcs = g->arcs;
     if (R) *R = g->R;
+    return MF_OK;
+}
+
+int mf_graph_scc(mf_graph *g, int32_t *comp, int32_t *ncomp, long long *m_contracted) {
+    if (!g) return fail(MF_ERR_ARG, "graph is NULL");
+    SccIn in{g->n, g->arcs, g->row, g->col, g->rev, g->cap, g->new_id.data(), g->old_id.data()};
+    g->scc_done = false;
+    CK(mf_scc_run(in, g->stream, g->scc));
+    g->scc_done = true;
+    if (comp) memcpy(comp, g->scc.comp.data(), sizeof(int) * (size_t)g->n);
+    if (ncomp) *ncomp = g->scc.ncomp;
+    if (m_contracted) *m_contracted = (long long)g->scc.cu.size();
+    return MF_OK;
+}
+
+int mf_graph_scc_contracted(const mf_graph *g, int32_t *cu, int32_t *cv, int64_t *cap, long long max) {
+    if (!g) return fail(MF_ERR_ARG, "graph is NULL");
+    if (!g->scc_done) return fail(MF_ERR_ARG, "mf_graph_scc has not run on this graph");
+    const size_t K = g->scc.cu.size();
+    if (max < (long long)K) return fail(MF_ERR_ARG, "room for %lld contracted arcs, %zu needed", max, K);
+    if (K == 0) return MF_OK;
+    if (!cu || !cv || !cap) return fail(MF_ERR_ARG, "NULL output array");
+    memcpy(cu, g->scc.cu.data(), sizeof(int) * K);
+    memcpy(cv, g->scc.cv.data(), sizeof(int) * K);
+    memcpy(cap, g->scc.cap.data(), sizeof(int64_t) * K);
     return MF_OK;
 }
 

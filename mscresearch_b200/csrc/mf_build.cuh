@@ -53,5 +53,10 @@ struct TextEdges {
 cudaError_t mf_device_csr(int n, i64 m, const int *u, const int *v, const i64 *c, cudaStream_t st,
                           DevCsr &out);
 void mf_free_dev_csr(DevCsr &c);
+// Stable LSD radix sort (8-bit digits) of N (key, val) pairs by key in
+// [0, key_max]; key2 / val2 are scratch of N entries.  The sorted pairs end
+// in key / val (the pointers are swapped as the passes require).
+cudaError_t mf_radix_sort_pairs(int N, int key_max, int *&key, int *&val, int *&key2, int *&val2,
+                                cudaStream_t st);
 cudaError_t mf_parse_graph_text(const unsigned char *txt, i64 S, cudaStream_t st, TextEdges &out);
 void mf_free_text_edges(TextEdges &t);

@@ -300,6 +300,28 @@ cudaError_t mf_device_csr(int n, i64 m, const int *u, const int *v, const i64 *c
     return e;
 }
 
+cudaError_t mf_radix_sort_pairs(int N, int key_max, int *&key, int *&val, int *&key2, int *&val2,
+                                cudaStream_t st) {
+    if (N <= 0 || key_max <= 0) return cudaSuccess;
+    const int nchunks = (N + RS_CHUNK - 1) / RS_CHUNK;
+    const int nbins = RS_BINS * nchunks;
+    DevScope tmp;
+    int *cnt = nullptr, *off = nullptr, *stmp = nullptr;
+    cudaError_t e;
+    if ((e = tmp.alloc(&cnt, sizeof(int) * (size_t)nbins)) || (e = tmp.alloc(&off, sizeof(int) * ((size_t)nbins + 1))) ||
+        (e = tmp.alloc(&stmp, sizeof(int) * ((size_t)nbins / 1024 + 2))))
+        return e;
+    for (unsigned x = (unsigned)key_max, shift = 0; x; x >>= 8, shift += 8) {
+        k_rs_hist<<<nchunks, 512, 0, st>>>(N, key, (int)shift, nchunks, cnt);
+        mf_exclusive_scan(nbins, cnt, off, stmp, st);
+        k_rs_place<<<nchunks, 32 * RS_WARPS, 0, st>>>(N, key, val, (int)shift, nchunks, off, key2, val2);
+        std::swap(key, key2);
+        std::swap(val, val2);
+    }
+    if ((e = cudaGetLastError())) return e;
+    return cudaStreamSynchronize(st);  // the scratch is freed on return
+}
+
 void mf_free_dev_csr(DevCsr &c) {
     mf_dfree(c.row);
     mf_dfree(c.col);

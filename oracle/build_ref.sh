@@ -1,8 +1,10 @@
 #!/usr/bin/env bash
 # Compiles the reference's own CUDA solver from its sources where they lie
 # (read-only) into oracle/_ref/ra_ref, for sm_100a, with the device shim
-# above.  Nothing is copied out of the reference tree; the only output is the
-# executable.  Test infrastructure only: the engine never runs it.
+# above, and its host-only SCC contraction tool (SCC_CONTRACT/scc_contract.cpp)
+# into oracle/_ref/scc_contract.  Nothing is copied out of the reference
+# tree; the only outputs are the executables.  Test infrastructure only: the
+# engine never runs them.
 #   usage: oracle/build_ref.sh REFERENCE_ROOT   (or MF_REFERENCE_ROOT set)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
@@ -21,3 +23,8 @@ NVCC="${NVCC:-nvcc}"
 "$NVCC" -O3 -gencode arch=compute_100a,code=sm_100a -cudart shared \
   -o "$HERE/_ref/ra_ref" "$SRC" "$HERE/ref_device_shim.c" -ldl
 echo "build_ref: built $HERE/_ref/ra_ref"
+SCC_SRC="$REF/SCC_CONTRACT/scc_contract.cpp"
+if [ -f "$SCC_SRC" ]; then
+  "${CXX:-g++}" -O3 -std=c++17 -o "$HERE/_ref/scc_contract" "$SCC_SRC"
+  echo "build_ref: built $HERE/_ref/scc_contract"
+fi

@@ -12,6 +12,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "ra_ref")
+REF_SCC_BIN = os.path.join(HERE, "_ref", "scc_contract")
 
 
 def build():
@@ -19,7 +20,7 @@ def build():
 
 
 if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(
-        os.path.getmtime(os.path.join(HERE, f)) for f in ("oracle.c", "gen.c")):
+        os.path.getmtime(os.path.join(HERE, f)) for f in ("oracle.c", "gen.c", "scc.c")):
     build()
 _lib = C.CDLL(LIB)
 
@@ -50,6 +51,8 @@ _sig = {
     "gn_queries_hub": (C.c_int, [C.c_int, C.c_longlong, i32p, i32p, C.c_int, C.c_int, C.c_uint64, i32p, i32p]),
     "gn_write_graph_txt": (C.c_int, [C.c_char_p, C.c_int, C.c_longlong, i32p, i32p, i64p]),
     "gn_write_test_txt": (C.c_int, [C.c_char_p, C.c_int, i32p, i32p]),
+    "or_scc_kosaraju": (C.c_int, [C.c_int, C.c_longlong, i32p, i32p, i64p, i32p]),
+    "or_scc_contract": (C.c_longlong, [C.c_int, C.c_longlong, i32p, i32p, i64p, i32p, i32p, i32p, i64p]),
 }
 for _n, (_r, _a) in _sig.items():
     _f = getattr(_lib, _n)
@@ -264,3 +267,38 @@ def write_test_txt(path, s, t):
     s, t = _c(s, np.int32), _c(t, np.int32)
     if _lib.gn_write_test_txt(path.encode(), len(s), _p(s, C.c_int32), _p(t, C.c_int32)) != 0:
         raise IOError(path)
+
+
+def scc_kosaraju(n, u, v, cap):
+    """Component of every vertex (0-based, Kosaraju's discovery order;
+    SCC_CONTRACT/scc_contract.cpp:43-96) and the number of components."""
+    u, v, cap = _c(u, np.int32), _c(v, np.int32), _c(cap, np.int64)
+    comp = np.zeros(max(n, 1), np.int32)
+    k = _lib.or_scc_kosaraju(int(n), len(u), _p(u, C.c_int32), _p(v, C.c_int32), _p(cap, C.c_int64),
+                             _p(comp, C.c_int32))
+    if k < 0:
+        raise MemoryError("or_scc_kosaraju")
+    return comp[:n].copy(), int(k)
+
+
+def scc_contract(n, u, v, cap, comp):
+    """Contracted arcs (cu, cv, summed cap) in increasing (cu, cv) for the
+    labelling comp (SCC_CONTRACT/scc_contract.cpp:98-128)."""
+    u, v, cap, comp = _c(u, np.int32), _c(v, np.int32), _c(cap, np.int64), _c(comp, np.int32)
+    m = max(len(u), 1)
+    cu, cv, cc = np.zeros(m, np.int32), np.zeros(m, np.int32), np.zeros(m, np.int64)
+    k = _lib.or_scc_contract(int(n), len(u), _p(u, C.c_int32), _p(v, C.c_int32), _p(cap, C.c_int64),
+                             _p(comp, C.c_int32), _p(cu, C.c_int32), _p(cv, C.c_int32), _p(cc, C.c_int64))
+    if k < 0:
+        raise MemoryError("or_scc_contract")
+    return cu[:k].copy(), cv[:k].copy(), cc[:k].copy()
+
+
+def write_scc_files(path, n, comp, ncomp, cu, cv, cc):
+    """The reference tool's two outputs: path ("n' m'" then "cu cv cap"
+    lines, 1-based) and path + ".map" ("vertex component" lines, 1-based)."""
+    with open(path, "w") as f:
+        f.write("%d %d\n" % (ncomp, len(cu)))
+        f.writelines("%d %d %d\n" % (a + 1, b + 1, c) for a, b, c in zip(cu.tolist(), cv.tolist(), cc.tolist()))
+    with open(path + ".map", "w") as f:
+        f.writelines("%d %d\n" % (i + 1, x + 1) for i, x in enumerate(np.asarray(comp)[:n].tolist()))
