@@ -20,7 +20,12 @@ times (res_mt.txt, integer ms, prune included, RA:2808).
 Multi-GPU (torchrun): queries shard across ranks (one graph replica per
 GPU, no data-path collective); timing is the max over ranks.
 
-Other workloads (not the headline line):
+A full 1-GPU headline run also runs the three other workloads below, each
+in its own process after the headline measurement, and appends their
+figures to its line as "other_workloads" (--no-other skips them, and so
+does --no-cpu, which marks a measurement-only run such as a profiling one).
+
+Other workloads (their own lines when run alone):
   --workload mix       8 device-resident R-MAT graphs (2^14..2^20) served to
                        Poisson-arriving requests, against the plain loop;
   --workload gridsets  a 2048 x 2048 segmentation grid, 64 queries that vary
@@ -317,6 +322,8 @@ def run_engine(args):
         assert [int(flows[i]) for i in idx] == [int(x) for x in cflows], "engine differs from oracle"
         res["cpu_baseline"] = cb
         res["oracle_agreement"] = "%d of %d sampled answers equal to the oracle's Dinic" % (len(idx), len(idx))
+    if rank == 0 and world == 1 and not args.no_other and not args.no_cpu:
+        res["other_workloads"] = other_workloads(args)
     if rank == 0:
         print(json.dumps(res), flush=True)
     if args.dump and rank == 0:
@@ -336,6 +343,35 @@ def run_engine(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+OTHER_KEYS = {
+    "gridsets": ["metric", "value", "unit", "ms_per_step", "e2e", "roofline", "oracle_agreement"],
+    "dynamic": ["metric", "value", "unit", "initial_exact", "batches"],
+    "mix": ["metric", "value", "unit", "plain", "served", "served_with_updates"],
+}
+
+
+def other_workloads(args):
+    """The three other workload shapes, each run as its own process after the
+    headline measurement (outside its timed region; a failure there is
+    recorded, not raised): their own JSON lines, trimmed to the figures."""
+    out = {}
+    for wl, keys in OTHER_KEYS.items():
+        cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--workload", wl, "--no-cpu"]
+        t0 = time.perf_counter()
+        try:
+            p = subprocess.run(cmd, capture_output=True, text=True, timeout=args.other_timeout)
+            lines = [x for x in p.stdout.splitlines() if x.startswith("{")]
+            if p.returncode != 0 or not lines:
+                out[wl] = {"error": "exit %d: %s" % (p.returncode, (p.stderr or "").strip()[-300:])}
+                continue
+            d = json.loads(lines[-1])
+            out[wl] = {k: d[k] for k in keys if k in d}
+        except subprocess.TimeoutExpired:
+            out[wl] = {"error": "no result within %d s" % args.other_timeout}
+        out[wl]["wall_s"] = round(time.perf_counter() - t0, 1)
+    return out
 
 
 def serve_run(mf, g, s, t, flows, o, rate, nreq=256, seed=0):
@@ -832,6 +868,10 @@ def main():
     ap.add_argument("--mix-requests", type=int, default=512)
     ap.add_argument("--mix-update-share", type=float, default=0.1,
                     help="mix: share of requests that are capacity-update batches in the extra served run")
+    ap.add_argument("--no-other", action="store_true",
+                    help="headline run: skip the other workloads (gridsets, dynamic, mix) that a full 1-GPU "
+                         "run appends to its line as other_workloads (--no-cpu skips them too)")
+    ap.add_argument("--other-timeout", type=int, default=420, help="seconds allowed to each other workload")
     ap.add_argument("--mix-rates", type=float, nargs="+", default=[0.5, 1.0, 2.0, 4.0],
                     help="arrival rates as multiples of the plain loop's throughput")
     args = ap.parse_args()
