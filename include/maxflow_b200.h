@@ -251,8 +251,8 @@ int mf_certify(mf_graph *g, int32_t s, int32_t t, const mf_opts *opts, int64_t *
  * rejected with MF_ERR_ARG.  The call makes no cudaMalloc / cudaFree or
  * other allocating call.  Its first call on a device resolves the array's
  * device address and zeroes it (once per device, also when several host
- * threads make their first call together); make that first call before any
- * stream capture.  The address is kept for the process's life, so a
+ * threads make their first call together).  The address is kept for the
+ * process's life, so a
  * cudaDeviceReset of that device is not supported afterwards.  Options are
  * resolved and device statuses reported exactly as mf_solve does.  Every
  * call waits for its stream to finish its work before returning.  Every call
