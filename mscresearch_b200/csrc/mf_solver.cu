@@ -58,6 +58,7 @@
 #define CNT_ACT 40    // global relabel: active vertices to label
 #define CNT_FOUND 41  // global relabel: active vertices labelled so far
 #define CNT_FARCS 42  // global relabel: arcs of the vertices labelled so far
+#define CNT_OPENED 43 // repair: an update opened a residual arc or cancelled flow
 #define CNT_Q 8      // query handed to the group
 #define CNT_FLAG 9   // misc uniform flag
 #define CNT_RS 10    // serving: request source / sink / graph
@@ -1918,8 +1919,12 @@ __device__ bool rm_pass(QCtx &c, int nv, unsigned M, int hlo, int hhi, int s, in
 // of discharge (+ hot sweep, path push, RM, stagnation control) -> relabel
 // ... until a relabel finds nothing to do.  start_phase PH_A: maximum preflow
 // for (s,t); PH_C: return excess to s.
+// dead_in: the dead-mark state a warm start inherits (0: none; 1: heights
+// above n are dead marks; 2: also the visited bitmap of a complete search,
+// see repair); dead_out (may be NULL): the state this call leaves, for the
+// next warm start.
 __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsigned M,
-                           int start_phase, QOut &qo, int &status) {
+                           int start_phase, QOut &qo, int &status, int dead_in = 0, int *dead_out = nullptr) {
     const int n = c.n;
     int phase = start_phase;
     int K = o.K;
@@ -1934,8 +1939,9 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
     int gr_depth = 0;  // levels of the last global relabel's search
     // dead marks (see global_relabel): phase A only, from the second relabel
     // of the phase on; new ones only after a complete search
-    int dead_phase = -1;      // phase of the last relabel (-1: none in this call)
-    bool last_complete = false;
+    int dead_phase = (dead_in > 0 && start_phase == PH_A && o.gr_stop) ? PH_A : -1;  // phase of the last relabel
+    bool last_complete = dead_phase == PH_A && dead_in == 2;
+    if (dead_out) *dead_out = 0;
     for (;;) {
         int sinkv = (phase == PH_A) ? t : (phase == PH_B ? -1 : s);
         int blockv = (phase == PH_C) ? t : s;
@@ -1961,7 +1967,10 @@ __device__ bool run_phases(QCtx &c, const KOpts &o, int s, int t, int nv, unsign
         qo.relabels++;
         if (naf + nab == 0) {
             if (phase == PH_A) {
-                if (nd == 0) return true;
+                if (nd == 0) {
+                    if (dead_out && o.gr_stop) *dead_out = last_complete ? 2 : 1;
+                    return true;
+                }
                 phase = PH_B;
                 qo.deficit_phases++;
                 continue;
@@ -2274,7 +2283,19 @@ __device__ bool write_full_residual(QCtx &c, unsigned M, i64 *out) {
 // re-saturates.
 __device__ bool repair_deltas(QCtx &c, const KParams &p, unsigned Mn, unsigned O);
 
-__device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int &nv, bool &t_reach) {
+// dead_in (out): the dead-mark state the repaired solve may start from.
+// The previous solve left meta[7] (see run_phases): its dead vertices (and,
+// with 2, the kept vertices its last, complete search did not reach) could
+// reach neither the sink nor a deficit.  A vertex's residual reach grows
+// only through an arc whose residual goes from 0 to positive, and a new
+// deficit appears only where flow is cancelled; when no update of the batch
+// on the kept arcs does either, those vertices still reach neither (the
+// repair's preflow only opens arcs into the source, which phase A never
+// crosses), so the marks carry over and the first relabel need not search
+// for them.  Otherwise, and after a re-prune, the solve starts clean.
+__device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int &nv, bool &t_reach,
+                       int &dead_in) {
+    dead_in = 0;
     int *meta = c.st.meta;
     int vf_old = ldcg(&meta[4]);
     int nv_old = ldcg(&meta[1]);
@@ -2305,8 +2326,10 @@ __device__ bool repair(QCtx &c, const KParams &p, int s, int t, unsigned &M, int
         t_reach = ldcg(&meta[5]) != 0;
         nv = nv_old;
         if (c.leader) c.st.acc[ACC_TOT + T_MASKARCS] = ldcg(&meta[6]);
+        if (c.leader) c.st.cnt[CNT_OPENED] = 0;
         if (!c.sync()) return false;
         if (!repair_deltas(c, p, Mn, O)) return false;
+        if (ldcg(&c.st.cnt[CNT_OPENED]) == 0) dead_in = ldcg(&meta[7]);
         M = Mn;
         if (!t_reach) return true;
         return preflow(c, s);
@@ -2437,7 +2460,9 @@ __device__ bool repair_deltas(QCtx &c, const KParams &p, unsigned Mn, unsigned O
         i64 f = u.old_cap - r;
         if (f <= u.new_cap) {
             atomic_add_i64(&c.st.res[e], u.new_cap - u.old_cap);
+            if (r <= 0 && u.new_cap > u.old_cap) atomicOr(&c.st.cnt[CNT_OPENED], 1);  // x -> w opened
         } else {
+            atomicOr(&c.st.cnt[CNT_OPENED], 1);  // flow cancelled: a deficit at w
             i64 over = f - u.new_cap;
             atomic_add_i64(&c.st.res[e], -r);
             atomic_add_i64(&c.st.res[re], -over);
@@ -2474,8 +2499,9 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
     unsigned M = 0;
     int nv = 0;
     bool t_reach = false;
+    int dead_in = 0, dead_out = 0;  // dead-mark state carried between warm starts (run_phases)
     if (p.mode == KM_REPAIR) {
-        if (!repair(c, p, s, t, M, nv, t_reach)) return;
+        if (!repair(c, p, s, t, M, nv, t_reach, dead_in)) return;
     } else {
         unsigned S = ++c.clock;
         M = ++c.clock;
@@ -2599,9 +2625,10 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
                 hd[v] = (ldcg(&c.st.mark[v]) >= M) ? ldcg(&c.st.h[v]) : c.n;
             if (!c.sync()) return;
         } else {
-            if (!run_phases(c, o, s, t, nv, M, PH_A, qo, status)) return;
+            if (!run_phases(c, o, s, t, nv, M, PH_A, qo, status, dead_in, &dead_out)) return;
             flow = ldcg(&c.st.ex[t]);
             if (p.mode == KM_CERTIFY && status == MFD_OK) {
+                dead_out = 0;
                 if (!run_phases(c, o, s, t, nv, M, PH_C, qo, status)) return;
                 if (status == MFD_OK && !certify(c, s, t, nv, M, flow, qo, status)) return;
             }
@@ -2654,6 +2681,7 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
         c.st.meta[4] = c.vf;
         c.st.meta[5] = t_reach ? 1 : 0;
         c.st.meta[6] = (int)min(tot[T_MASKARCS], (i64)INT_MAX);
+        c.st.meta[7] = status == MFD_OK ? dead_out : 0;
     }
     c.sync();
 }

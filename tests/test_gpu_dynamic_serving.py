@@ -67,6 +67,32 @@ def test_session_incremental_equals_fresh(scale, policy, monkeypatch):
         ss.close()
 
 
+@pytest.mark.parametrize("scale", [12, 15])
+def test_session_many_small_batches_equal_oracle(scale):
+    """Many small batches in a row (decreases and increases of 1..5): batches
+    that open no residual arc and cancel no flow on a query's kept arcs let
+    its repair keep the previous solve's dead marks; every answer after every
+    batch equals the oracle's Dinic on the updated graph."""
+    n = 1 << scale
+    u, v, c = mf.gen_rmat(scale, 16 * n, seed=50 + scale)
+    s, t = mf.gen_queries_hub(n, u, v, 8, 8, seed=9)
+    g = O.build_csr(n, u, v, c)
+    fwd = g.cap > 0
+    rng = np.random.default_rng(100 + scale)
+    with mf.Graph.from_edges(n, u, v, c, R=32) as eg:
+        with mf.Session(eg, s, t) as ss:
+            assert list(ss.solve()) == [O.dinic(g, a, b) for a, b in zip(s, t)]
+            for b in range(16):
+                k = int(rng.integers(1, 24))
+                idx = rng.integers(0, len(u), k)
+                sign = -1 if b % 3 == 0 else (1 if b % 3 == 1 else 0)
+                mag = rng.integers(1, 6, k)
+                d = mag * (sign if sign else np.where(rng.random(k) < 0.5, -1, 1))
+                fr = ss.update(u[idx], v[idx], d)
+                apply_updates_oracle(g, fwd, u[idx], v[idx], d)
+                assert list(fr) == [O.dinic(g, a, b2) for a, b2 in zip(s, t)], b
+
+
 def test_update_caps_hub_tail_parallel_arcs():
     """Updates on (hub, leaf) pairs are resolved through the leaf's shorter
     list; with parallel edges the first forward arc in input order must take
