@@ -614,6 +614,15 @@ def run_gridsets(args):
             best_ms, best_R = ms, r
     if g.info[2] != best_R:
         g.repartition(best_R)
+    # and the prune: fwd(s) & bwd(t) (default) or every vertex kept
+    o2 = type(best_o).from_buffer_copy(best_o)
+    o2.prune_mode = 2
+    g.solve_batch_override(s[:smp], t[:smp], tu, tv, caps[:smp], o2)
+    ms = est(g.last_device_ms, o2.group_ctas)
+    tune.append({"gr_freq": o2.gr_freq, "gr_alpha": o2.gr_work_alpha, "G": o2.group_ctas, "R": best_R,
+                 "prune_mode": 2, "batch_ms_est": round(ms, 2)})
+    if ms < best_ms:
+        best_o, best_ms = o2, ms
     o = best_o
     for _ in range(args.warmup):
         g.solve_batch_override(s, t, tu, tv, caps, o)
@@ -639,7 +648,7 @@ def run_gridsets(args):
                    "per-query terminal masks, weights U[0,255])" % (W, W),
            "config": {"workload": "grid%d_%dsets" % (W, nq), "n": n, "arcs": arcs, "queries": nq,
                       "R": best_R, "gr_freq": o.gr_freq, "gr_alpha": o.gr_work_alpha, "group_ctas": o.group_ctas,
-                      "overridden_arcs": len(tu), "tuning": tune,
+                      "prune_mode": o.prune_mode, "overridden_arcs": len(tu), "tuning": tune,
                       "l2": "inputs larger than L2 (capacities %.2f GB)" % (caps.nbytes / 1e9)},
            "e2e": {"value": round(nq / (float(np.mean(e2e_ms)) / 1e3), 3), "unit": "queries/s",
                    "h2d_bytes_per_step": int(caps.nbytes + 8 * len(tu) + 8 * nq),

@@ -50,7 +50,8 @@ typedef struct mf_opts {
                               downhill arc); 0 = 8 */
     int gr_freq;           /* rounds between global relabels at most (default 16; RA:1466 uses 128) */
     double gr_work_alpha;  /* also relabel once scanned arcs exceed alpha x mask arcs (0 = off) */
-    int prune_mode;        /* 0: RA:1391-1445 mask (fwd(s) & undirected comp(t)); 1: fwd(s) & bwd(t) (default) */
+    int prune_mode;        /* 0: RA:1391-1445 mask (fwd(s) & undirected comp(t)); 1: fwd(s) & bwd(t) (default);
+                              2: no prune, every vertex kept (graphs whose terminals touch most vertices) */
     int path_push_switch;  /* active count at or below which path-push starts (RA:1480) */
     int max_path_len;      /* path-push hop limit (RA:1481) */
     int use_path_push;     /* 1 = enable sparse-phase path push (RA:1765-1831) */

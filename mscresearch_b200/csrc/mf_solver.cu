@@ -2532,6 +2532,20 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
         } else if (kc_case == 2) {
             if (!prune_ext(c, s, t, S, M, nv)) return;
             t_reach = true;
+        } else if (o.prune_mode == 2) {
+            // no prune: every vertex is kept.  The kept set only has to
+            // contain fwd(s) & bwd(t); where the terminals touch most of the
+            // graph (segmentation grids) the two searches cost more than the
+            // few extra vertices, which no push reaches or no relabel labels
+            int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+            for (int v = gt; v < c.n; v += gT) {
+                c.st.vlist[v] = v;
+                c.st.mark[v] = M;
+            }
+            nv = c.n;
+            c.vf = c.n;
+            t_reach = true;
+            if (!c.sync()) return;
         } else if (!prune(c, s, t, o.prune_mode, S, M, nv, t_reach, use_kc ? g.kc_fb : nullptr)) {
             return;
         }

@@ -169,12 +169,13 @@ def test_batch_certify_option(rmat14):
     dict(use_rm=0, use_path_push=0, use_hot_sweep=0, gr_freq=1, gr_work_alpha=0.0),
     dict(kernel_cycles=64, gr_freq=100000, gr_work_alpha=0.0),
     dict(prune_mode=0),
+    dict(prune_mode=2),
     dict(use_kept_cache=0),
     dict(kernel_cycles=32),
     dict(local_relabel=1),
     dict(local_relabel=1, gr_freq=64, gr_work_alpha=0.0, use_rm=1, force_rm=1, rm_freq=2),
     dict(local_relabel=3, kernel_cycles=2, use_hot_sweep=1, hot_regions=2),
-], ids=["rm", "path_push", "hot", "relabel_every_round", "rare_relabel", "ref_prune", "no_kept_cache",
+], ids=["rm", "path_push", "hot", "relabel_every_round", "rare_relabel", "ref_prune", "no_prune", "no_kept_cache",
         "k32", "local_relabel", "local_relabel_rare_global", "local_relabel_every_3rd_hot"])
 def test_heuristics_stay_exact(rmat14, kw):
     n, u, v, c, g, s, t, eg = rmat14
@@ -280,6 +281,9 @@ def test_batch_override_terminal_sets():
     s, t = [S] * nq, [T] * nq
     with mf.Graph.from_edges(n, gu, gv, gc, R=16) as eg:
         assert list(eg.solve_batch_override(s, t, tu, tv, caps)) == exp
+        # without the prune (every vertex kept)
+        assert list(eg.solve_batch_override(s, t, tu, tv, caps, mf.opts(prune_mode=2))) == exp
+        assert list(eg.solve_batch_override([T, T], [S, S], tu, tv, caps[:2], mf.opts(prune_mode=2))) == [0, 0]
         # all capacities at the graph's own values: the plain batch
         full = np.tile(gc[nbr:], (2, 1))
         assert list(eg.solve_batch_override([S, 7], [T, T], tu, tv, full)) == list(eg.solve_batch([S, 7], [T, T]))
