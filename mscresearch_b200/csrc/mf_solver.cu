@@ -2616,6 +2616,34 @@ __device__ void solve_query(QCtx &c, const KParams &p, int q, int s, int t) {
                 if (c.lane == 0 && c.gw == 0) c.w_verts += nv;
                 if (!c.sync()) return;
                 if (kc_case == 2 && !fix_extra_arcs(c, M, nv)) return;
+            } else if (o.prune_mode == 2 && nv == c.n) {
+                // every vertex kept: the initial residuals are the
+                // capacities, copied whole like the cached image (no per-arc
+                // test of the head)
+                const i64 A = ldro(&c.row[c.n]);
+                int gt = c.crank * blockDim.x + threadIdx.x, gT = c.G * blockDim.x;
+                for (int v = gt; v < c.n; v += gT) {
+                    c.st.ex[v] = 0;
+                    c.st.h[v] = 0;
+                }
+                const bool vec = ((reinterpret_cast<uintptr_t>(c.cap) | reinterpret_cast<uintptr_t>(c.st.res)) & 15) == 0;
+                const i64 nvec = vec ? (A >> 1) : 0;
+                const longlong2 *src = reinterpret_cast<const longlong2 *>(c.cap);
+                longlong2 *dst = reinterpret_cast<longlong2 *>(c.st.res);
+                i64 k = gt;
+                for (; k + 3 * (i64)gT < nvec; k += 4 * (i64)gT) {
+                    const longlong2 x0 = ldcap2(&src[k]), x1 = ldcap2(&src[k + gT]);
+                    const longlong2 x2 = ldcap2(&src[k + 2 * (i64)gT]), x3 = ldcap2(&src[k + 3 * (i64)gT]);
+                    dst[k] = x0;
+                    dst[k + gT] = x1;
+                    dst[k + 2 * (i64)gT] = x2;
+                    dst[k + 3 * (i64)gT] = x3;
+                }
+                for (; k < nvec; k += gT) dst[k] = ldcap2(&src[k]);
+                for (i64 e = 2 * nvec + gt; e < A; e += gT) c.st.res[e] = ldcap(&c.cap[e]);
+                if (c.leader) c.st.acc[ACC_TOT + T_MASKARCS] = A;
+                if (c.lane == 0 && c.gw == 0) c.w_verts += nv;
+                if (!c.sync()) return;
             } else if (!init_state(c, nv, M)) {
                 return;
             }
