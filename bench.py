@@ -571,8 +571,9 @@ def run_gridsets(args):
     terminal set: each of the nq queries keeps S->p or p->T per pixel (seeded
     mask) at a weight uniform in [0, 255].  One step = one
     mf_solve_batch_override launch over all sets, the terminal capacities
-    resident on the device; gr_freq / gr_work_alpha and R are tuned on a
-    sample of the sets before timing."""
+    resident on the device; gr_freq / gr_work_alpha, the group size, R and
+    the prune are tuned on a sample of the sets before timing (R orders the
+    vertices: within a region they keep the input's row-major order)."""
     rank = int(os.environ.get("RANK", "0"))
     import torch
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
@@ -604,25 +605,24 @@ def run_gridsets(args):
         tune.append({"gr_freq": gf, "gr_alpha": al, "G": G, "R": R, "batch_ms_est": round(ms, 2)})
         if best_ms is None or ms < best_ms:
             best_o, best_ms = o, ms
-    for r in (32, 512):
-        g.repartition(r)
-        g.solve_batch_override(s[:smp], t[:smp], tu, tv, caps[:smp], best_o)
-        ms = est(g.last_device_ms, best_o.group_ctas)
-        tune.append({"gr_freq": best_o.gr_freq, "gr_alpha": best_o.gr_work_alpha, "G": best_o.group_ctas, "R": r,
-                     "batch_ms_est": round(ms, 2)})
-        if ms < best_ms:
-            best_ms, best_R = ms, r
+    # then R (it orders the vertices) with each prune: fwd(s) & bwd(t)
+    # (default) or every vertex kept
+    for r in (R, 1, 8, 32, 512):
+        if g.info[2] != r:
+            g.repartition(r)
+        for pm in (1, 2):
+            if r == R and pm == best_o.prune_mode:
+                continue  # measured above
+            o2 = type(best_o).from_buffer_copy(best_o)
+            o2.prune_mode = pm
+            g.solve_batch_override(s[:smp], t[:smp], tu, tv, caps[:smp], o2)
+            ms = est(g.last_device_ms, o2.group_ctas)
+            tune.append({"gr_freq": o2.gr_freq, "gr_alpha": o2.gr_work_alpha, "G": o2.group_ctas, "R": r,
+                         "prune_mode": pm, "batch_ms_est": round(ms, 2)})
+            if ms < best_ms:
+                best_o, best_ms, best_R = o2, ms, r
     if g.info[2] != best_R:
         g.repartition(best_R)
-    # and the prune: fwd(s) & bwd(t) (default) or every vertex kept
-    o2 = type(best_o).from_buffer_copy(best_o)
-    o2.prune_mode = 2
-    g.solve_batch_override(s[:smp], t[:smp], tu, tv, caps[:smp], o2)
-    ms = est(g.last_device_ms, o2.group_ctas)
-    tune.append({"gr_freq": o2.gr_freq, "gr_alpha": o2.gr_work_alpha, "G": o2.group_ctas, "R": best_R,
-                 "prune_mode": 2, "batch_ms_est": round(ms, 2)})
-    if ms < best_ms:
-        best_o, best_ms = o2, ms
     o = best_o
     for _ in range(args.warmup):
         g.solve_batch_override(s, t, tu, tv, caps, o)
