@@ -263,3 +263,69 @@ def test_partition_against_reference_libm_log():
             print("partition %s R=%d: %d of %d vertices in another region (max score rel. diff %.1e)"
                   % (name, R, diff, g.n, rel.max()))
             assert diff == 0, (name, R, diff)
+
+
+def _apply_to_residual(g, res, cap, e, delta):
+    """One capacity change on forward arc e, as a repair applies it to the
+    resident residual: returns (opened, cancelled)."""
+    old = int(cap[e])
+    new = max(0, old + int(delta))
+    r = int(res[e])
+    fl = old - r
+    opened = cancelled = False
+    if fl <= new:
+        res[e] = r + (new - old)
+        opened = r <= 0 and new > old
+    else:
+        res[e] = 0
+        res[g.rev[e]] -= fl - new
+        cancelled = True
+    cap[e] = new
+    return opened, cancelled
+
+
+def test_unreachable_set_survives_batches_that_open_no_arc():
+    """The argument behind carrying dead marks into a repair: after a max
+    flow, the vertices that cannot reach t in the residual graph (s blocked)
+    still cannot after a batch of capacity changes that opens no residual arc
+    (0 to positive) and cancels no flow.  And the condition is needed: one
+    opened arc out of that set can reconnect it."""
+    rng = np.random.default_rng(17)
+    checked = reconnected = 0
+    for trial in range(60):
+        n = int(rng.integers(30, 200))
+        m = int(rng.integers(2 * n, 6 * n))
+        u = rng.integers(0, n, m)
+        v = rng.integers(0, n, m)
+        c = rng.integers(1, 20, m)
+        g = O.build_csr(n, u, v, c)
+        s, t = 0, n - 1
+        _, res = O.dinic(g, s, t, want_res=True)
+        blocked = np.zeros(n, np.uint8)
+        blocked[s] = 1
+        U = O.bfs_heights(g, res, t, blocked=blocked) >= n
+        U[s] = False
+        cap = g.cap.copy()
+        fwd = np.nonzero(g.cap > 0)[0]
+        res2 = res.copy()
+        opened = cancelled = False
+        for e in rng.choice(fwd, size=min(len(fwd), int(rng.integers(1, 12))), replace=False):
+            o, x = _apply_to_residual(g, res2, cap, e, int(rng.integers(-5, 6)))
+            opened |= o
+            cancelled |= x
+        if not opened and not cancelled:
+            d1 = O.bfs_heights(O.CSR(n, g.row, g.col, cap, g.rev), res2, t, blocked=blocked)
+            assert (d1[U] >= n).all(), trial
+            checked += 1
+        # an arc x -> w from the set to a vertex that reaches t, saturated:
+        # raising its capacity opens it and x reaches t again
+        tails = np.repeat(np.arange(n), np.diff(g.row))
+        cut = [e for e in fwd if U[tails[e]] and not U[g.col[e]] and g.col[e] != s and res[e] == 0]
+        if cut:
+            res3, cap3 = res.copy(), g.cap.copy()
+            o, _ = _apply_to_residual(g, res3, cap3, cut[0], 3)
+            assert o
+            d2 = O.bfs_heights(O.CSR(n, g.row, g.col, cap3, g.rev), res3, t, blocked=blocked)
+            assert d2[tails[cut[0]]] < n
+            reconnected += 1
+    assert checked >= 10 and reconnected >= 10, (checked, reconnected)
