@@ -25,6 +25,17 @@
 // (cu, cv)) and <output>.map ("vertex component" lines), 1-based, with the
 // components computed on the GPU (mf_graph_scc) and numbered in the order
 // of their smallest vertex id.
+//
+//   maxflow_b200 --scc-convert-test <test.txt> <graph_scc.txt.map> <out_test_scc.txt>
+//   maxflow_b200 --scc-split-queries <test.txt> <graph_scc.txt.map> <test_inter.txt> <test_intra.txt>
+//
+// The reference's two query tools over a .map file (SCC_CONTRACT/
+// convert_test_to_scc.cpp, split_queries_by_scc.cpp): each query's ends
+// mapped to their components ("0 0" for an end outside the map), or the
+// queries split into those whose ends lie in different components (written
+// as component ids, or as given when an end is not mapped) and those inside
+// one component (written as given), with <test_inter.txt>.index listing
+// "query class line" per query.  Host-only text work (no device call).
 #include <sys/stat.h>
 
 #include <algorithm>
@@ -85,13 +96,112 @@ static int scc_main(const char *in, const char *out) {
     return 0;
 }
 
+// "vertex component" pairs (1-based) until the first line that does not
+// scan; a vertex listed twice keeps its last component.  comp[v] = -1 for a
+// vertex in [1, max] the map does not list.
+static bool read_scc_map(const char *path, std::vector<int> &comp, int &max_v) {
+    FILE *f = fopen(path, "r");
+    if (!f) return false;
+    std::vector<std::pair<int, int>> pairs;
+    int a, b;
+    max_v = 0;
+    while (fscanf(f, "%d %d", &a, &b) == 2) {
+        if (a < 0) continue;  // not a vertex id
+        pairs.push_back({a, b});
+        max_v = std::max(max_v, a);
+    }
+    fclose(f);
+    comp.assign((size_t)max_v + 1, -1);
+    for (auto &p : pairs) comp[(size_t)p.first] = p.second;
+    return true;
+}
+
+static int scc_convert_main(const char *test, const char *map, const char *out) {
+    std::vector<int> comp;
+    int max_v = 0;
+    if (!read_scc_map(map, comp, max_v)) {
+        fprintf(stderr, "Cannot open %s\n", map);
+        return 1;
+    }
+    FILE *tf = fopen(test, "r");
+    if (!tf) {
+        fprintf(stderr, "Cannot open %s\n", test);
+        return 1;
+    }
+    FILE *of = fopen(out, "w");
+    if (!of) {
+        fclose(tf);
+        fprintf(stderr, "Cannot open %s for write\n", out);
+        return 1;
+    }
+    int u, v;
+    while (fscanf(tf, "%d %d", &u, &v) == 2) {
+        const bool in = u > 0 && u <= max_v && v > 0 && v <= max_v;
+        const int cu = in ? comp[(size_t)u] : 0, cv = in ? comp[(size_t)v] : 0;
+        if (cu > 0 && cv > 0) fprintf(of, "%d %d\n", cu, cv);
+        else fprintf(of, "0 0\n");
+    }
+    fclose(tf);
+    fclose(of);
+    return 0;
+}
+
+static int scc_split_main(const char *test, const char *map, const char *inter, const char *intra) {
+    std::vector<int> comp;
+    int max_v = 0;
+    if (!read_scc_map(map, comp, max_v)) {
+        fprintf(stderr, "Cannot open %s\n", map);
+        return 1;
+    }
+    FILE *tf = fopen(test, "r");
+    if (!tf) {
+        fprintf(stderr, "Cannot open %s\n", test);
+        return 1;
+    }
+    FILE *fi = fopen(inter, "w"), *fa = fopen(intra, "w");
+    if (!fi || !fa) {
+        if (fi) fclose(fi);
+        if (fa) fclose(fa);
+        fclose(tf);
+        fprintf(stderr, "Cannot open the output query files\n");
+        return 1;
+    }
+    FILE *ix = fopen((std::string(inter) + ".index").c_str(), "w");
+    int u, v, q = 0, ni = 0, na = 0;
+    while (fscanf(tf, "%d %d", &u, &v) == 2) {
+        ++q;
+        const bool in = u > 0 && u <= max_v && v > 0 && v <= max_v;
+        const int cu = in ? comp[(size_t)u] : 0, cv = in ? comp[(size_t)v] : 0;
+        if (cu > 0 && cv > 0 && cu == cv) {
+            fprintf(fa, "%d %d\n", u, v);  // one component: the original graph's ids
+            if (ix) fprintf(ix, "%d intra %d\n", q, ++na);
+            continue;
+        }
+        if (cu > 0 && cv > 0) fprintf(fi, "%d %d\n", cu, cv);  // across components: their ids
+        else fprintf(fi, "%d %d\n", u, v);                     // an end the map does not list
+        if (ix) fprintf(ix, "%d inter %d\n", q, ++ni);
+    }
+    fclose(tf);
+    fclose(fi);
+    fclose(fa);
+    if (ix) fclose(ix);
+    fprintf(stderr, "[Split] total queries=%d, inter=%d, intra=%d\n", q, ni, na);
+    return 0;
+}
+
 int main(int argc, char **argv) {
     if (argc == 4 && !strcmp(argv[1], "--scc-contract")) return scc_main(argv[2], argv[3]);
+    if (argc == 5 && !strcmp(argv[1], "--scc-convert-test")) return scc_convert_main(argv[2], argv[3], argv[4]);
+    if (argc == 6 && !strcmp(argv[1], "--scc-split-queries"))
+        return scc_split_main(argv[2], argv[3], argv[4], argv[5]);
     if (argc < 3) {
         fprintf(stderr, "Usage: %s <input_dir> <output_dir> [mode] [--batch] [--R N] [--csr-cache FILE]\n",
                 argv[0]);
         fprintf(stderr, "  mode = static (default) | dynamic\n");
         fprintf(stderr, "   or: %s --scc-contract <input_graph.txt> <output_graph_scc.txt>\n", argv[0]);
+        fprintf(stderr, "   or: %s --scc-convert-test <test.txt> <graph_scc.txt.map> <out_test_scc.txt>\n", argv[0]);
+        fprintf(stderr, "   or: %s --scc-split-queries <test.txt> <graph_scc.txt.map> <test_inter.txt> <test_intra.txt>\n",
+                argv[0]);
         return 1;
     }
     std::string in = argv[1], outd = argv[2], mode = "static";

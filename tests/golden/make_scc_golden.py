@@ -9,7 +9,13 @@ oracle/build_ref.sh) and keeps its two outputs beside the graph:
 The cases under tests/golden_scc/ are made here first: seeded graphs rich in
 non-trivial components (overlapping random cycles joined by one-way edges,
 with parallel edges, self loops, zero or negative capacities and ids out of
-range, which the reader skips) and a sparse R-MAT.
+range, which the reader skips) and a sparse R-MAT, each with a query file
+scc_queries.txt (pairs in range, ends out of range, 0 and negative).
+The reference's two query tools (convert_test_to_scc.cpp,
+split_queries_by_scc.cpp, also compiled by oracle/build_ref.sh) then run on
+every case's queries (test.txt, or scc_queries.txt) against its
+ref_scc.txt.map; their outputs are kept as ref_scc_test.txt,
+ref_scc_inter.txt (+ .index) and ref_scc_intra.txt.
 
 usage: python tests/golden/make_scc_golden.py
 """
@@ -71,12 +77,28 @@ def main():
     for name, fn in (("cycles_3000", case_cycles), ("rmat12_sparse", case_rmat12)):
         d = os.path.join(SCC_DIR, name)
         os.makedirs(d, exist_ok=True)
-        write_raw(os.path.join(d, "graph.txt"), *fn())
+        n, u, v, c = fn()
+        write_raw(os.path.join(d, "graph.txt"), n, u, v, c)
+        rng = np.random.default_rng(len(name))
+        q = rng.integers(1, n + 1, (200, 2))
+        q[:6] = [[0, 5], [5, 0], [-3, 4], [4, n + 1], [n, n], [1, 1]]
+        with open(os.path.join(d, "scc_queries.txt"), "w") as f:
+            f.writelines("%d %d\n" % (a, b) for a, b in q.tolist())
     graphs = sorted(glob.glob(os.path.join(HERE, "*", "graph.txt")) + glob.glob(os.path.join(SCC_DIR, "*", "graph.txt")))
+    ref_dir = os.path.dirname(ref)
     for g in graphs:
-        out = os.path.join(os.path.dirname(g), "ref_scc.txt")
+        d = os.path.dirname(g)
+        out = os.path.join(d, "ref_scc.txt")
         subprocess.run([ref, g, out], check=True, stderr=subprocess.DEVNULL)
         print(os.path.relpath(out, ROOT), open(out).readline().strip())
+        qf = os.path.join(d, "test.txt")
+        if not os.path.exists(qf):
+            qf = os.path.join(d, "scc_queries.txt")
+        subprocess.run([os.path.join(ref_dir, "convert_test_to_scc"), qf, out + ".map",
+                        os.path.join(d, "ref_scc_test.txt")], check=True, stderr=subprocess.DEVNULL)
+        subprocess.run([os.path.join(ref_dir, "split_queries_by_scc"), qf, out + ".map",
+                        os.path.join(d, "ref_scc_inter.txt"), os.path.join(d, "ref_scc_intra.txt")],
+                       check=True, stderr=subprocess.DEVNULL)
 
 
 if __name__ == "__main__":

@@ -3,7 +3,9 @@
 
 CPU: the oracle's Kosaraju restatement writes byte-identical files to the
 reference tool's own outputs (tests/golden*/*/ref_scc.txt{,.map}, made by
-tests/golden/make_scc_golden.py from the tool compiled out of its source).
+tests/golden/make_scc_golden.py from the tool compiled out of its source),
+and the CLI's two query-tool modes write byte-identical files to the
+reference's convert_test_to_scc and split_queries_by_scc.
 GPU: the device decomposition (mf_graph_scc, and the CLI's --scc-contract)
 gives the reference's partition and, under the bijection between the two
 numberings, its contracted graph; on larger seeded graphs, and after
@@ -71,6 +73,30 @@ def test_oracle_kosaraju_writes_the_reference_files(d, tmp_path):
     for suffix in ("", ".map"):
         with open(out + suffix, "rb") as a, open(os.path.join(d, "ref_scc.txt" + suffix), "rb") as b:
             assert a.read() == b.read(), suffix
+
+
+def _queries(d):
+    q = os.path.join(d, "test.txt")
+    return q if os.path.exists(q) else os.path.join(d, "scc_queries.txt")
+
+
+@pytest.mark.parametrize("d", CASES, ids=IDS)
+def test_cli_query_tools_write_the_reference_files(d, tmp_path):
+    """--scc-convert-test and --scc-split-queries (host text work, no device
+    call) on each case's queries and the reference tool's map: byte for byte
+    the files of SCC_CONTRACT/convert_test_to_scc.cpp and
+    split_queries_by_scc.cpp, including ends out of range, 0 and negative."""
+    import mscresearch_b200 as mf
+    mp = os.path.join(d, "ref_scc.txt.map")
+    a = str(tmp_path / "test_scc.txt")
+    subprocess.run([mf.CLI_PATH, "--scc-convert-test", _queries(d), mp, a], check=True, capture_output=True)
+    inter, intra = str(tmp_path / "inter.txt"), str(tmp_path / "intra.txt")
+    subprocess.run([mf.CLI_PATH, "--scc-split-queries", _queries(d), mp, inter, intra], check=True,
+                   capture_output=True)
+    for mine, ref in ((a, "ref_scc_test.txt"), (inter, "ref_scc_inter.txt"), (intra, "ref_scc_intra.txt"),
+                      (inter + ".index", "ref_scc_inter.txt.index")):
+        with open(mine, "rb") as x, open(os.path.join(d, ref), "rb") as y:
+            assert x.read() == y.read(), ref
 
 
 def test_oracle_kosaraju_numbering_is_topological():
